@@ -1,0 +1,170 @@
+/*
+ * voila_cuda.h -- C ABI of the CUDA flavor for VOILA's data-parallel hot path on one
+ * NVIDIA B200 (sm_100a).
+ *
+ * Plain C: opaque handles, pointers and sizes only; no C++ or torch types cross it.  Every
+ * call returns a status (VC_OK on success) and never throws; vc_last_error() returns the
+ * calling thread's message for the last failed call.
+ *
+ * How the pieces map onto the reference (t1mm3/vldb_voila):
+ *
+ *   engine + tables   runtime::Database / Relation / Attribute with MinMaxInfo
+ *                     (db-engine-paradigms/include/common/runtime/Database.hpp:28-75,
+ *                      common/runtime/Types.hpp:11-33).  Columns live in HBM.
+ *   plan text         the relalg tree (relalg.hpp:12-178) a benchmark query builds
+ *                     (bench_tpch_rel.cpp), serialised as an S-expression
+ *   query new/run/    the generated-library ABI voila_query_new/run/reset/free
+ *   reset/free        (codegen.cpp:371-392; called by Compiler::_run, compiler.cpp:488-533)
+ *   flavor string     the per-pipeline blend, computation_type=cuda(...) next to
+ *                     scalar/avx512/vector(N) (blend_space_point.hpp:10-45)
+ *   result text       QueryResult rows "a|b|c\n" (runtime_framework.cpp:77-111), compared
+ *                     order-insensitively like Query::check_result (:220-280)
+ *
+ * Threading: one engine may be used from several host threads; calls on the same query
+ * must be serialised by the caller.  Streams are passed as a plain cudaStream_t cast to
+ * void* (NULL = the legacy default stream).
+ */
+#ifndef VOILA_CUDA_H
+#define VOILA_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define VC_OK 0
+#define VC_ERR_INVALID 1     /* bad argument, unknown table/column, malformed plan */
+#define VC_ERR_CUDA 2        /* a CUDA runtime call failed (message names it) */
+#define VC_ERR_CAPACITY 3    /* a device table ran out of slots */
+#define VC_ERR_TIMEOUT 4     /* a bounded device wait gave up */
+#define VC_ERR_COMPILE 5     /* NVRTC rejected generated code (log in the message) */
+#define VC_ERR_UNSUPPORTED 6 /* valid plan the CUDA flavor does not handle (e.g. int64 overflow) */
+#define VC_ERR_NO_DEVICE 7   /* no usable CUDA device */
+
+/* column types (same values as vc_gen_spec.type) */
+#define VC_U8 1
+#define VC_I16 2
+#define VC_I32 3
+#define VC_I64 4
+
+typedef struct vc_engine vc_engine;
+typedef struct vc_query vc_query;
+
+/* Thread-local message of the last failing call ("" if none). Replaces the reference's
+ * ASSERT/exception reporting (runtime.hpp:38-49, compiler.cpp:564-571). */
+const char* vc_last_error(void);
+
+/* Library version string. */
+const char* vc_version(void);
+
+/* ---------------------------------------------------------------- engine / database --- */
+
+/* Creates an engine on CUDA device `device`.  Replaces constructing runtime::Database
+ * (main.cpp:66) for the device side. */
+int vc_engine_create(int device, vc_engine** out);
+int vc_engine_destroy(vc_engine* eng);
+
+/* Creates an engine without a device: vc_query_new then lowers the plan, generates the
+ * kernels and compiles them for sm_100a (so code generation is testable on a build host),
+ * but queries cannot run.  `sms` sizes grids as on a device with that many SMs. */
+int vc_engine_create_offline(int sms, vc_engine** out);
+
+/* Declares a table of `rows` rows (Relation with nrTuples, Database.hpp:66-75). */
+int vc_table_create(vc_engine* eng, const char* table, int64_t rows);
+int vc_table_drop(vc_engine* eng, const char* table);
+
+/* Declares a column with its value domain [lo, hi] (Relation::insert + Attribute::minmax,
+ * Database.hpp:32-44; read by the reference's codegen at codegen.cpp:11-19) and allocates
+ * its device storage. */
+int vc_column_add(vc_engine* eng, const char* table, const char* column, int type, int64_t lo, int64_t hi);
+
+/* Copies `rows` values from host memory into the column (Attribute::operator=,
+ * Database.hpp:59-62).  Asynchronous on `stream`; pinned host memory gives full speed. */
+int vc_column_upload(vc_engine* eng, const char* table, const char* column, const void* host, int64_t rows,
+	void* stream);
+
+/* Copies the column back to host memory (for checking). */
+int vc_column_download(vc_engine* eng, const char* table, const char* column, void* host, int64_t rows,
+	void* stream);
+
+/* Uses caller-owned device memory (16-byte aligned, `rows` values) as the column; the
+ * engine's own buffer is freed.  The memory must outlive every query that reads it. */
+int vc_column_attach(vc_engine* eng, const char* table, const char* column, void* device_ptr);
+
+/* Device address of the column's data. */
+int vc_column_device_ptr(vc_engine* eng, const char* table, const char* column, void** out);
+
+/* Fills the column on the device from a seeded generator (see vc_gen_spec in datagen.h:
+ * kind, type, a, b, c, s, seed, n).  `zipf_cdf` (host, b doubles) is required for a skewed
+ * VC_GEN_ZIPF column.  Stands in for the TPC-H/SSB import (Import.cpp:165-250). */
+int vc_column_generate(vc_engine* eng, const char* table, const char* column, int32_t kind, int64_t a,
+	int64_t b, int64_t c, double s, uint64_t seed, const double* zipf_cdf, void* stream);
+
+/* Host-side generator for the same columns: writes rows [begin, begin+count) into `out`
+ * (element type `type`). */
+int vc_gen_host(int32_t kind, int32_t type, int64_t a, int64_t b, int64_t c, double s, uint64_t seed, int64_t n,
+	const double* zipf_cdf, int64_t begin, int64_t count, void* out);
+
+/* Inverse-CDF table of Zipf(s) over n keys (n doubles). */
+int vc_gen_zipf_cdf(double s, int64_t n, double* out);
+
+/* Text description of a synthetic workload spec such as
+ * "join_aggr:build=1500000,probe=6000000,sel=0.2,seed=2": tables, column generators with
+ * their domains and the plan text.  Writes at most `cap` bytes; *len gets the full length. */
+int vc_workload_describe(const char* spec, char* buf, size_t cap, size_t* len);
+
+/* Spec strings of the seeded mixed batch (one per line). */
+int vc_workload_batch(int count, uint64_t seed, int64_t min_rows, int64_t max_rows, char* buf, size_t cap,
+	size_t* len);
+
+/* ---------------------------------------------------------------- queries ------------- */
+
+/* Translates plan text into fused CUDA pipelines with the flavor's knobs, generates and
+ * compiles their kernels (NVRTC, cached by source) and allocates the query's device
+ * state.  Replaces Compiler::_generate + call_cxx_compiler + voila_query_new
+ * (compiler.cpp:19-57, :343-385; codegen.cpp:371-376).
+ * flavor: "" or "cuda(threads=256,rows=4,aggr=auto,cache=1024,grid=0,graph=0)". */
+int vc_query_new(vc_engine* eng, const char* plan, const char* flavor, vc_query** out);
+
+/* Launches the query's pipelines on `stream` (voila_query_run, codegen.cpp:390; the
+ * pipelines run in order like Query::run, runtime_framework.cpp:166-198).  Asynchronous:
+ * results are read with vc_query_result_*. */
+int vc_query_run(vc_query* q, void* stream);
+
+/* Clears the query's state between runs (voila_query_reset, codegen.cpp:391).  vc_query_run
+ * resets the device state itself, so this only drops the host copy of the last result. */
+int vc_query_reset(vc_query* q);
+
+/* voila_query_free (codegen.cpp:392). */
+int vc_query_free(vc_query* q);
+
+/* Waits for the last run and reports its result shape (rows x cols, int64 values). */
+int vc_query_result_shape(vc_query* q, int64_t* rows, int32_t* cols);
+
+/* Copies the last result, column-major (cols x rows int64), into `out` (capacity `cap`
+ * values). */
+int vc_query_result_copy(vc_query* q, int64_t* out, int64_t cap);
+
+/* The last result as QueryResult text (runtime_framework.cpp:77-111): decimal values
+ * separated by '|', one row per line, in device order (compare after sorting lines). */
+int vc_query_result_text(vc_query* q, char* buf, size_t cap, size_t* len);
+
+/* JSON description: pipelines, kernels, flavor, algorithmic bytes, generated source size. */
+int vc_query_info(vc_query* q, char* buf, size_t cap, size_t* len);
+
+/* Generated CUDA source of the query (for inspection and tests). */
+int vc_query_source(vc_query* q, char* buf, size_t cap, size_t* len);
+
+/* Per-launch device times of the last run, in launch order (enable first with
+ * vc_query_profile).  `names` receives kernel names separated by '\n'. */
+int vc_query_profile(vc_query* q, int enable);
+int vc_query_timings(vc_query* q, float* ms, int cap, int* n, char* names, size_t names_cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -120,7 +120,7 @@ size_t load_workload(runtime::Database& db, const vc_workload::Workload& w, int6
 			std::vector<double> cdf;
 			if (c.spec.kind == VC_GEN_ZIPF && c.spec.s != 0.0) {
 				cdf.resize((size_t)c.spec.b);
-				vc_gen_zipf_cdf(c.spec.s, c.spec.b, cdf.data());
+				vc_gen_build_zipf_cdf(c.spec.s, c.spec.b, cdf.data());
 			}
 			std::unique_ptr<algebra::Type> type;
 			switch (c.spec.type) {

@@ -1,0 +1,244 @@
+"""CPU oracle for the hot path -- TEST INFRASTRUCTURE ONLY.
+
+A numpy restatement of what the reference's generated pipelines compute for a relational
+plan: scans, selections, projections, Join01/JoinN hash joins and hash / global
+aggregations, with exact int64 arithmetic, emitting QueryResult text rows.  Only tests/,
+__graft_entry__.smoke() and bench.py's cpu_baseline leg may use it, and only as the checker
+(or the timed CPU port); the product path never calls it.
+
+Pinned: tests/golden holds the reference's own outputs (its hyper and vectorwise flavors,
+compiled from the reference sources by oracle/ref/Makefile and run by oracle/ref/ref_run)
+for seeded workloads; tests/test_oracle_golden.py checks this oracle against them.
+
+Semantics followed (reference file:line):
+  - Scan: every row of the base table, columns named "table.col" (relalg_translator.cpp:202-272)
+  - Select: rows whose predicate holds (seltrue + emit, relalg_translator.cpp:343-378;
+    comparison primitives kernel_generator.py:414-454)
+  - Project: visible columns become the projection list; assignments are visible to later
+    entries of the same list (relalg_translator.cpp:275-341)
+  - arithmetic: exact integers (the typing pass widens results so nothing wraps,
+    typing_pass.cpp:164-176; vectorwise primitives compute in the result type,
+    kernel_generator.py:439-445)
+  - HashJoin: visible after the probe: probe columns, build keys (= probe key values),
+    build payloads (relalg_translator.cpp:955-1012); JoinN emits one row per match,
+    Join01 stops after the first match (:1032-1042)
+  - HashAggr: groups by keys, sums and counts; a hidden count if none is given (:469-472);
+    output = keys then visible aggregates for groups with count > 0 (:692-771); global
+    aggregation is one group (:430-441) and is emitted only when its count is > 0
+  - output text: decimal integers joined by '|', one line per row
+    (voila_cast::to_cstr runtime.hpp:346-391, QueryResult::push_col runtime_framework.cpp:77-111),
+    compared after sorting lines (Query::check_result, runtime_framework.cpp:220-280)
+"""
+import numpy as np
+
+_FUNS = {
+    "<=": "le", "<": "lt", ">=": "ge", ">": "gt", "=": "eq", "!=": "ne", "+": "add", "-": "sub", "*": "mul",
+}
+
+
+def parse_sexpr(text):
+    """Plan text -> nested lists of atoms (strings)."""
+    tokens = text.replace("(", " ( ").replace(")", " ) ").split()
+    pos = 0
+
+    def read():
+        nonlocal pos
+        t = tokens[pos]
+        pos += 1
+        if t == "(":
+            out = []
+            while tokens[pos] != ")":
+                out.append(read())
+            pos += 1
+            return out
+        if t == ")":
+            raise ValueError("unexpected ')'")
+        return t
+
+    node = read()
+    if pos != len(tokens):
+        raise ValueError("trailing text after plan")
+    return node
+
+
+class Frame:
+    """An ordered set of named columns of equal length (the reference's 'flow')."""
+
+    def __init__(self, cols, n):
+        self.cols = cols  # list of (name, ndarray int64)
+        self.n = n
+
+    def get(self, name):
+        for k, v in reversed(self.cols):
+            if k == name:
+                return v
+        raise KeyError(f"cannot find '{name}' among the visible columns")
+
+    def take(self, idx):
+        return Frame([(k, v[idx]) for k, v in self.cols], int(len(idx)))
+
+
+def _eval(e, frame, env):
+    head = e[0]
+    if head == "const":
+        return np.full(frame.n, int(e[1]), dtype=np.int64)
+    if head == "col":
+        if e[1] in env:
+            return env[e[1]]
+        return frame.get(e[1])
+    if head == "fun":
+        f = _FUNS.get(e[1], e[1])
+        a = [_eval(x, frame, env) for x in e[2:]]
+        if f == "add":
+            return a[0] + a[1]
+        if f == "sub":
+            return a[0] - a[1]
+        if f == "mul":
+            return a[0] * a[1]
+        if f == "lt":
+            return a[0] < a[1]
+        if f == "le":
+            return a[0] <= a[1]
+        if f == "gt":
+            return a[0] > a[1]
+        if f == "ge":
+            return a[0] >= a[1]
+        if f == "eq":
+            return a[0] == a[1]
+        if f == "ne":
+            return a[0] != a[1]
+        if f == "and":
+            return a[0] & a[1]
+        if f == "or":
+            return a[0] | a[1]
+        raise ValueError(f"unknown function {e[1]}")
+    raise ValueError(f"bad expression {e}")
+
+
+def _check_int64(arrs):
+    # values are computed in int64; the product rejects plans whose declared ranges could
+    # leave int64, so the oracle only needs to detect accidental overflow
+    for a in arrs:
+        if a.dtype == np.int64 and a.size and (a.max() > 2**62 or a.min() < -2**62):
+            raise OverflowError("oracle value range close to int64 limits")
+
+
+def _pack_keys(cols):
+    """Unique int64 code per key tuple (via np.unique on stacked keys)."""
+    if len(cols) == 1:
+        return cols[0]
+    stacked = np.stack(cols, axis=1)
+    _, inv = np.unique(stacked, axis=0, return_inverse=True)
+    return inv.reshape(-1).astype(np.int64)
+
+
+def _op(node, db):
+    head = node[0]
+    if head == "scan":
+        table = node[1]
+        cols = [(f"{table}.{c}", np.asarray(db[table][c]).astype(np.int64)) for c in node[2]]
+        n = len(cols[0][1]) if cols else 0
+        return Frame(cols, n)
+    if head == "select":
+        f = _op(node[2], db)
+        m = _eval(node[1], f, {}).astype(bool)
+        return f.take(np.nonzero(m)[0])
+    if head == "project":
+        f = _op(node[2], db)
+        env = {}
+        out = []
+        for e in node[1]:
+            if e[0] == "assign":
+                v = _eval(e[2], f, env)
+                env[e[1]] = v
+                out.append((e[1], v))
+            elif e[0] == "col":
+                out.append((e[1], env[e[1]] if e[1] in env else f.get(e[1])))
+            else:
+                raise ValueError("projection entries must be columns or assignments")
+        return Frame(out, f.n)
+    if head == "join":
+        join01 = node[1] == "join01"
+        probe = _op(node[4], db)
+        build = _op(node[7], db)
+        pk = [_eval(k, probe, {}) for k in node[2]]
+        bk = [_eval(k, build, {}) for k in node[5]]
+        bpay = [(p[1], _eval(p, build, {})) for p in node[6]]
+        # one code space for probe and build key tuples
+        if len(pk) == 1:
+            pc, bc = pk[0], bk[0]
+        else:
+            both = [np.concatenate([a, b]) for a, b in zip(pk, bk)]
+            code = _pack_keys(both)
+            pc, bc = code[:probe.n], code[probe.n:]
+        order = np.argsort(bc, kind="stable")
+        sb = bc[order]
+        lo = np.searchsorted(sb, pc, side="left")
+        hi = np.searchsorted(sb, pc, side="right")
+        cnt = hi - lo
+        if join01:
+            cnt = np.minimum(cnt, 1)
+        rows = np.repeat(np.arange(probe.n), cnt)
+        starts = np.repeat(lo, cnt)
+        offs = np.arange(len(rows)) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+        bidx = order[starts + offs] if len(rows) else np.zeros(0, dtype=np.int64)
+        out = probe.take(rows)
+        for i, k in enumerate(node[5]):
+            # build keys take the probe key values (relalg_translator.cpp:965-975)
+            out.cols.append((k[1], pk[i][rows]))
+        for name, v in bpay:
+            out.cols.append((name, v[bidx]))
+        return out
+    raise ValueError(f"unsupported operator {head}")
+
+
+def run_plan(plan, db):
+    """Result rows (list of tuples of ints) of plan text over db = {table: {col: array}}."""
+    node = parse_sexpr(plan) if isinstance(plan, str) else plan
+    if node[0] != "aggr":
+        f = _op(node, db)
+        return [tuple(int(v[i]) for _, v in f.cols) for i in range(f.n)]
+    glob = node[1] == "global"
+    f = _op(node[4], db)
+    keys = [_eval(k, f, {}) for k in node[2]]
+    aggs = []
+    has_count = False
+    for a in node[3]:
+        if a[1] == "count":
+            aggs.append(("count", None, True))
+            has_count = True
+        else:
+            aggs.append(("sum", _eval(a[2], f, {}).astype(np.int64), True))
+    if not has_count:
+        aggs.append(("count", None, False))
+    _check_int64(keys + [v for _, v, _ in aggs if v is not None])
+    if glob:
+        if f.n == 0:
+            return []
+        row = []
+        for kind, v, vis in aggs:
+            if vis:
+                row.append(int(f.n) if kind == "count" else int(v.sum(dtype=np.int64)))
+        return [tuple(row)]
+    if f.n == 0:
+        return []
+    stacked = np.stack(keys, axis=1)
+    uniq, inv = np.unique(stacked, axis=0, return_inverse=True)
+    inv = inv.reshape(-1)
+    order = np.argsort(inv, kind="stable")
+    bounds = np.concatenate([[0], np.nonzero(np.diff(inv[order]))[0] + 1])
+    counts = np.diff(np.concatenate([bounds, [f.n]]))
+    cols = [uniq[:, i] for i in range(uniq.shape[1])]
+    for kind, v, vis in aggs:
+        if not vis:
+            continue
+        if kind == "count":
+            cols.append(counts.astype(np.int64))
+        else:
+            cols.append(np.add.reduceat(v[order], bounds).astype(np.int64))
+    return [tuple(int(c[i]) for c in cols) for i in range(len(uniq))]
+
+
+def result_lines(rows):
+    """QueryResult text lines, sorted (the reference's order-insensitive comparison)."""
+    return sorted("|".join(str(v) for v in r) for r in rows)

@@ -164,7 +164,7 @@ VC_GEN_FN void vc_gen_store(int32_t type, void* out, int64_t i, int64_t v)
  * Host only; the device generator receives the finished table.  Built with one left-to-right
  * summation and no fused multiply-add, so every build of this header yields the same doubles.
  */
-static inline void vc_gen_zipf_cdf(double s, int64_t n, double* cdf)
+static inline void vc_gen_build_zipf_cdf(double s, int64_t n, double* cdf)
 {
 	double acc = 0.0;
 	for (int64_t k = 1; k <= n; k++) {

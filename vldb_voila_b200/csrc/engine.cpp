@@ -1,0 +1,955 @@
+/*
+ * Runtime of the CUDA flavor and the C ABI declared in include/voila_cuda.h.
+ *
+ * A query follows the reference's lifecycle (Compiler::_generate -> call_cxx_compiler ->
+ * voila_query_new -> per repetition voila_query_reset + voila_query_run, compiler.cpp:343-533):
+ * plan text is lowered into pipelines, the pipelines' device state is allocated, one CUDA
+ * module is generated and compiled for the whole query, and each run launches the pipelines
+ * in order on one stream (Query::run runs pipelines sequentially, runtime_framework.cpp:166-198;
+ * here the parallelism is inside each kernel instead of tbb::parallel_for over threads).
+ */
+#include <algorithm>
+#include <cinttypes>
+#include <cstring>
+#include <sstream>
+
+#include "engine_internal.hpp"
+#include "workloads.hpp"
+#include "../../include/voila_cuda.h"
+
+namespace vc {
+
+/* AOT kernels (datagen.cu) */
+cudaError_t launch_generate(void* out, const vc_gen_spec& spec, const double* zipf_cdf_dev, int64_t rows,
+	cudaStream_t stream);
+
+static thread_local std::string g_last_error;
+
+static int64_t pow2_at_least(int64_t x)
+{
+	int64_t p = 1;
+	while (p < x) {
+		p <<= 1;
+	}
+	return p;
+}
+
+/* ------------------------------------------------------------------ flavor ------------- */
+
+std::string Flavor::str() const
+{
+	std::ostringstream o;
+	o << "cuda(threads=" << threads << ",rows=" << rows << ",aggr=" << aggr << ",cache=" << cache_slots
+	  << ",grid=" << grid << ",dense=" << dense_limit << ",graph=" << (graph ? 1 : 0) << ")";
+	return o.str();
+}
+
+Flavor Flavor::parse(const std::string& s0)
+{
+	Flavor f;
+	std::string s = s0;
+	s.erase(std::remove_if(s.begin(), s.end(), ::isspace), s.end());
+	if (s.empty() || s == "cuda" || s == "cuda()") {
+		return f;
+	}
+	if (s.rfind("computation_type=", 0) == 0) {
+		s = s.substr(17);
+	}
+	if (s.rfind("cuda(", 0) != 0 || s.back() != ')') {
+		throw Error(1, "flavor must look like cuda(key=value,...), got '" + s0 + "'");
+	}
+	std::stringstream ss(s.substr(5, s.size() - 6));
+	std::string item;
+	while (std::getline(ss, item, ',')) {
+		if (item.empty()) {
+			continue;
+		}
+		auto eq = item.find('=');
+		if (eq == std::string::npos) {
+			throw Error(1, "flavor item without '=': " + item);
+		}
+		std::string k = item.substr(0, eq), v = item.substr(eq + 1);
+		auto num = [&](int lo, int hi) {
+			int x = 0;
+			try {
+				x = std::stoi(v);
+			} catch (...) {
+				throw Error(1, "flavor " + k + " must be an integer");
+			}
+			if (x < lo || x > hi) {
+				throw Error(1, "flavor " + k + " out of range");
+			}
+			return x;
+		};
+		if (k == "threads") {
+			f.threads = num(32, 1024);
+			if (f.threads % 32) {
+				throw Error(1, "threads must be a multiple of 32");
+			}
+		} else if (k == "rows") {
+			f.rows = num(1, 16);
+			if (f.rows & (f.rows - 1)) {
+				throw Error(1, "rows must be a power of two");
+			}
+		} else if (k == "aggr") {
+			if (v != "auto" && v != "dense" && v != "global" && v != "cache") {
+				throw Error(1, "aggr must be auto, dense, global or cache");
+			}
+			f.aggr = v;
+		} else if (k == "cache") {
+			f.cache_slots = num(32, 8192);
+		} else if (k == "grid") {
+			f.grid = num(0, 64);
+		} else if (k == "dense") {
+			f.dense_limit = num(1, 1 << 22);
+		} else if (k == "graph") {
+			f.graph = num(0, 1) != 0;
+		} else {
+			throw Error(1, "unknown flavor knob '" + k + "'");
+		}
+	}
+	return f;
+}
+
+/* ------------------------------------------------------------------ engine ------------- */
+
+Engine::~Engine()
+{
+	if (offline) {
+		return;
+	}
+	cudaSetDevice(device);
+	for (auto& t : tables) {
+		for (auto& c : t.second.cols) {
+			if (c.owned && c.dev) {
+				cudaFree(c.dev);
+			}
+		}
+	}
+}
+
+static void* dev_alloc(Query& q, size_t bytes)
+{
+	void* p = nullptr;
+	if (q.eng->offline) {
+		/* stand-in addresses: offline engines only generate and compile code */
+		p = (void*)q.eng->fake_next;
+		q.eng->fake_next += ((bytes + 255) / 256 + 1) * 256;
+		return p;
+	}
+	VC_CHECK_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 256)));
+	q.allocations.push_back(p);
+	return p;
+}
+
+Query::~Query()
+{
+	if (eng && eng->offline) {
+		return;
+	}
+	if (eng) {
+		cudaSetDevice(eng->device);
+	}
+	if (graph) {
+		cudaGraphExecDestroy(graph);
+	}
+	for (auto e : ev) {
+		cudaEventDestroy(e);
+	}
+	for (void* p : allocations) {
+		cudaFree(p);
+	}
+}
+
+struct QueryState {
+	std::vector<PipeDeviceState> pipes;
+	std::vector<cudaKernel_t> kernels;
+	std::vector<int> occupancy;
+	std::vector<std::pair<void*, size_t>> memsets;
+};
+
+static std::map<Query*, QueryState> g_state;
+static std::mutex g_state_mu;
+
+static QueryState& state_of(Query& q)
+{
+	std::lock_guard<std::mutex> g(g_state_mu);
+	return g_state[&q];
+}
+
+void query_prepare(Query& q)
+{
+	Engine& e = *q.eng;
+	if (!e.offline) {
+		VC_CHECK_CUDA(cudaSetDevice(e.device));
+	}
+	RelOpP root = parse_plan(q.plan_text);
+	q.plan = lower_plan(root, e.tables, q.flavor);
+	LoweredPlan& plan = q.plan;
+	QueryState& st = state_of(q);
+	st.pipes.assign(plan.pipes.size(), PipeDeviceState());
+
+	q.err = (unsigned*)dev_alloc(q, 256);
+	q.out_count = (unsigned long long*)dev_alloc(q, 256);
+	st.memsets.push_back({q.err, 256});
+	st.memsets.push_back({q.out_count, 256});
+
+	for (auto& jd : plan.joins) {
+		const int64_t rows = std::max<int64_t>(jd.build_rows, 1);
+		const int sb = jd.slot_bytes();
+		const int spb = std::max(1, 32 / sb);
+		const int64_t slots = std::max<int64_t>(pow2_at_least(2 * rows), 2 * spb);
+		jd.max_buckets = slots / spb;
+		jd.table = dev_alloc(q, (size_t)slots * sb);
+		jd.stage_keys = dev_alloc(q, (size_t)rows * (jd.key64 ? 8 : 4));
+		jd.stage_pay = dev_alloc(q, (size_t)rows * (jd.pay64 ? 8 : 4));
+		jd.words = (unsigned long long*)dev_alloc(q, 256);
+		st.memsets.push_back({jd.words, 256});
+	}
+	Pipeline& rp = plan.pipes[plan.result_pipe];
+	for (auto& p : plan.pipes) {
+		PipeDeviceState& ps = st.pipes[p.id];
+		const int A = (int)p.sink.aggs.size();
+		switch (p.sink.kind) {
+		case Sink::JoinBuild:
+			ps.stage_hash = dev_alloc(q, (size_t)std::max<int64_t>(plan.joins[p.sink.join].build_rows, 1) * 8);
+			break;
+		case Sink::AggGlobal:
+			ps.sink_cap = 1;
+			ps.sink_bytes = (size_t)A * 8;
+			break;
+		case Sink::AggDense:
+			ps.sink_cap = (int64_t)p.sink.domain;
+			ps.sink_bytes = (size_t)p.sink.domain * A * 8;
+			break;
+		case Sink::AggHash:
+			ps.sink_cap = std::max<int64_t>(pow2_at_least(2 * std::max<int64_t>(p.sink.groups_bound, 1)), 1024);
+			ps.sink_bytes = (size_t)ps.sink_cap * (1 + A) * 8;
+			break;
+		case Sink::Emit:
+			break;
+		}
+		if (ps.sink_bytes) {
+			ps.sink_dev = dev_alloc(q, ps.sink_bytes);
+			st.memsets.push_back({ps.sink_dev, ps.sink_bytes});
+		}
+	}
+	switch (rp.sink.kind) {
+	case Sink::AggGlobal: q.out_cap = 1; break;
+	case Sink::AggDense: q.out_cap = (int64_t)rp.sink.domain; break;
+	default: q.out_cap = std::max<int64_t>(rp.sink.groups_bound, 1); break;
+	}
+	q.out = (int64_t*)dev_alloc(q, (size_t)q.out_cap * plan.result_cols * 8);
+
+	q.code = generate_cuda(plan, q.flavor, st.pipes, q.out, q.out_cap, q.out_count, q.params);
+	std::string log;
+	if (e.offline) {
+		jit_cubin(q.code.source, &log);
+		return;
+	}
+	q.mod = jit_compile(q.code.source, &log);
+
+	st.kernels.clear();
+	st.occupancy.clear();
+	for (auto& l : q.code.launches) {
+		cudaKernel_t k;
+		VC_CHECK_CUDA(cudaLibraryGetKernel(&k, q.mod->lib, l.kernel.c_str()));
+		if (l.smem > 48 * 1024) {
+			VC_CHECK_CUDA(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem));
+		}
+		int occ = 0;
+		VC_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k, l.threads, l.smem));
+		if (occ < 1) {
+			throw Error(6, "kernel " + l.kernel + " cannot be resident with its shared memory");
+		}
+		st.kernels.push_back(k);
+		st.occupancy.push_back(occ);
+	}
+	/* fixed parameter slots: error word and column pointers */
+	for (auto& p : plan.pipes) {
+		auto& prm = q.params[p.id];
+		prm[p.err_slot] = (unsigned long long)(uintptr_t)q.err;
+		for (size_t c = 0; c < p.cols.size(); c++) {
+			Table& t = e.tables.at(p.cols[c].table);
+			Column* col = t.find(p.cols[c].name);
+			prm[p.col_slots[c]] = (unsigned long long)(uintptr_t)col->dev;
+		}
+	}
+}
+
+static void refresh_column_params(Query& q)
+{
+	for (auto& p : q.plan.pipes) {
+		auto& prm = q.params[p.id];
+		for (size_t c = 0; c < p.cols.size(); c++) {
+			Table& t = q.eng->tables.at(p.cols[c].table);
+			Column* col = t.find(p.cols[c].name);
+			if (!col || !col->dev) {
+				throw Error(1, "column " + p.cols[c].table + "." + p.cols[c].name + " has no data");
+			}
+			prm[p.col_slots[c]] = (unsigned long long)(uintptr_t)col->dev;
+		}
+	}
+}
+
+static void launch_all(Query& q, cudaStream_t stream)
+{
+	QueryState& st = state_of(q);
+	for (auto& m : st.memsets) {
+		VC_CHECK_CUDA(cudaMemsetAsync(m.first, 0, m.second, stream));
+	}
+	const size_t n = q.code.launches.size();
+	if (q.profile && q.ev.size() != 2 * n) {
+		for (auto e : q.ev) {
+			cudaEventDestroy(e);
+		}
+		q.ev.assign(2 * n, nullptr);
+		for (auto& e : q.ev) {
+			VC_CHECK_CUDA(cudaEventCreate(&e));
+		}
+	}
+	for (size_t i = 0; i < n; i++) {
+		const Launch& l = q.code.launches[i];
+		const int occ = st.occupancy[i];
+		int64_t per_sm = q.flavor.grid > 0 ? std::min(q.flavor.grid, occ) : occ;
+		int64_t grid = (int64_t)q.eng->sms * per_sm;
+		if (l.grid_items > 0) {
+			grid = std::min<int64_t>(grid, l.grid_items);
+		}
+		grid = std::max<int64_t>(grid, 1);
+		void* args[] = {q.params[l.pipe].data()};
+		if (q.profile) {
+			VC_CHECK_CUDA(cudaEventRecord(q.ev[2 * i], stream));
+		}
+		VC_CHECK_CUDA(cudaLaunchKernel((const void*)st.kernels[i], dim3((unsigned)grid), dim3((unsigned)l.threads), args,
+			l.smem, stream));
+		if (q.profile) {
+			VC_CHECK_CUDA(cudaEventRecord(q.ev[2 * i + 1], stream));
+		}
+	}
+}
+
+void query_launch(Query& q, cudaStream_t stream)
+{
+	if (q.eng->offline) {
+		throw Error(7, "an offline engine only generates and compiles code");
+	}
+	VC_CHECK_CUDA(cudaSetDevice(q.eng->device));
+	refresh_column_params(q);
+	q.stream = stream;
+	q.result_rows = -1;
+	if (q.flavor.graph && !q.profile) {
+		if (!q.graph) {
+			cudaStream_t cs;
+			VC_CHECK_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+			cudaGraph_t g;
+			VC_CHECK_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+			try {
+				launch_all(q, cs);
+			} catch (...) {
+				cudaStreamEndCapture(cs, &g);
+				cudaStreamDestroy(cs);
+				throw;
+			}
+			VC_CHECK_CUDA(cudaStreamEndCapture(cs, &g));
+			VC_CHECK_CUDA(cudaGraphInstantiate(&q.graph, g, 0));
+			cudaGraphDestroy(g);
+			cudaStreamDestroy(cs);
+		}
+		VC_CHECK_CUDA(cudaGraphLaunch(q.graph, stream));
+	} else {
+		launch_all(q, stream);
+	}
+	VC_CHECK_CUDA(cudaGetLastError());
+	q.ran = true;
+}
+
+void query_fetch(Query& q)
+{
+	if (!q.ran || q.eng->offline) {
+		throw Error(1, "query has not been run");
+	}
+	if (q.result_rows >= 0) {
+		return;
+	}
+	VC_CHECK_CUDA(cudaSetDevice(q.eng->device));
+	VC_CHECK_CUDA(cudaStreamSynchronize(q.stream));
+	unsigned err = 0;
+	unsigned long long cnt = 0;
+	VC_CHECK_CUDA(cudaMemcpy(&err, q.err, sizeof(err), cudaMemcpyDeviceToHost));
+	VC_CHECK_CUDA(cudaMemcpy(&cnt, q.out_count, sizeof(cnt), cudaMemcpyDeviceToHost));
+	if (err & 1u) {
+		throw Error(3, "a device hash table ran out of slots");
+	}
+	if (err & 2u) {
+		throw Error(4, "a bounded device wait gave up");
+	}
+	if (err) {
+		throw Error(3, "device error bits " + std::to_string(err));
+	}
+	if ((int64_t)cnt > q.out_cap) {
+		throw Error(3, "result has more rows than its buffer");
+	}
+	q.result_rows = (int64_t)cnt;
+	if (q.profile) {
+		q.last_ms.assign(q.code.launches.size(), 0.f);
+		for (size_t i = 0; i < q.code.launches.size(); i++) {
+			VC_CHECK_CUDA(cudaEventElapsedTime(&q.last_ms[i], q.ev[2 * i], q.ev[2 * i + 1]));
+		}
+	}
+	const int C = q.plan.result_cols;
+	q.result_host.assign((size_t)C * cnt, 0);
+	for (int c = 0; c < C && cnt > 0; c++) {
+		VC_CHECK_CUDA(cudaMemcpy(q.result_host.data() + (size_t)c * cnt, q.out + (size_t)c * q.out_cap, cnt * 8,
+			cudaMemcpyDeviceToHost));
+	}
+}
+
+std::string query_result_text(Query& q)
+{
+	query_fetch(q);
+	const int C = q.plan.result_cols;
+	const int64_t R = q.result_rows;
+	std::string s;
+	s.reserve((size_t)R * C * 12);
+	char buf[32];
+	for (int64_t r = 0; r < R; r++) {
+		for (int c = 0; c < C; c++) {
+			if (c) {
+				s.push_back('|');
+			}
+			int len = std::snprintf(buf, sizeof(buf), "%" PRId64, q.result_host[(size_t)c * R + r]);
+			s.append(buf, (size_t)len);
+		}
+		s.push_back('\n');
+	}
+	return s;
+}
+
+} // namespace vc
+
+/* ====================================================================== C ABI ======== */
+
+using namespace vc;
+
+struct vc_engine {
+	Engine e;
+};
+struct vc_query {
+	Query q;
+};
+
+template <typename F>
+static int guarded(F&& f)
+{
+	try {
+		f();
+		g_last_error.clear();
+		return VC_OK;
+	} catch (const Error& e) {
+		g_last_error = e.what();
+		return e.code;
+	} catch (const std::bad_alloc&) {
+		g_last_error = "out of host memory";
+		return VC_ERR_INVALID;
+	} catch (const std::exception& e) {
+		g_last_error = e.what();
+		return VC_ERR_INVALID;
+	}
+}
+
+static int copy_out(const std::string& s, char* buf, size_t cap, size_t* len)
+{
+	if (len) {
+		*len = s.size();
+	}
+	if (buf && cap) {
+		size_t n = std::min(cap - 1, s.size());
+		std::memcpy(buf, s.data(), n);
+		buf[n] = 0;
+	}
+	return VC_OK;
+}
+
+static Table& table_of(vc_engine* eng, const char* t)
+{
+	if (!eng || !t) {
+		throw Error(VC_ERR_INVALID, "null engine or table name");
+	}
+	auto it = eng->e.tables.find(t);
+	if (it == eng->e.tables.end()) {
+		throw Error(VC_ERR_INVALID, std::string("unknown table '") + t + "'");
+	}
+	return it->second;
+}
+
+static Column& column_of(vc_engine* eng, const char* t, const char* c)
+{
+	Table& tb = table_of(eng, t);
+	Column* col = c ? tb.find(c) : nullptr;
+	if (!col) {
+		throw Error(VC_ERR_INVALID, std::string("unknown column '") + t + "." + (c ? c : "(null)") + "'");
+	}
+	return *col;
+}
+
+extern "C" {
+
+const char* vc_last_error(void)
+{
+	return g_last_error.c_str();
+}
+
+const char* vc_version(void)
+{
+	return "voila-b200 0.1 (sm_100a)";
+}
+
+int vc_engine_create(int device, vc_engine** out)
+{
+	return guarded([&] {
+		if (!out) {
+			throw Error(VC_ERR_INVALID, "null output");
+		}
+		int n = 0;
+		if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+			cudaGetLastError();
+			throw Error(VC_ERR_NO_DEVICE, "no CUDA device is available");
+		}
+		if (device < 0 || device >= n) {
+			throw Error(VC_ERR_INVALID, "device index out of range");
+		}
+		VC_CHECK_CUDA(cudaSetDevice(device));
+		cudaDeviceProp prop;
+		VC_CHECK_CUDA(cudaGetDeviceProperties(&prop, device));
+		if (prop.major < 10) {
+			throw Error(VC_ERR_NO_DEVICE, "the CUDA flavor is built for sm_100a (B200); device is sm_" +
+				std::to_string(prop.major) + std::to_string(prop.minor));
+		}
+		auto* e = new vc_engine();
+		e->e.device = device;
+		e->e.sms = prop.multiProcessorCount;
+		*out = e;
+	});
+}
+
+int vc_engine_create_offline(int sms, vc_engine** out)
+{
+	return guarded([&] {
+		if (!out || sms < 1) {
+			throw Error(VC_ERR_INVALID, "bad arguments");
+		}
+		auto* e = new vc_engine();
+		e->e.offline = true;
+		e->e.sms = sms;
+		*out = e;
+	});
+}
+
+int vc_engine_destroy(vc_engine* eng)
+{
+	return guarded([&] { delete eng; });
+}
+
+int vc_table_create(vc_engine* eng, const char* table, int64_t rows)
+{
+	return guarded([&] {
+		if (!eng || !table || !*table || rows < 0) {
+			throw Error(VC_ERR_INVALID, "bad table arguments");
+		}
+		std::lock_guard<std::mutex> g(eng->e.mu);
+		if (eng->e.tables.count(table)) {
+			throw Error(VC_ERR_INVALID, std::string("table '") + table + "' exists");
+		}
+		Table t;
+		t.name = table;
+		t.rows = rows;
+		eng->e.tables[table] = t;
+	});
+}
+
+int vc_table_drop(vc_engine* eng, const char* table)
+{
+	return guarded([&] {
+		Table& t = table_of(eng, table);
+		cudaSetDevice(eng->e.device);
+		for (auto& c : t.cols) {
+			if (c.owned && c.dev) {
+				cudaFree(c.dev);
+			}
+		}
+		eng->e.tables.erase(table);
+	});
+}
+
+int vc_column_add(vc_engine* eng, const char* table, const char* column, int type, int64_t lo, int64_t hi)
+{
+	return guarded([&] {
+		Table& t = table_of(eng, table);
+		if (!column || !*column || type < VC_U8 || type > VC_I64 || lo > hi) {
+			throw Error(VC_ERR_INVALID, "bad column arguments");
+		}
+		if (t.find(column)) {
+			throw Error(VC_ERR_INVALID, std::string("column '") + column + "' exists");
+		}
+		const int64_t tmin = type == VC_U8 ? 0 : type == VC_I16 ? INT16_MIN : type == VC_I32 ? INT32_MIN : INT64_MIN;
+		const int64_t tmax = type == VC_U8 ? 255 : type == VC_I16 ? INT16_MAX : type == VC_I32 ? INT32_MAX : INT64_MAX;
+		if (lo < tmin || hi > tmax) {
+			throw Error(VC_ERR_INVALID, "column domain does not fit its type");
+		}
+		Column c;
+		c.name = column;
+		c.type = type;
+		c.lo = lo;
+		c.hi = hi;
+		const size_t bytes = (size_t)std::max<int64_t>(t.rows, 1) * vc_gen_type_size(type);
+		if (eng->e.offline) {
+			c.dev = (void*)eng->e.fake_next;
+			eng->e.fake_next += ((bytes + 255) / 256 + 1) * 256;
+		} else {
+			VC_CHECK_CUDA(cudaSetDevice(eng->e.device));
+			VC_CHECK_CUDA(cudaMalloc(&c.dev, ((bytes + 255) / 256) * 256));
+			c.owned = true;
+		}
+		t.cols.push_back(c);
+	});
+}
+
+int vc_column_upload(vc_engine* eng, const char* table, const char* column, const void* host, int64_t rows,
+	void* stream)
+{
+	return guarded([&] {
+		Table& t = table_of(eng, table);
+		Column& c = column_of(eng, table, column);
+		if (!host || rows != t.rows) {
+			throw Error(VC_ERR_INVALID, "upload must provide exactly the table's rows");
+		}
+		VC_CHECK_CUDA(cudaSetDevice(eng->e.device));
+		if (rows) {
+			VC_CHECK_CUDA(cudaMemcpyAsync(c.dev, host, (size_t)rows * vc_gen_type_size(c.type), cudaMemcpyHostToDevice,
+				(cudaStream_t)stream));
+		}
+	});
+}
+
+int vc_column_download(vc_engine* eng, const char* table, const char* column, void* host, int64_t rows,
+	void* stream)
+{
+	return guarded([&] {
+		Table& t = table_of(eng, table);
+		Column& c = column_of(eng, table, column);
+		if (!host || rows != t.rows) {
+			throw Error(VC_ERR_INVALID, "download must take exactly the table's rows");
+		}
+		VC_CHECK_CUDA(cudaSetDevice(eng->e.device));
+		if (rows) {
+			VC_CHECK_CUDA(cudaMemcpyAsync(host, c.dev, (size_t)rows * vc_gen_type_size(c.type), cudaMemcpyDeviceToHost,
+				(cudaStream_t)stream));
+			VC_CHECK_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+		}
+	});
+}
+
+int vc_column_attach(vc_engine* eng, const char* table, const char* column, void* device_ptr)
+{
+	return guarded([&] {
+		Column& c = column_of(eng, table, column);
+		if (!device_ptr || ((uintptr_t)device_ptr & 15u)) {
+			throw Error(VC_ERR_INVALID, "attached column memory must be non-null and 16-byte aligned");
+		}
+		VC_CHECK_CUDA(cudaSetDevice(eng->e.device));
+		if (c.owned && c.dev) {
+			VC_CHECK_CUDA(cudaFree(c.dev));
+		}
+		c.dev = device_ptr;
+		c.owned = false;
+	});
+}
+
+int vc_column_device_ptr(vc_engine* eng, const char* table, const char* column, void** out)
+{
+	return guarded([&] {
+		Column& c = column_of(eng, table, column);
+		if (!out) {
+			throw Error(VC_ERR_INVALID, "null output");
+		}
+		*out = c.dev;
+	});
+}
+
+int vc_column_generate(vc_engine* eng, const char* table, const char* column, int32_t kind, int64_t a, int64_t b,
+	int64_t c, double s, uint64_t seed, const double* zipf_cdf, void* stream)
+{
+	return guarded([&] {
+		Table& t = table_of(eng, table);
+		Column& col = column_of(eng, table, column);
+		vc_gen_spec spec;
+		spec.kind = kind;
+		spec.type = col.type;
+		spec.a = a;
+		spec.b = b;
+		spec.c = c;
+		spec.s = s;
+		spec.seed = seed;
+		spec.n = t.rows;
+		if (kind < VC_GEN_UNIFORM || kind > VC_GEN_MOD) {
+			throw Error(VC_ERR_INVALID, "unknown generator kind");
+		}
+		if ((kind == VC_GEN_DIV || kind == VC_GEN_MOD) && b <= 0) {
+			throw Error(VC_ERR_INVALID, "generator divisor must be positive");
+		}
+		if (kind == VC_GEN_UNIFORM && (b < a || (uint64_t)(b - a) >= (1ull << 32))) {
+			throw Error(VC_ERR_INVALID, "uniform range must be non-empty and below 2^32");
+		}
+		const bool skew = kind == VC_GEN_ZIPF && s != 0.0;
+		if (skew && (!zipf_cdf || b < 1)) {
+			throw Error(VC_ERR_INVALID, "skewed Zipf generation needs the CDF table");
+		}
+		VC_CHECK_CUDA(cudaSetDevice(eng->e.device));
+		double* dcdf = nullptr;
+		if (skew) {
+			VC_CHECK_CUDA(cudaMalloc(&dcdf, (size_t)b * sizeof(double)));
+			VC_CHECK_CUDA(cudaMemcpyAsync(dcdf, zipf_cdf, (size_t)b * sizeof(double), cudaMemcpyHostToDevice,
+				(cudaStream_t)stream));
+		}
+		cudaError_t rc = launch_generate(col.dev, spec, dcdf, t.rows, (cudaStream_t)stream);
+		if (dcdf) {
+			cudaStreamSynchronize((cudaStream_t)stream);
+			cudaFree(dcdf);
+		}
+		VC_CHECK_CUDA(rc);
+	});
+}
+
+int vc_gen_host(int32_t kind, int32_t type, int64_t a, int64_t b, int64_t c, double s, uint64_t seed, int64_t n,
+	const double* zipf_cdf, int64_t begin, int64_t count, void* out)
+{
+	return guarded([&] {
+		if (!out || count < 0 || begin < 0 || type < VC_U8 || type > VC_I64) {
+			throw Error(VC_ERR_INVALID, "bad generator arguments");
+		}
+		vc_gen_spec spec{kind, type, a, b, c, s, seed, n};
+		for (int64_t i = 0; i < count; i++) {
+			vc_gen_store(type, out, i, vc_gen_value(&spec, zipf_cdf, begin + i));
+		}
+	});
+}
+
+int vc_gen_zipf_cdf(double s, int64_t n, double* out)
+{
+	return guarded([&] {
+		if (!out || n < 1) {
+			throw Error(VC_ERR_INVALID, "bad zipf arguments");
+		}
+		vc_gen_build_zipf_cdf(s, n, out);
+	});
+}
+
+int vc_workload_describe(const char* spec, char* buf, size_t cap, size_t* len)
+{
+	return guarded([&] {
+		if (!spec) {
+			throw Error(VC_ERR_INVALID, "null spec");
+		}
+		std::string d;
+		try {
+			d = vc_workload::describe(vc_workload::make(spec));
+		} catch (const std::invalid_argument& e) {
+			throw Error(VC_ERR_INVALID, e.what());
+		}
+		copy_out(d, buf, cap, len);
+	});
+}
+
+int vc_workload_batch(int count, uint64_t seed, int64_t min_rows, int64_t max_rows, char* buf, size_t cap,
+	size_t* len)
+{
+	return guarded([&] {
+		if (count < 0 || min_rows < 1 || max_rows < min_rows) {
+			throw Error(VC_ERR_INVALID, "bad batch arguments");
+		}
+		std::string s;
+		for (auto& w : vc_workload::make_batch(count, seed, min_rows, max_rows)) {
+			s += w + "\n";
+		}
+		copy_out(s, buf, cap, len);
+	});
+}
+
+int vc_query_new(vc_engine* eng, const char* plan, const char* flavor, vc_query** out)
+{
+	vc_query* q = nullptr;
+	int rc = guarded([&] {
+		if (!eng || !plan || !out) {
+			throw Error(VC_ERR_INVALID, "null argument");
+		}
+		q = new vc_query();
+		q->q.eng = &eng->e;
+		q->q.plan_text = plan;
+		q->q.flavor = Flavor::parse(flavor ? flavor : "");
+		query_prepare(q->q);
+		*out = q;
+	});
+	if (rc != VC_OK && q) {
+		std::string msg = g_last_error;
+		{
+			std::lock_guard<std::mutex> g(g_state_mu);
+			g_state.erase(&q->q);
+		}
+		delete q;
+		g_last_error = msg;
+	}
+	return rc;
+}
+
+int vc_query_run(vc_query* q, void* stream)
+{
+	return guarded([&] {
+		if (!q) {
+			throw Error(VC_ERR_INVALID, "null query");
+		}
+		query_launch(q->q, (cudaStream_t)stream);
+	});
+}
+
+int vc_query_reset(vc_query* q)
+{
+	return guarded([&] {
+		if (!q) {
+			throw Error(VC_ERR_INVALID, "null query");
+		}
+		q->q.result_rows = -1;
+		q->q.result_host.clear();
+	});
+}
+
+int vc_query_free(vc_query* q)
+{
+	return guarded([&] {
+		if (q) {
+			{
+				std::lock_guard<std::mutex> g(g_state_mu);
+				g_state.erase(&q->q);
+			}
+			delete q;
+		}
+	});
+}
+
+int vc_query_result_shape(vc_query* q, int64_t* rows, int32_t* cols)
+{
+	return guarded([&] {
+		if (!q) {
+			throw Error(VC_ERR_INVALID, "null query");
+		}
+		query_fetch(q->q);
+		if (rows) {
+			*rows = q->q.result_rows;
+		}
+		if (cols) {
+			*cols = q->q.plan.result_cols;
+		}
+	});
+}
+
+int vc_query_result_copy(vc_query* q, int64_t* out, int64_t cap)
+{
+	return guarded([&] {
+		if (!q || !out) {
+			throw Error(VC_ERR_INVALID, "null argument");
+		}
+		query_fetch(q->q);
+		const size_t n = q->q.result_host.size();
+		if ((int64_t)n > cap) {
+			throw Error(VC_ERR_INVALID, "result buffer too small");
+		}
+		std::memcpy(out, q->q.result_host.data(), n * 8);
+	});
+}
+
+int vc_query_result_text(vc_query* q, char* buf, size_t cap, size_t* len)
+{
+	return guarded([&] {
+		if (!q) {
+			throw Error(VC_ERR_INVALID, "null query");
+		}
+		copy_out(query_result_text(q->q), buf, cap, len);
+	});
+}
+
+int vc_query_info(vc_query* q, char* buf, size_t cap, size_t* len)
+{
+	return guarded([&] {
+		if (!q) {
+			throw Error(VC_ERR_INVALID, "null query");
+		}
+		Query& qq = q->q;
+		std::ostringstream o;
+		static const char* sinks[] = {"join_build", "aggr_global", "aggr_dense", "aggr_hash", "emit"};
+		o << "{\"flavor\": \"" << qq.flavor.str() << "\", \"result_cols\": " << qq.plan.result_cols
+		  << ", \"source_bytes\": " << qq.code.source.size() << ", \"pipelines\": [";
+		for (size_t i = 0; i < qq.plan.pipes.size(); i++) {
+			auto& p = qq.plan.pipes[i];
+			int64_t bytes = 0;
+			for (auto& c : p.cols) {
+				bytes += p.rows * vc_gen_type_size(c.type);
+			}
+			o << (i ? ", " : "") << "{\"table\": \"" << p.table << "\", \"rows\": " << p.rows << ", \"columns\": "
+			  << p.cols.size() << ", \"ops\": " << p.ops.size() << ", \"sink\": \"" << sinks[p.sink.kind]
+			  << "\", \"scan_bytes\": " << bytes << ", \"result\": " << (p.id == qq.plan.result_pipe ? "true" : "false")
+			  << "}";
+		}
+		o << "], \"kernels\": [";
+		for (size_t i = 0; i < qq.code.launches.size(); i++) {
+			auto& l = qq.code.launches[i];
+			o << (i ? ", " : "") << "{\"name\": \"" << l.kernel << "\", \"pipeline\": " << l.pipe << ", \"smem\": "
+			  << l.smem << ", \"threads\": " << l.threads << ", \"dominant\": " << (l.dominant ? "true" : "false") << "}";
+		}
+		o << "]}";
+		copy_out(o.str(), buf, cap, len);
+	});
+}
+
+int vc_query_source(vc_query* q, char* buf, size_t cap, size_t* len)
+{
+	return guarded([&] {
+		if (!q) {
+			throw Error(VC_ERR_INVALID, "null query");
+		}
+		copy_out(q->q.code.source, buf, cap, len);
+	});
+}
+
+int vc_query_profile(vc_query* q, int enable)
+{
+	return guarded([&] {
+		if (!q) {
+			throw Error(VC_ERR_INVALID, "null query");
+		}
+		q->q.profile = enable != 0;
+	});
+}
+
+int vc_query_timings(vc_query* q, float* ms, int cap, int* n, char* names, size_t names_cap)
+{
+	return guarded([&] {
+		if (!q) {
+			throw Error(VC_ERR_INVALID, "null query");
+		}
+		query_fetch(q->q);
+		const auto& t = q->q.last_ms;
+		if (n) {
+			*n = (int)t.size();
+		}
+		for (int i = 0; i < (int)t.size() && i < cap && ms; i++) {
+			ms[i] = t[i];
+		}
+		std::string s;
+		for (auto& l : q->q.code.launches) {
+			s += l.kernel + "\n";
+		}
+		copy_out(s, names, names_cap, nullptr);
+	});
+}
+
+} // extern "C"

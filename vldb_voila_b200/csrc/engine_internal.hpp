@@ -1,0 +1,284 @@
+/*
+ * Host-side internals of the CUDA flavor: the relational plan mirror, the lowered
+ * pipelines, the kernel generator's output and the runtime objects behind the C ABI.
+ */
+#ifndef VOILA_B200_ENGINE_INTERNAL_HPP
+#define VOILA_B200_ENGINE_INTERNAL_HPP
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "datagen.h"
+#include "sexpr.hpp"
+
+namespace vc {
+
+/* An error that maps to a C ABI status code. */
+struct Error : std::runtime_error {
+	int code;
+	Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define VC_CHECK_CUDA(call)                                                                       \
+	do {                                                                                          \
+		cudaError_t _e = (call);                                                                  \
+		if (_e != cudaSuccess) {                                                                  \
+			throw ::vc::Error(2 /* VC_ERR_CUDA */, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+		}                                                                                         \
+	} while (0)
+
+/* ------------------------------------------------------------------ relational plan ---- */
+
+/* Mirror of the reference's relalg expressions (relalg.hpp:12-74). */
+struct RelExpr {
+	enum Kind { Const, ColId, Fun, Assign } kind;
+	std::string text;                         /* constant literal, column id, function or assign name */
+	std::vector<std::shared_ptr<RelExpr>> args;
+};
+using RelExprP = std::shared_ptr<RelExpr>;
+
+/* Mirror of the reference's relalg operators (relalg.hpp:76-172). */
+struct RelOp {
+	enum Kind { Scan, Select, Project, HashAggr, HashJoin } kind;
+	std::string table;                        /* Scan */
+	std::vector<std::string> columns;         /* Scan */
+	RelExprP predicate;                       /* Select */
+	std::vector<RelExprP> exprs;              /* Project: projections; HashAggr: keys */
+	std::vector<RelExprP> aggregates;         /* HashAggr */
+	bool global = false;                      /* HashAggr::Global */
+	bool join01 = true;                       /* HashJoin::Join01 (else JoinN) */
+	std::vector<RelExprP> left_keys, left_payl, right_keys, right_payl;
+	std::shared_ptr<RelOp> left, right;       /* child / probe side, build side */
+};
+using RelOpP = std::shared_ptr<RelOp>;
+
+RelOpP parse_plan(const std::string& text);
+
+/* ------------------------------------------------------------------ database ----------- */
+
+struct Column {
+	std::string name;
+	int type = VC_TYPE_I32;
+	int64_t lo = 0, hi = 0;   /* declared domain (the reference's MinMaxInfo) */
+	void* dev = nullptr;      /* device data */
+	bool owned = false;
+};
+
+struct Table {
+	std::string name;
+	int64_t rows = 0;
+	std::vector<Column> cols;
+	Column* find(const std::string& c) {
+		for (auto& x : cols) {
+			if (x.name == c) {
+				return &x;
+			}
+		}
+		return nullptr;
+	}
+};
+
+/* ------------------------------------------------------------------ lowered pipelines -- */
+
+struct Bounds {
+	__int128 lo = 0, hi = 0;
+};
+
+struct BExpr;
+using BExprP = std::shared_ptr<BExpr>;
+
+struct BExpr {
+	enum Kind { Col, Const, ProbeOut, Fun } kind;
+	int col = -1;              /* Col: index into Pipeline::cols */
+	int64_t cval = 0;          /* Const */
+	int param = -1;            /* Const: parameter slot */
+	int probe = -1, pidx = -1; /* ProbeOut: op index, payload index */
+	std::string fn;            /* Fun: lt le gt ge eq ne and or add sub mul */
+	std::vector<BExprP> args;
+	Bounds b;
+	bool boolean = false;
+};
+
+struct JoinDesc {
+	int id = 0;
+	std::string build_table;
+	int64_t build_rows = 0;          /* upper bound of inserted rows */
+	std::vector<Bounds> key_b, pay_b;
+	std::vector<int> key_shift, pay_shift;
+	int key_bits = 0, pay_bits = 0;
+	bool key64 = false, pay64 = false;
+	bool join01 = true;
+	/* device state */
+	void* table = nullptr;           /* JoinSlot array, capacity for build_rows */
+	void* stage_keys = nullptr;      /* materialised packed keys */
+	void* stage_pay = nullptr;       /* materialised packed payloads */
+	unsigned long long* words = nullptr; /* [0] materialised count, [1] bucket mask */
+	int64_t max_buckets = 0;
+	int slot_bytes() const { return (key64 || pay64) ? 16 : 8; }
+};
+
+struct Op {
+	enum Kind { Filter, Probe } kind;
+	BExprP pred;                 /* Filter */
+	int join = -1;               /* Probe: index into LoweredPlan::joins */
+	std::vector<BExprP> keys;    /* Probe keys */
+	int npay = 0;                /* Probe: payload outputs */
+};
+
+struct Sink {
+	enum Kind { JoinBuild, AggGlobal, AggDense, AggHash, Emit } kind;
+	int join = -1;
+	std::vector<BExprP> keys;    /* build keys / group keys */
+	std::vector<BExprP> pay;     /* build payloads */
+	struct Agg {
+		bool count = false;
+		BExprP arg;
+		bool visible = true;
+	};
+	std::vector<Agg> aggs;       /* group/global aggregates (+ hidden count) */
+	int count_idx = -1;
+	std::vector<BExprP> outs;    /* Emit columns */
+	/* group key packing */
+	std::vector<int> key_shift;
+	std::vector<int64_t> key_radix;
+	int key_bits = 0;
+	__int128 domain = 0;         /* product of key ranges */
+	int64_t groups_bound = 0;    /* upper bound of distinct groups */
+};
+
+struct PipeColumn {
+	std::string table, name;
+	int type;
+	int64_t lo, hi;
+};
+
+struct Pipeline {
+	int id = 0;
+	std::string table;
+	int64_t rows = 0;
+	std::vector<PipeColumn> cols;
+	std::vector<Op> ops;
+	Sink sink;
+	int err_slot = -1;           /* parameter slot of the device error word */
+	std::vector<int> col_slots;  /* parameter slots of the column pointers */
+};
+
+/* the tunable knobs of one CUDA flavor (the computation_type=cuda(...) blend) */
+struct Flavor {
+	int threads = 256;        /* threads per CTA */
+	int rows = 4;             /* consecutive rows per thread and tile step */
+	std::string aggr = "auto";/* auto | dense | global | cache */
+	int cache_slots = 1024;   /* shared-memory group cache (aggr=cache) */
+	int bucket = 32;          /* join bucket bytes: 32 (sector) or the slot size */
+	int grid = 0;             /* CTAs per SM (0 = occupancy) */
+	int dense_limit = 4096;   /* largest dense key domain */
+	bool graph = false;       /* replay the query's launches from a CUDA graph */
+
+	std::string str() const;
+	static Flavor parse(const std::string& s);
+};
+
+struct LoweredPlan {
+	std::vector<Pipeline> pipes;
+	std::vector<JoinDesc> joins;
+	int result_pipe = -1;
+	int result_cols = 0;
+};
+
+LoweredPlan lower_plan(const RelOpP& root, std::map<std::string, Table>& tables, const Flavor& fl);
+
+/* ------------------------------------------------------------------ generated code ----- */
+
+struct Launch {
+	enum Kind { Kernel, MemsetZero } kind = Kernel;
+	std::string kernel;
+	int pipe = -1;
+	int stage = 0;               /* which kernel of the pipeline */
+	size_t smem = 0;
+	int threads = 256;
+	int64_t grid_items = 0;      /* work items that bound the grid (0 = persistent over SMs) */
+	bool dominant = false;       /* the fact pipeline's main kernel */
+	void** memset_ptr = nullptr; /* MemsetZero */
+	size_t memset_bytes = 0;
+};
+
+struct GeneratedCode {
+	std::string source;
+	std::vector<Launch> launches;
+};
+
+/* device state of one pipeline's sink, allocated before code generation */
+struct PipeDeviceState {
+	void* sink_dev = nullptr;
+	int64_t sink_cap = 0;
+	size_t sink_bytes = 0;
+	void* stage_hash = nullptr;
+};
+
+GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<PipeDeviceState>& st, void* out,
+	int64_t out_cap, unsigned long long* out_count, std::vector<std::vector<unsigned long long>>& params);
+
+/* ------------------------------------------------------------------ JIT ---------------- */
+
+struct JitModule {
+	cudaLibrary_t lib = nullptr;
+	std::map<std::string, cudaKernel_t> kernels;
+};
+
+std::shared_ptr<JitModule> jit_compile(const std::string& source, std::string* log_out);
+std::string jit_cubin(const std::string& source, std::string* log_out);
+const std::string& device_header_source();
+
+/* ------------------------------------------------------------------ engine ------------- */
+
+struct Engine {
+	int device = 0;
+	int sms = 0;
+	bool offline = false;       /* code generation and compilation only, no device */
+	uintptr_t fake_next = 0x100000;
+	std::map<std::string, Table> tables;
+	std::mutex mu;
+	~Engine();
+};
+
+struct Query {
+	Engine* eng = nullptr;
+	std::string plan_text;
+	Flavor flavor;
+	LoweredPlan plan;
+	GeneratedCode code;
+	std::shared_ptr<JitModule> mod;
+	std::vector<void*> allocations;
+	unsigned* err = nullptr;             /* device error word */
+	unsigned long long* out_count = nullptr;
+	int64_t* out = nullptr;              /* result_cols x out_cap, column-major */
+	int64_t out_cap = 0;
+	std::vector<std::vector<unsigned long long>> params; /* per pipeline */
+	cudaStream_t stream = nullptr;
+	bool profile = false;
+	std::vector<cudaEvent_t> ev;         /* per launch begin/end when profiling */
+	std::vector<float> last_ms;
+	cudaGraphExec_t graph = nullptr;
+	cudaStream_t graph_stream = nullptr;
+	bool ran = false;
+	int64_t result_rows = -1;
+	std::vector<int64_t> result_host;    /* column-major copy of the last result */
+	~Query();
+};
+
+void query_prepare(Query& q);
+void query_launch(Query& q, cudaStream_t stream);
+void query_fetch(Query& q);
+std::string query_result_text(Query& q);
+
+} // namespace vc
+
+#endif

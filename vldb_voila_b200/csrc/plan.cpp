@@ -1,0 +1,591 @@
+/*
+ * Plan text -> relational plan mirror -> lowered pipelines.
+ *
+ * The lowering follows the pipeline structure the reference's RelOpTranslator produces
+ * (relalg_translator.cpp:169-1124), re-expressed for fused GPU pipelines:
+ *   - Scan opens a pipeline over a base table (relalg_translator.cpp:202-272);
+ *   - Select adds a filter (seltrue + emit, :343-378);
+ *   - Project replaces the visible columns; later assignments may use earlier ones
+ *     (:275-341, expr_cache);
+ *   - HashJoin closes the build side's pipeline with a table-build sink (materialize +
+ *     bucket_build, :828-931) and appends a probe to the probe side's pipeline; after it the
+ *     visible columns are the probe side's, then the build keys (taking the probe key values,
+ *     :965-975) and the build payloads (:1000-1012).  Join01 stops at the first match
+ *     (:1032-1042);
+ *   - HashAggr ends the pipeline with a group-by or global aggregation; a count is added
+ *     when the plan has none (:469-472) and result rows are the groups whose count is > 0
+ *     (:692-701).
+ *
+ * Typing: like the reference's typing pass (typing_pass.cpp:9-23, :164-176, :244-259) every
+ * value carries an exact [lo, hi] range derived from the columns' declared min/max.  Here
+ * all arithmetic runs in int64 and a plan whose ranges (or sums, bounded by the row count)
+ * could leave int64 is rejected instead of being widened to 128 bits.
+ */
+#include <algorithm>
+#include <climits>
+
+#include "engine_internal.hpp"
+
+namespace vc {
+
+static const int kErrInvalid = 1;
+static const int kErrUnsupported = 6;
+
+/* ------------------------------------------------------------------ plan text ---------- */
+
+static RelExprP parse_expr(const vc_sexpr::Node& n)
+{
+	auto e = std::make_shared<RelExpr>();
+	const std::string& h = n.head();
+	if (h == "const") {
+		e->kind = RelExpr::Const;
+		e->text = n.atom_text(1);
+	} else if (h == "col") {
+		e->kind = RelExpr::ColId;
+		e->text = n.atom_text(1);
+	} else if (h == "assign") {
+		e->kind = RelExpr::Assign;
+		e->text = n.atom_text(1);
+		e->args.push_back(parse_expr(n.at(2)));
+	} else if (h == "fun") {
+		e->kind = RelExpr::Fun;
+		e->text = n.atom_text(1);
+		for (size_t i = 2; i < n.kids.size(); i++) {
+			e->args.push_back(parse_expr(n.kids[i]));
+		}
+	} else {
+		throw Error(kErrInvalid, "plan: unknown expression '" + h + "'");
+	}
+	return e;
+}
+
+static std::vector<RelExprP> parse_expr_list(const vc_sexpr::Node& n)
+{
+	if (n.atom) {
+		throw Error(kErrInvalid, "plan: expected an expression list, got '" + n.text + "'");
+	}
+	std::vector<RelExprP> r;
+	for (auto& k : n.kids) {
+		r.push_back(parse_expr(k));
+	}
+	return r;
+}
+
+static RelOpP parse_op(const vc_sexpr::Node& n)
+{
+	auto op = std::make_shared<RelOp>();
+	const std::string& h = n.head();
+	if (h == "scan") {
+		op->kind = RelOp::Scan;
+		op->table = n.atom_text(1);
+		const auto& cols = n.at(2);
+		if (cols.atom) {
+			throw Error(kErrInvalid, "plan: scan expects a column list");
+		}
+		for (auto& c : cols.kids) {
+			if (!c.atom) {
+				throw Error(kErrInvalid, "plan: scan columns must be names");
+			}
+			op->columns.push_back(c.text);
+		}
+	} else if (h == "select") {
+		op->kind = RelOp::Select;
+		op->predicate = parse_expr(n.at(1));
+		op->left = parse_op(n.at(2));
+	} else if (h == "project") {
+		op->kind = RelOp::Project;
+		op->exprs = parse_expr_list(n.at(1));
+		op->left = parse_op(n.at(2));
+	} else if (h == "aggr") {
+		op->kind = RelOp::HashAggr;
+		const std::string& v = n.atom_text(1);
+		if (v != "hash" && v != "global") {
+			throw Error(kErrInvalid, "plan: aggr variant must be hash or global");
+		}
+		op->global = v == "global";
+		op->exprs = parse_expr_list(n.at(2));
+		op->aggregates = parse_expr_list(n.at(3));
+		op->left = parse_op(n.at(4));
+	} else if (h == "join") {
+		op->kind = RelOp::HashJoin;
+		const std::string& v = n.atom_text(1);
+		if (v != "join01" && v != "joinN") {
+			throw Error(kErrInvalid, "plan: join variant must be join01 or joinN");
+		}
+		op->join01 = v == "join01";
+		op->left_keys = parse_expr_list(n.at(2));
+		op->left_payl = parse_expr_list(n.at(3));
+		op->left = parse_op(n.at(4));
+		op->right_keys = parse_expr_list(n.at(5));
+		op->right_payl = parse_expr_list(n.at(6));
+		op->right = parse_op(n.at(7));
+		if (op->left_keys.empty() || op->left_keys.size() != op->right_keys.size()) {
+			throw Error(kErrInvalid, "plan: join needs the same non-zero number of probe and build keys");
+		}
+	} else {
+		throw Error(kErrInvalid, "plan: unknown operator '" + h + "'");
+	}
+	return op;
+}
+
+RelOpP parse_plan(const std::string& text)
+{
+	try {
+		return parse_op(vc_sexpr::parse(text));
+	} catch (const Error&) {
+		throw;
+	} catch (const std::exception& e) {
+		throw Error(kErrInvalid, e.what());
+	}
+}
+
+/* ------------------------------------------------------------------ bounds ------------- */
+
+static const __int128 kI64Max = (__int128)INT64_MAX;
+static const __int128 kI64Min = (__int128)INT64_MIN;
+
+static void check_range(const Bounds& b, const std::string& what)
+{
+	if (b.lo < kI64Min || b.hi > kI64Max) {
+		throw Error(kErrUnsupported, "value range of " + what + " exceeds int64; the CUDA flavor keeps "
+			"every value and sum an exact int64");
+	}
+}
+
+static int bits_for(__int128 range)
+{
+	/* bits needed to store values 0 .. range-1 */
+	int b = 0;
+	while (b < 127 && ((__int128)1 << b) < range) {
+		b++;
+	}
+	return b;
+}
+
+/* ------------------------------------------------------------------ lowering ----------- */
+
+namespace {
+
+struct ScopeEntry {
+	std::string name;
+	BExprP e;
+	std::string table, column; /* unresolved base column */
+};
+
+struct Scope {
+	std::vector<ScopeEntry> cols;
+	ScopeEntry* find(const std::string& n) {
+		for (auto it = cols.rbegin(); it != cols.rend(); ++it) {
+			if (it->name == n) {
+				return &*it;
+			}
+		}
+		return nullptr;
+	}
+};
+
+struct Lowerer {
+	std::map<std::string, Table>& tables;
+	const Flavor& fl;
+	LoweredPlan out;
+
+	Lowerer(std::map<std::string, Table>& t, const Flavor& f) : tables(t), fl(f) {}
+
+	Table& table(const std::string& n) {
+		auto it = tables.find(n);
+		if (it == tables.end()) {
+			throw Error(kErrInvalid, "unknown table '" + n + "'");
+		}
+		return it->second;
+	}
+
+	BExprP resolve(ScopeEntry& s, Pipeline& p) {
+		if (s.e) {
+			return s.e;
+		}
+		Table& t = table(s.table);
+		Column* c = t.find(s.column);
+		if (!c) {
+			throw Error(kErrInvalid, "unknown column '" + s.table + "." + s.column + "'");
+		}
+		auto e = std::make_shared<BExpr>();
+		e->kind = BExpr::Col;
+		e->col = -1;
+		for (size_t i = 0; i < p.cols.size(); i++) {
+			if (p.cols[i].table == s.table && p.cols[i].name == s.column) {
+				e->col = (int)i;
+			}
+		}
+		if (e->col < 0) {
+			e->col = (int)p.cols.size();
+			p.cols.push_back(PipeColumn{s.table, s.column, c->type, c->lo, c->hi});
+		}
+		e->b.lo = c->lo;
+		e->b.hi = c->hi;
+		s.e = e;
+		return e;
+	}
+
+	BExprP bind(const RelExprP& re, Scope& sc, Pipeline& p) {
+		switch (re->kind) {
+		case RelExpr::Const: {
+			auto e = std::make_shared<BExpr>();
+			e->kind = BExpr::Const;
+			try {
+				size_t used = 0;
+				e->cval = std::stoll(re->text, &used);
+				if (used != re->text.size()) {
+					throw std::invalid_argument("trailing");
+				}
+			} catch (const std::exception&) {
+				throw Error(kErrUnsupported, "constant '" + re->text + "' is not an int64 literal");
+			}
+			e->b.lo = e->b.hi = e->cval;
+			return e;
+		}
+		case RelExpr::ColId: {
+			ScopeEntry* s = sc.find(re->text);
+			if (!s) {
+				throw Error(kErrInvalid, "cannot find '" + re->text + "' among the visible columns");
+			}
+			return resolve(*s, p);
+		}
+		case RelExpr::Assign:
+			throw Error(kErrInvalid, "assign is only allowed in a projection list");
+		case RelExpr::Fun:
+			break;
+		}
+		static const std::map<std::string, std::string> names = {
+			{"<=", "le"}, {"<", "lt"}, {">=", "ge"}, {">", "gt"}, {"=", "eq"}, {"!=", "ne"},
+			{"+", "add"}, {"-", "sub"}, {"*", "mul"},
+			{"le", "le"}, {"lt", "lt"}, {"ge", "ge"}, {"gt", "gt"}, {"eq", "eq"}, {"ne", "ne"},
+			{"add", "add"}, {"sub", "sub"}, {"mul", "mul"}, {"and", "and"}, {"or", "or"}};
+		auto it = names.find(re->text);
+		if (it == names.end()) {
+			throw Error(kErrUnsupported, "function '" + re->text + "' is not supported by the CUDA flavor");
+		}
+		auto e = std::make_shared<BExpr>();
+		e->kind = BExpr::Fun;
+		e->fn = it->second;
+		for (auto& a : re->args) {
+			e->args.push_back(bind(a, sc, p));
+		}
+		if (e->args.size() != 2) {
+			throw Error(kErrInvalid, "function '" + re->text + "' takes two arguments");
+		}
+		const Bounds& a = e->args[0]->b;
+		const Bounds& b = e->args[1]->b;
+		if (e->fn == "add") {
+			e->b.lo = a.lo + b.lo;
+			e->b.hi = a.hi + b.hi;
+		} else if (e->fn == "sub") {
+			e->b.lo = a.lo - b.hi;
+			e->b.hi = a.hi - b.lo;
+		} else if (e->fn == "mul") {
+			__int128 c[4] = {a.lo * b.lo, a.lo * b.hi, a.hi * b.lo, a.hi * b.hi};
+			e->b.lo = *std::min_element(c, c + 4);
+			e->b.hi = *std::max_element(c, c + 4);
+		} else {
+			e->boolean = true;
+			e->b.lo = 0;
+			e->b.hi = 1;
+			if ((e->fn == "and" || e->fn == "or") && !(e->args[0]->boolean && e->args[1]->boolean)) {
+				throw Error(kErrInvalid, "'" + re->text + "' needs two predicates");
+			}
+		}
+		if (!e->boolean && (e->args[0]->boolean || e->args[1]->boolean)) {
+			throw Error(kErrUnsupported, "arithmetic on predicates is not supported");
+		}
+		check_range(e->b, "'" + re->text + "'");
+		return e;
+	}
+
+	/* Returns the index of the still-open pipeline that produces op's rows. */
+	int lower(const RelOpP& op, Scope& sc) {
+		switch (op->kind) {
+		case RelOp::Scan: {
+			Table& t = table(op->table);
+			Pipeline p;
+			p.id = (int)out.pipes.size();
+			p.table = op->table;
+			p.rows = t.rows;
+			sc.cols.clear();
+			for (auto& c : op->columns) {
+				if (!t.find(c)) {
+					throw Error(kErrInvalid, "unknown column '" + op->table + "." + c + "'");
+				}
+				sc.cols.push_back(ScopeEntry{op->table + "." + c, nullptr, op->table, c});
+			}
+			p.sink.kind = Sink::Emit;
+			out.pipes.push_back(p);
+			return p.id;
+		}
+		case RelOp::Select: {
+			int pi = lower(op->left, sc);
+			BExprP pred = bind(op->predicate, sc, out.pipes[pi]);
+			if (!pred->boolean) {
+				throw Error(kErrInvalid, "select predicate is not a comparison");
+			}
+			Op f;
+			f.kind = Op::Filter;
+			f.pred = pred;
+			out.pipes[pi].ops.push_back(f);
+			return pi;
+		}
+		case RelOp::Project: {
+			int pi = lower(op->left, sc);
+			Scope ns;
+			Scope lookup = sc; /* earlier assignments become visible to later ones */
+			for (auto& pe : op->exprs) {
+				if (pe->kind == RelExpr::Assign) {
+					BExprP e = bind(pe->args[0], lookup, out.pipes[pi]);
+					ns.cols.push_back(ScopeEntry{pe->text, e, "", ""});
+					lookup.cols.push_back(ScopeEntry{pe->text, e, "", ""});
+				} else if (pe->kind == RelExpr::ColId) {
+					ScopeEntry* s = lookup.find(pe->text);
+					if (!s) {
+						throw Error(kErrInvalid, "cannot find '" + pe->text + "' among the visible columns");
+					}
+					ns.cols.push_back(*s);
+					ns.cols.back().name = pe->text;
+				} else {
+					throw Error(kErrInvalid, "projection entries must be columns or assignments");
+				}
+			}
+			/* unresolved base columns stay lazily resolvable through the copied entries
+			 * (resolve() shares one column slot per base column) */
+			sc = ns;
+			return pi;
+		}
+		case RelOp::HashJoin: {
+			/* build side first: its pipeline must run before the probe */
+			Scope bs;
+			int bi = lower(op->right, bs);
+			JoinDesc jd;
+			jd.id = (int)out.joins.size();
+			jd.join01 = op->join01;
+			jd.build_table = out.pipes[bi].table;
+			jd.build_rows = rows_bound(out.pipes[bi]);
+			Sink sink;
+			sink.kind = Sink::JoinBuild;
+			sink.join = jd.id;
+			int shift = 0;
+			for (auto& k : op->right_keys) {
+				BExprP e = bind(k, bs, out.pipes[bi]);
+				if (e->boolean) {
+					throw Error(kErrUnsupported, "join keys must be values");
+				}
+				sink.keys.push_back(e);
+				jd.key_b.push_back(e->b);
+				jd.key_shift.push_back(shift);
+				shift += bits_for(e->b.hi - e->b.lo + 1);
+			}
+			jd.key_bits = shift;
+			if (jd.key_bits > 62) {
+				throw Error(kErrUnsupported, "join key domain needs more than 62 bits");
+			}
+			jd.key64 = jd.key_bits > 31;
+			shift = 0;
+			for (auto& pe : op->right_payl) {
+				BExprP e = bind(pe, bs, out.pipes[bi]);
+				if (e->boolean) {
+					throw Error(kErrUnsupported, "join payloads must be values");
+				}
+				sink.pay.push_back(e);
+				jd.pay_b.push_back(e->b);
+				jd.pay_shift.push_back(shift);
+				shift += bits_for(e->b.hi - e->b.lo + 1);
+			}
+			jd.pay_bits = shift;
+			if (jd.pay_bits > 64) {
+				throw Error(kErrUnsupported, "join payload needs more than 64 bits");
+			}
+			jd.pay64 = jd.pay_bits > 32;
+			if (out.pipes[bi].sink.kind != Sink::Emit) {
+				throw Error(kErrUnsupported, "the build side of a join must be a scan/select/project/join chain");
+			}
+			out.pipes[bi].sink = sink;
+			out.joins.push_back(jd);
+
+			int pi = lower(op->left, sc);
+			Op pr;
+			pr.kind = Op::Probe;
+			pr.join = jd.id;
+			for (auto& k : op->left_keys) {
+				BExprP e = bind(k, sc, out.pipes[pi]);
+				if (e->boolean) {
+					throw Error(kErrUnsupported, "join keys must be values");
+				}
+				pr.keys.push_back(e);
+			}
+			pr.npay = (int)jd.pay_b.size();
+			const int opi = (int)out.pipes[pi].ops.size();
+			out.pipes[pi].ops.push_back(pr);
+			/* visible after the join: probe columns, build keys (= probe keys), payloads */
+			for (size_t k = 0; k < op->right_keys.size(); k++) {
+				if (op->right_keys[k]->kind != RelExpr::ColId) {
+					throw Error(kErrUnsupported, "build keys must be column references");
+				}
+				sc.cols.push_back(ScopeEntry{op->right_keys[k]->text, pr.keys[k], "", ""});
+			}
+			for (size_t k = 0; k < op->right_payl.size(); k++) {
+				if (op->right_payl[k]->kind != RelExpr::ColId) {
+					throw Error(kErrUnsupported, "build payloads must be column references");
+				}
+				auto e = std::make_shared<BExpr>();
+				e->kind = BExpr::ProbeOut;
+				e->probe = opi;
+				e->pidx = (int)k;
+				e->b = jd.pay_b[k];
+				sc.cols.push_back(ScopeEntry{op->right_payl[k]->text, e, "", ""});
+			}
+			return pi;
+		}
+		case RelOp::HashAggr:
+			throw Error(kErrUnsupported, "aggregation is only supported at the root of the plan");
+		}
+		throw Error(kErrInvalid, "bad operator");
+	}
+
+	int64_t rows_bound(const Pipeline& p) {
+		__int128 r = p.rows;
+		for (auto& o : p.ops) {
+			if (o.kind == Op::Probe && !out.joins[o.join].join01) {
+				r *= std::max<int64_t>(1, out.joins[o.join].build_rows);
+			}
+		}
+		return r > kI64Max ? INT64_MAX : (int64_t)r;
+	}
+
+	void aggregate(const RelOpP& op) {
+		Scope sc;
+		int pi = lower(op->left, sc);
+		Pipeline& p = out.pipes[pi];
+		Sink sink;
+		const int64_t rows = rows_bound(p);
+		for (auto& k : op->exprs) {
+			BExprP e = bind(k, sc, p);
+			if (e->boolean) {
+				throw Error(kErrUnsupported, "group keys must be values");
+			}
+			sink.keys.push_back(e);
+		}
+		for (auto& a : op->aggregates) {
+			if (a->kind != RelExpr::Fun || (a->text != "sum" && a->text != "count")) {
+				throw Error(kErrUnsupported, "aggregates must be sum(expr) or count()");
+			}
+			Sink::Agg ag;
+			if (a->text == "count") {
+				ag.count = true;
+				sink.count_idx = (int)sink.aggs.size();
+			} else {
+				if (a->args.size() != 1) {
+					throw Error(kErrInvalid, "sum takes one argument");
+				}
+				ag.arg = bind(a->args[0], sc, p);
+				if (ag.arg->boolean) {
+					throw Error(kErrUnsupported, "sum over a predicate is not supported");
+				}
+				Bounds sb;
+				sb.lo = ag.arg->b.lo < 0 ? ag.arg->b.lo * rows : 0;
+				sb.hi = ag.arg->b.hi > 0 ? ag.arg->b.hi * rows : 0;
+				check_range(sb, "sum(...) over " + std::to_string(rows) + " rows");
+			}
+			sink.aggs.push_back(ag);
+		}
+		if (sink.count_idx < 0) {
+			Sink::Agg ag;
+			ag.count = true;
+			ag.visible = false;
+			sink.count_idx = (int)sink.aggs.size();
+			sink.aggs.push_back(ag);
+		}
+		if (op->global) {
+			sink.kind = Sink::AggGlobal;
+			sink.groups_bound = 1;
+		} else {
+			if (sink.keys.empty()) {
+				throw Error(kErrInvalid, "hash aggregation needs keys");
+			}
+			__int128 domain = 1;
+			int shift = 0;
+			for (auto& k : sink.keys) {
+				const __int128 range = k->b.hi - k->b.lo + 1;
+				sink.key_shift.push_back(shift);
+				shift += bits_for(range);
+				domain *= range;
+				if (domain > ((__int128)1 << 100)) {
+					domain = (__int128)1 << 100;
+				}
+			}
+			/* mixed-radix strides for the dense slot index (last key fastest) */
+			sink.key_radix.assign(sink.keys.size(), 1);
+			__int128 stride = 1;
+			for (int i = (int)sink.keys.size() - 1; i >= 0; i--) {
+				sink.key_radix[i] = stride > kI64Max ? 0 : (int64_t)stride;
+				stride *= sink.keys[i]->b.hi - sink.keys[i]->b.lo + 1;
+				if (stride > kI64Max) {
+					stride = kI64Max;
+				}
+			}
+			sink.key_bits = shift;
+			sink.domain = domain;
+			__int128 gb = std::min<__int128>(domain, std::max<int64_t>(rows, 1));
+			sink.groups_bound = (int64_t)gb;
+			const bool dense_ok = domain <= (__int128)fl.dense_limit;
+			if (fl.aggr == "dense" && domain > (__int128)(1 << 22)) {
+				throw Error(kErrUnsupported, "aggr=dense needs a key domain of at most 2^22 slots");
+			}
+			if (fl.aggr == "dense" || (fl.aggr == "auto" && dense_ok)) {
+				sink.kind = Sink::AggDense;
+			} else {
+				if (sink.key_bits > 62) {
+					throw Error(kErrUnsupported, "group key domain needs more than 62 bits");
+				}
+				sink.kind = Sink::AggHash;
+			}
+		}
+		p.sink = sink;
+		out.result_pipe = pi;
+		int vis = (int)sink.keys.size();
+		for (auto& a : sink.aggs) {
+			vis += a.visible ? 1 : 0;
+		}
+		out.result_cols = vis;
+	}
+
+	void root(const RelOpP& op) {
+		if (op->kind == RelOp::HashAggr) {
+			aggregate(op);
+			return;
+		}
+		Scope sc;
+		int pi = lower(op, sc);
+		Pipeline& p = out.pipes[pi];
+		p.sink.kind = Sink::Emit;
+		for (auto& s : sc.cols) {
+			BExprP e = resolve(s, p);
+			if (e->boolean) {
+				throw Error(kErrUnsupported, "predicate columns cannot be emitted");
+			}
+			p.sink.outs.push_back(e);
+		}
+		p.sink.groups_bound = rows_bound(p);
+		out.result_pipe = pi;
+		out.result_cols = (int)p.sink.outs.size();
+	}
+};
+
+} // namespace
+
+LoweredPlan lower_plan(const RelOpP& root, std::map<std::string, Table>& tables, const Flavor& fl)
+{
+	Lowerer l(tables, fl);
+	l.root(root);
+	if (l.out.result_cols == 0) {
+		throw Error(kErrInvalid, "the plan produces no columns");
+	}
+	return l.out;
+}
+
+} // namespace vc

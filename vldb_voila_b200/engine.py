@@ -1,0 +1,363 @@
+"""ctypes binding of the C ABI in include/voila_cuda.h.
+
+The Python side mirrors the reference's query lifecycle: a Database of typed columns with
+declared min/max (runtime::Database, db-engine-paradigms/include/common/runtime/Database.hpp:28-75),
+a plan (relalg tree, relalg.hpp) and a query that is created with a flavor, run, reset and
+freed (voila_query_new/run/reset/free, codegen.cpp:371-392).  Results come back as
+QueryResult text rows "a|b|c" (runtime_framework.cpp:77-111) or as int64 columns.
+
+There is no CPU execution path: without the compiled library or a B200 the calls fail.
+"""
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libvoila_cuda.so")
+
+VC_OK = 0
+ERRORS = {1: "invalid", 2: "cuda", 3: "capacity", 4: "timeout", 5: "compile", 6: "unsupported", 7: "no device"}
+
+TYPES = {"u8": 1, "i16": 2, "i32": 3, "i64": 4}
+NP_TYPES = {1: np.uint8, 2: np.int16, 3: np.int32, 4: np.int64}
+
+GEN_KINDS = {"uniform": 0, "seq": 1, "perm": 2, "zipf": 3, "choice": 4, "div": 5, "mod": 6}
+
+_lib_handle = None
+
+
+class VoilaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{ERRORS.get(code, code)}] {msg}")
+        self.code = code
+
+
+def lib():
+    """Loads libvoila_cuda.so (built in-tree by python -m vldb_voila_b200.build)."""
+    global _lib_handle
+    if _lib_handle is not None:
+        return _lib_handle
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m vldb_voila_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    c = ctypes
+    P = c.c_void_p
+    sigs = {
+        "vc_last_error": (c.c_char_p, []),
+        "vc_version": (c.c_char_p, []),
+        "vc_engine_create": (c.c_int, [c.c_int, c.POINTER(P)]),
+        "vc_engine_create_offline": (c.c_int, [c.c_int, c.POINTER(P)]),
+        "vc_engine_destroy": (c.c_int, [P]),
+        "vc_table_create": (c.c_int, [P, c.c_char_p, c.c_int64]),
+        "vc_table_drop": (c.c_int, [P, c.c_char_p]),
+        "vc_column_add": (c.c_int, [P, c.c_char_p, c.c_char_p, c.c_int, c.c_int64, c.c_int64]),
+        "vc_column_upload": (c.c_int, [P, c.c_char_p, c.c_char_p, P, c.c_int64, P]),
+        "vc_column_download": (c.c_int, [P, c.c_char_p, c.c_char_p, P, c.c_int64, P]),
+        "vc_column_attach": (c.c_int, [P, c.c_char_p, c.c_char_p, P]),
+        "vc_column_device_ptr": (c.c_int, [P, c.c_char_p, c.c_char_p, c.POINTER(P)]),
+        "vc_column_generate": (c.c_int, [P, c.c_char_p, c.c_char_p, c.c_int32, c.c_int64, c.c_int64, c.c_int64,
+                                         c.c_double, c.c_uint64, P, P]),
+        "vc_gen_host": (c.c_int, [c.c_int32, c.c_int32, c.c_int64, c.c_int64, c.c_int64, c.c_double, c.c_uint64,
+                                  c.c_int64, P, c.c_int64, c.c_int64, P]),
+        "vc_gen_zipf_cdf": (c.c_int, [c.c_double, c.c_int64, P]),
+        "vc_workload_describe": (c.c_int, [c.c_char_p, P, c.c_size_t, c.POINTER(c.c_size_t)]),
+        "vc_workload_batch": (c.c_int, [c.c_int, c.c_uint64, c.c_int64, c.c_int64, P, c.c_size_t,
+                                        c.POINTER(c.c_size_t)]),
+        "vc_query_new": (c.c_int, [P, c.c_char_p, c.c_char_p, c.POINTER(P)]),
+        "vc_query_run": (c.c_int, [P, P]),
+        "vc_query_reset": (c.c_int, [P]),
+        "vc_query_free": (c.c_int, [P]),
+        "vc_query_result_shape": (c.c_int, [P, c.POINTER(c.c_int64), c.POINTER(c.c_int32)]),
+        "vc_query_result_copy": (c.c_int, [P, P, c.c_int64]),
+        "vc_query_result_text": (c.c_int, [P, P, c.c_size_t, c.POINTER(c.c_size_t)]),
+        "vc_query_info": (c.c_int, [P, P, c.c_size_t, c.POINTER(c.c_size_t)]),
+        "vc_query_source": (c.c_int, [P, P, c.c_size_t, c.POINTER(c.c_size_t)]),
+        "vc_query_profile": (c.c_int, [P, c.c_int]),
+        "vc_query_timings": (c.c_int, [P, c.POINTER(c.c_float), c.c_int, c.POINTER(c.c_int), P, c.c_size_t]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib_handle = L
+    return L
+
+
+def check(rc):
+    if rc != VC_OK:
+        raise VoilaError(rc, lib().vc_last_error().decode())
+
+
+def _b(s):
+    return s.encode() if isinstance(s, str) else s
+
+
+def _text_call(fn, *args):
+    n = ctypes.c_size_t(0)
+    check(fn(*args, None, 0, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(n.value + 1)
+    check(fn(*args, buf, n.value + 1, ctypes.byref(n)))
+    return buf.raw[:n.value].decode()
+
+
+def _stream_ptr(stream):
+    """Accepts None, an int handle, or a torch.cuda.Stream."""
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return ctypes.c_void_p(stream)
+    return ctypes.c_void_p(int(stream.cuda_stream))
+
+
+# ---------------------------------------------------------------------------- workloads
+
+
+@dataclass
+class ColumnSpec:
+    table: str
+    name: str
+    type: int
+    kind: int
+    a: int
+    b: int
+    c: int
+    s: float
+    seed: int
+    n: int
+    lo: int
+    hi: int
+
+    @property
+    def dtype(self):
+        return NP_TYPES[self.type]
+
+
+@dataclass
+class Workload:
+    spec: str
+    template: str
+    fact_table: str
+    fact_rows: int
+    algo_bytes: int
+    probe_bytes: int
+    tables: dict = field(default_factory=dict)     # name -> rows
+    columns: list = field(default_factory=list)    # ColumnSpec
+    plan: str = ""
+
+    def table_columns(self, table):
+        return [c for c in self.columns if c.table == table]
+
+
+def workload(spec):
+    """Tables, generators and plan of a synthetic workload spec (see csrc/workloads.hpp)."""
+    text = _text_call(lib().vc_workload_describe, _b(spec))
+    w = Workload(spec=spec, template="", fact_table="", fact_rows=0, algo_bytes=0, probe_bytes=0)
+    for line in text.splitlines():
+        tag, _, rest = line.partition(" ")
+        if tag == "template":
+            w.template = rest
+        elif tag == "fact":
+            t, n = rest.split()
+            w.fact_table, w.fact_rows = t, int(n)
+        elif tag == "bytes":
+            a, p = rest.split()
+            w.algo_bytes, w.probe_bytes = int(a), int(p)
+        elif tag == "table":
+            t, n = rest.split()
+            w.tables[t] = int(n)
+        elif tag == "column":
+            f = rest.split()
+            w.columns.append(ColumnSpec(f[0], f[1], int(f[2]), int(f[3]), int(f[4]), int(f[5]), int(f[6]),
+                                        float(f[7]), int(f[8]), int(f[9]), int(f[10]), int(f[11])))
+        elif tag == "plan":
+            w.plan = rest
+    return w
+
+
+def batch_specs(count, seed, min_rows=10_000, max_rows=60_000_000):
+    return _text_call(lib().vc_workload_batch, count, seed, min_rows, max_rows).split()
+
+
+def zipf_cdf(s, n):
+    out = np.empty(n, dtype=np.float64)
+    check(lib().vc_gen_zipf_cdf(s, n, out.ctypes.data))
+    return out
+
+
+def generate_host(col, begin=0, count=None, cdf=None):
+    """The column's values for rows [begin, begin+count), generated on the host."""
+    count = col.n - begin if count is None else count
+    out = np.empty(count, dtype=col.dtype)
+    if col.kind == GEN_KINDS["zipf"] and col.s != 0.0 and cdf is None:
+        cdf = zipf_cdf(col.s, col.b)
+    check(lib().vc_gen_host(col.kind, col.type, col.a, col.b, col.c, col.s, col.seed, col.n,
+                            None if cdf is None else cdf.ctypes.data, begin, count, out.ctypes.data))
+    return out
+
+
+def generate_workload_host(w):
+    """{table: {column: ndarray}} for every column of the workload."""
+    data = {t: {} for t in w.tables}
+    cdfs = {}
+    for c in w.columns:
+        cdf = None
+        if c.kind == GEN_KINDS["zipf"] and c.s != 0.0:
+            key = (c.s, c.b)
+            if key not in cdfs:
+                cdfs[key] = zipf_cdf(c.s, c.b)
+            cdf = cdfs[key]
+        data[c.table][c.name] = generate_host(c, cdf=cdf)
+    return data
+
+
+# ---------------------------------------------------------------------------- engine
+
+
+class Engine:
+    """A device (or, with offline=True, a compile-only) database of columns in HBM."""
+
+    def __init__(self, device=0, offline=False, sms=148):
+        h = ctypes.c_void_p()
+        if offline:
+            check(lib().vc_engine_create_offline(sms, ctypes.byref(h)))
+        else:
+            check(lib().vc_engine_create(device, ctypes.byref(h)))
+        self._h = h
+        self.offline = offline
+        self.tables = {}
+
+    def close(self):
+        if self._h:
+            check(lib().vc_engine_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def create_table(self, name, rows):
+        check(lib().vc_table_create(self._h, _b(name), rows))
+        self.tables[name] = {"rows": rows, "columns": {}}
+
+    def add_column(self, table, name, type_, lo, hi):
+        t = TYPES[type_] if isinstance(type_, str) else type_
+        check(lib().vc_column_add(self._h, _b(table), _b(name), t, int(lo), int(hi)))
+        self.tables[table]["columns"][name] = t
+
+    def upload(self, table, name, array, stream=None):
+        t = self.tables[table]["columns"][name]
+        a = np.ascontiguousarray(array, dtype=NP_TYPES[t])
+        check(lib().vc_column_upload(self._h, _b(table), _b(name), a.ctypes.data, len(a), _stream_ptr(stream)))
+        return a
+
+    def upload_ptr(self, table, name, host_ptr, rows, stream=None):
+        check(lib().vc_column_upload(self._h, _b(table), _b(name), ctypes.c_void_p(host_ptr), rows,
+                                     _stream_ptr(stream)))
+
+    def download(self, table, name):
+        t = self.tables[table]["columns"][name]
+        out = np.empty(self.tables[table]["rows"], dtype=NP_TYPES[t])
+        check(lib().vc_column_download(self._h, _b(table), _b(name), out.ctypes.data, len(out), None))
+        return out
+
+    def attach(self, table, name, device_ptr):
+        check(lib().vc_column_attach(self._h, _b(table), _b(name), ctypes.c_void_p(device_ptr)))
+
+    def device_ptr(self, table, name):
+        p = ctypes.c_void_p()
+        check(lib().vc_column_device_ptr(self._h, _b(table), _b(name), ctypes.byref(p)))
+        return p.value
+
+    def generate(self, col, cdf=None, stream=None):
+        if col.kind == GEN_KINDS["zipf"] and col.s != 0.0 and cdf is None:
+            cdf = zipf_cdf(col.s, col.b)
+        check(lib().vc_column_generate(self._h, _b(col.table), _b(col.name), col.kind, col.a, col.b, col.c, col.s,
+                                       col.seed, None if cdf is None else cdf.ctypes.data, _stream_ptr(stream)))
+
+    def load_workload(self, w, data=None, on_device=True, stream=None):
+        """Declares the workload's tables and fills them: from `data` ({table: {col: array}}),
+        else with the device generator (on_device) or host generation + upload."""
+        for t, rows in w.tables.items():
+            self.create_table(t, rows)
+        for c in w.columns:
+            self.add_column(c.table, c.name, c.type, c.lo, c.hi)
+            if self.offline:
+                continue
+            if data is not None:
+                self.upload(c.table, c.name, data[c.table][c.name], stream)
+            elif on_device:
+                self.generate(c, stream=stream)
+            else:
+                self.upload(c.table, c.name, generate_host(c), stream)
+
+    def query(self, plan, flavor=""):
+        return Query(self, plan, flavor)
+
+
+class Query:
+    """A compiled query: vc_query_new / run / reset / free."""
+
+    def __init__(self, engine, plan, flavor=""):
+        self.engine = engine
+        h = ctypes.c_void_p()
+        check(lib().vc_query_new(engine._h, _b(plan), _b(flavor or ""), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            check(lib().vc_query_free(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, stream=None):
+        check(lib().vc_query_run(self._h, _stream_ptr(stream)))
+        return self
+
+    def reset(self):
+        check(lib().vc_query_reset(self._h))
+
+    def shape(self):
+        r = ctypes.c_int64()
+        c = ctypes.c_int32()
+        check(lib().vc_query_result_shape(self._h, ctypes.byref(r), ctypes.byref(c)))
+        return r.value, c.value
+
+    def result(self):
+        """int64 array of shape (rows, cols)."""
+        r, c = self.shape()
+        out = np.empty(max(r * c, 1), dtype=np.int64)
+        check(lib().vc_query_result_copy(self._h, out.ctypes.data, out.size))
+        return out[: r * c].reshape(c, r).T.copy()
+
+    def result_text(self):
+        return _text_call(lib().vc_query_result_text, self._h)
+
+    def result_lines(self):
+        return sorted(l for l in self.result_text().split("\n") if l)
+
+    def info(self):
+        import json
+        return json.loads(_text_call(lib().vc_query_info, self._h))
+
+    def source(self):
+        return _text_call(lib().vc_query_source, self._h)
+
+    def profile(self, enable=True):
+        check(lib().vc_query_profile(self._h, 1 if enable else 0))
+
+    def timings(self):
+        ms = (ctypes.c_float * 256)()
+        n = ctypes.c_int()
+        names = ctypes.create_string_buffer(1 << 16)
+        check(lib().vc_query_timings(self._h, ms, 256, ctypes.byref(n), names, len(names)))
+        kn = names.value.decode().split("\n")
+        return [(kn[i], float(ms[i])) for i in range(n.value)]

@@ -1,0 +1,385 @@
+"""Benchmark of the CUDA flavor on VOILA's hot path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload config2] [--impl ours|reference]
+
+A step is one run of the workload's query (all of its fused pipelines: join-table build,
+probe + aggregation, result extraction) over one batch of synthetic input resident in HBM.
+Default workload: the hash join + global aggregate (1.5M-row build filtered to 20 %, 6M-row
+probe).  `value` is fact (probe) rows per second over the whole job; between timed steps
+L2 is flushed by writing a 256 MiB buffer.  `e2e` is the same metric through the public
+C ABI with the inputs uploaded from pinned host memory and the result read back every step.
+
+Under torchrun (N > 1) every rank runs the same query over its own fact shard (weak
+scaling) and the global aggregate's partial sums are combined with an NCCL all-reduce
+(the exchange step of the reference's flush2partitions + re-aggregation).
+
+--impl reference times the reference's own CPU implementation (its hyper and vectorwise
+flavors compiled from source into oracle/_ref, all host threads) on the same workload; if
+that build is not usable on this host it falls back to the numpy port of the oracle.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+WORKLOADS = {
+    "config1": "sel_aggr:rows=6000000,seed=1",
+    "config2": "join_aggr:build=1500000,probe=6000000,sel=0.2,seed=2",
+    "config3": "groupby:rows=6000000,keys=1500000,zipf=1.25,seed=3",
+    "config4": "star:rows=60000000,seed=4",
+}
+REF_NAMES = {"sel_aggr": "sel_aggr", "join_aggr": "join_aggr", "groupby": "groupby", "star": "star"}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--workload", default="config2")
+    ap.add_argument("--flavor", default="")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def spec_of(name, rank=0):
+    spec = WORKLOADS.get(name, name)
+    if rank:
+        # each rank generates its own tables from its own seed
+        spec = spec.replace("seed=", f"seed={rank}00")
+    return spec
+
+
+# ---------------------------------------------------------------------------- clocks
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        mhz, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                maxes.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not mhz:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": max(maxes), "reasons": sorted(reasons),
+                "samples": len(mhz)}
+
+
+# ---------------------------------------------------------------------------- CPU baseline
+
+
+def _ref_dir():
+    d = os.path.join(REPO, "oracle", "_ref", "avx512")
+    try:
+        with open("/proc/cpuinfo") as f:
+            if "avx512f" not in f.read():
+                return None
+    except OSError:
+        return None
+    return d if os.path.exists(os.path.join(d, "ref_run")) else None
+
+
+def reference_cpu(spec, reps, warmup, threads=None):
+    """Times the reference's generated query libraries (hyper and vectorwise) with ref_run.
+    Returns {flavor: [ms per rep]} or None when the reference build is unavailable."""
+    d = _ref_dir()
+    if d is None:
+        return None
+    threads = threads or os.cpu_count()
+    tmpl = spec.split(":")[0]
+    out = {}
+    for fl in ("hyper", "vectorwise"):
+        lib = os.path.join(d, f"q_{REF_NAMES[tmpl]}_{fl}.so")
+        if not os.path.exists(lib):
+            continue
+        r = subprocess.run([os.path.join(d, "ref_run"), "--workload", spec, "--lib", lib, "--flavor", fl,
+                            "--threads", str(threads), "--reps", str(reps + warmup), "--no-result", "1"],
+                           capture_output=True, text=True, timeout=1800)
+        if r.returncode != 0:
+            continue
+        info = json.loads(r.stdout.strip().splitlines()[-1])
+        out[fl] = info["times_ms"][warmup:]
+    return out or None
+
+
+def port_cpu(spec, reps):
+    """Times the numpy oracle port (single process) on the workload."""
+    from oracle.voila_oracle import run_plan
+    from vldb_voila_b200 import generate_workload_host, workload
+    w = workload(spec)
+    data = generate_workload_host(w)
+    times = []
+    for _ in range(reps):
+        t = time.perf_counter()
+        run_plan(w.plan, data)
+        times.append((time.perf_counter() - t) * 1e3)
+    return times
+
+
+def cpu_baseline(spec, fact_rows, reps=5, warmup=1):
+    ref = reference_cpu(spec, reps, warmup)
+    if ref:
+        best = min(ref, key=lambda k: statistics.median(ref[k]))
+        ms = statistics.median(ref[best])
+        return {"value": fact_rows / (ms / 1e3), "unit": "fact rows/s", "cores": os.cpu_count(),
+                "kind": "reference", "flavor": best,
+                "flavors_ms": {k: round(statistics.median(v), 3) for k, v in ref.items()},
+                "sample": f"the full workload {spec}, {reps} hot runs (qrun interval, no result printing), "
+                          f"median; reference built from source, -march=skylake-avx512"}
+    ms = statistics.median(port_cpu(spec, max(1, reps // 2)))
+    return {"value": fact_rows / (ms / 1e3), "unit": "fact rows/s", "cores": 1, "kind": "port",
+            "sample": f"the full workload {spec} through the numpy oracle, median"}
+
+
+# ---------------------------------------------------------------------------- reference arm
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from vldb_voila_b200 import workload
+    spec = spec_of(args.workload)
+    w = workload(spec)
+    t0 = time.perf_counter()
+    ref = reference_cpu(spec, args.steps, args.warmup)
+    if ref:
+        best = min(ref, key=lambda k: statistics.median(ref[k]))
+        times = ref[best]
+        kind, cores = "reference", os.cpu_count()
+        sample = f"{spec}: each step one full hot run (qrun) of the reference's {best} flavor"
+    else:
+        times = port_cpu(spec, args.steps)
+        kind, cores, best = "port", 1, "numpy"
+        sample = f"{spec}: each step one run of the numpy oracle port"
+    ms = statistics.mean(times)
+    value = w.fact_rows / (ms / 1e3)
+    line = {
+        "impl": "reference", "metric": "fact rows/s (probe pipeline)", "value": value, "unit": "fact rows/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": spec, "template": w.template, "fact_rows": w.fact_rows, "flavor": best},
+        "cpu_baseline": {"value": value, "unit": "fact rows/s", "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "fact rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": round(time.perf_counter() - t0, 1),
+    }
+    if ref:
+        line["flavors_ms"] = {k: round(statistics.mean(v), 3) for k, v in ref.items()}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------- our arm
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from vldb_voila_b200 import Engine, workload
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    spec = spec_of(args.workload, rank)
+    w = workload(spec)
+    eng = Engine(local)
+    stream = torch.cuda.current_stream()
+    eng.load_workload(w, on_device=True, stream=stream)
+    torch.cuda.synchronize()
+    q = eng.query(w.plan, args.flavor)
+    info = q.info()
+    kernels = [k["name"] for k in info["kernels"]]
+    dom = [i for i, k in enumerate(info["kernels"]) if k["dominant"]][0]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step():
+        q.run(stream)
+
+    def combine():
+        if world > 1 and w.template == "join_aggr":
+            part = torch.from_numpy(q.result().reshape(-1).astype(np.int64)).cuda()
+            if part.numel() == 0:
+                part = torch.zeros(2, dtype=torch.int64, device="cuda")
+            dist.all_reduce(part)
+
+    for i in range(args.warmup):
+        flush.fill_(i & 0xff)
+        step()
+        combine()
+    torch.cuda.synchronize()
+
+    q.profile(True)
+    step_ms, dom_ms, all_ms = [], [], []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.fill_((i + 1) & 0xff)
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            step()
+            ev1.record(stream)
+            combine()
+            ev1.synchronize()
+            step_ms.append(ev0.elapsed_time(ev1))
+            t = q.timings()
+            dom_ms.append(t[dom][1])
+            all_ms.append([x[1] for x in t])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    q.profile(False)
+    ms = statistics.mean(step_ms)
+    if world > 1:
+        tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * w.fact_rows / (ms / 1e3)
+
+    # e2e through the public API: pinned host inputs uploaded every step, result read back
+    from vldb_voila_b200.engine import generate_workload_host
+    host = generate_workload_host(w)
+    pinned = {}
+    h2d = 0
+    for c in w.columns:
+        a = host[c.table][c.name]
+        t = torch.from_numpy(a.view(np.uint8) if a.dtype != np.uint8 else a).pin_memory()
+        pinned[(c.table, c.name)] = (t, len(a))
+        h2d += a.nbytes
+    e2e_ms = []
+    d2h = 0
+    for i in range(args.warmup + args.steps):
+        flush.fill_(i & 0xff)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for (tb, cn), (t, n) in pinned.items():
+            eng.upload_ptr(tb, cn, t.data_ptr(), n, stream)
+        q.run(stream)
+        res = q.result()
+        combine()
+        t1 = time.perf_counter()
+        d2h = res.nbytes + 16
+        if i >= args.warmup:
+            e2e_ms.append((t1 - t0) * 1e3)
+    e2e = statistics.mean(e2e_ms)
+    if world > 1:
+        tt = torch.tensor([e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e = float(tt.item())
+
+    peaks = {}
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    dom_avg = statistics.mean(dom_ms)
+    achieved = w.probe_bytes / (dom_avg / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(w.template)
+
+    if rank == 0:
+        line = {
+            "metric": "fact rows/s (probe pipeline)",
+            "value": value,
+            "unit": "fact rows/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "int64",
+            "data": "synthetic (seeded generator, resident in HBM)",
+            "config": {"workload": spec, "template": w.template, "fact_rows": w.fact_rows,
+                       "flavor": info["flavor"], "l2": "flushed between timed steps (256 MiB write)",
+                       "parallelism": f"dp{world}" if world > 1 else "single GPU"},
+            "e2e": {"value": world * w.fact_rows / (e2e / 1e3), "unit": "fact rows/s", "ms_per_step": e2e,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "kernel": kernels[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes": w.probe_bytes, "kernel_ms": dom_avg,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
+                         else "fallback 6650 GB/s"},
+            "gpu_launches": len(kernels) * args.steps,
+            "kernel_ms": {k: round(statistics.mean(r[i] for r in all_ms), 5) for i, k in enumerate(kernels)},
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(spec, w.fact_rows)
+        print(json.dumps(line))
+    q.close()
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

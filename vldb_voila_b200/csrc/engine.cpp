@@ -338,8 +338,23 @@ void query_launch(Query& q, cudaStream_t stream)
 	refresh_column_params(q);
 	q.stream = stream;
 	q.result_rows = -1;
-	if (q.flavor.graph && !q.profile) {
+	if (q.flavor.graph) {
+		if (q.graph && q.graph_profiled != q.profile) {
+			/* profiling events are nodes of the graph: re-capture when profiling toggles */
+			cudaGraphExecDestroy(q.graph);
+			q.graph = nullptr;
+		}
+		if (q.profile && q.ev.size() != 2 * q.code.launches.size()) {
+			for (auto e : q.ev) {
+				cudaEventDestroy(e);
+			}
+			q.ev.assign(2 * q.code.launches.size(), nullptr);
+			for (auto& e : q.ev) {
+				VC_CHECK_CUDA(cudaEventCreate(&e));
+			}
+		}
 		if (!q.graph) {
+			q.graph_profiled = q.profile;
 			cudaStream_t cs;
 			VC_CHECK_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
 			cudaGraph_t g;

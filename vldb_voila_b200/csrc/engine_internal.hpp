@@ -180,7 +180,7 @@ struct Flavor {
 	int bucket = 32;          /* join bucket bytes: 32 (sector) or the slot size */
 	int grid = 0;             /* CTAs per SM (0 = occupancy) */
 	int dense_limit = 4096;   /* largest dense key domain */
-	bool graph = false;       /* replay the query's launches from a CUDA graph */
+	bool graph = true;        /* replay the query's launches from a CUDA graph */
 
 	std::string str() const;
 	static Flavor parse(const std::string& s);
@@ -267,6 +267,7 @@ struct Query {
 	std::vector<cudaEvent_t> ev;         /* per launch begin/end when profiling */
 	std::vector<float> last_ms;
 	cudaGraphExec_t graph = nullptr;
+	bool graph_profiled = false;         /* the graph records the profiling events */
 	cudaStream_t graph_stream = nullptr;
 	bool ran = false;
 	int64_t result_rows = -1;

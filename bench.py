@@ -267,12 +267,12 @@ def main():
         combine()
     torch.cuda.synchronize()
 
-    q.profile(True)
     step_ms, dom_ms, all_ms = [], [], []
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
+        # timed steps: device time of each step (no per-kernel events inside)
         for i in range(args.steps):
             flush.fill_((i + 1) & 0xff)
             ev0 = torch.cuda.Event(enable_timing=True)
@@ -283,13 +283,22 @@ def main():
             combine()
             ev1.synchronize()
             step_ms.append(ev0.elapsed_time(ev1))
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        # profiled pass: per-kernel device times from events on the launch stream
+        q.profile(True)
+        for i in range(args.steps):
+            flush.fill_((i + 1) & 0xff)
+            step()
+            combine()
             t = q.timings()
             dom_ms.append(t[dom][1])
             all_ms.append([x[1] for x in t])
+        q.profile(False)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    q.profile(False)
     ms = statistics.mean(step_ms)
     if world > 1:
         tt = torch.tensor([ms], dtype=torch.float64, device="cuda")

@@ -4,22 +4,25 @@
  * This is the CUDA counterpart of the reference's per-pipeline code generators
  * (cg_hyper.cpp gen_pipeline :804-845, cg_vector.cpp :793-923): where those emit a
  * tuple-at-a-time loop or a chain of vector primitives, this emits a CUDA kernel in which
- * every thread owns `rows` consecutive rows of a tile (vector loads), evaluates the
- * pipeline's filters and probes for all of them (op-major, so independent hash-table loads
- * overlap) and feeds its sink.  Per pipeline sink:
+ * every thread owns `rows` consecutive rows of a tile, evaluates the pipeline's filters and
+ * probes for all of them (op-major, so independent hash-table loads overlap) and feeds its
+ * sink.  Column tiles arrive either by vector loads (load=ldg) or through a multi-stage
+ * shared-memory ring filled by bulk asynchronous copies (load=tma).  Per pipeline sink:
  *
- *   JoinBuild  materialise  (compacted packed keys/payloads/hashes; write/write_pos,
- *                            relalg_translator.cpp:828-907)
- *              clear + insert (bucket_build; runtime_struct.cpp:1283-1324)
- *   AggGlobal  registers -> block reduction -> one atomic per CTA (aggr_gsum/gcount)
- *   AggDense   shared-memory slots over the key domain, warp-combined updates, merged
- *              into a global slot array at CTA end; extract kernel emits count > 0 slots
- *   AggHash    global open-addressing group table, warp-combined leader updates,
- *              optional per-CTA shared-memory cache for hot keys; extract kernel
- *   Emit       warp-aggregated append of the selected rows
+ *   JoinBuild  direct: filter + insert into a table sized for every build row
+ *              staged: materialise (write/write_pos, relalg_translator.cpp:828-907) with a
+ *                      block-aggregated append, then clear + insert sized by the count
+ *                      (bucket_build / build_index, runtime_struct.cpp:1283-1324)
+ *   AggGlobal  registers -> block reduction -> one atomic per CTA (aggr_gsum/gcount); the
+ *              last CTA publishes the row
+ *   AggDense   shared-memory slots over the key domain with warp-combined updates, merged
+ *              into a global slot array; the last CTA emits slots with count > 0
+ *   AggHash    global open-addressing group table with warp-combined leader updates and an
+ *              optional per-CTA shared-memory cache for hot keys; separate extract kernel
+ *   Emit       block-aggregated append of the selected rows
  *
  * The source depends only on the plan's shape (column types, operators, aggregate count)
- * and the flavor knobs.  Every data-dependent number (row counts, constants, key ranges,
+ * and the flavor knobs; every data-dependent number (row counts, constants, key ranges,
  * pointers) is a kernel parameter, so one compiled module serves every instance of a shape.
  */
 #include <algorithm>
@@ -39,6 +42,11 @@ static const char* ctype(int t)
 	}
 }
 
+static int type_bytes(int t)
+{
+	return vc_gen_type_size(t);
+}
+
 static int64_t pow2_at_least(int64_t x)
 {
 	int64_t p = 1;
@@ -54,13 +62,25 @@ struct PipeGen {
 	Pipeline& p;
 	LoweredPlan& plan;
 	const Flavor& fl;
+	const PipeDeviceState& st;
+	const QueryDeviceState& qs;
 	std::vector<unsigned long long>& params;
 	std::ostringstream o;
 	std::string name;
 	int V;
+	int T;
+	size_t smem_sink = 0;      /* dynamic shared memory used by the sink */
+	size_t smem_total = 0;
+	int cache_slots = 0;
+	bool dense_in_smem = false;
+	int replicas = 1;          /* per-warp copies of the dense slot array (lowcard=atomic) */
+	bool private_acc = false;  /* per-thread private accumulators (lowcard=private) */
+	static constexpr int kGmax = 8; /* distinct groups per block held in private accumulators */
+	static constexpr int kExtractK = 4; /* slot groups per warp step of the group extraction */
 
-	PipeGen(Pipeline& pp, LoweredPlan& pl, const Flavor& f, std::vector<unsigned long long>& prm)
-		: p(pp), plan(pl), fl(f), params(prm), V(f.rows) {
+	PipeGen(Pipeline& pp, LoweredPlan& pl, const Flavor& f, const PipeDeviceState& s, const QueryDeviceState& q,
+		std::vector<unsigned long long>& prm)
+		: p(pp), plan(pl), fl(f), st(s), qs(q), params(prm), V(f.rows), T(f.threads) {
 		name = "vc_p" + std::to_string(p.id);
 	}
 
@@ -95,10 +115,17 @@ struct PipeGen {
 			static const std::map<std::string, std::string> ops = {
 				{"add", "+"}, {"sub", "-"}, {"mul", "*"}, {"lt", "<"}, {"le", "<="}, {"gt", ">"},
 				{"ge", ">="}, {"eq", "=="}, {"ne", "!="}, {"and", "&&"}, {"or", "||"}};
+			if (e->fn == "mul" && fits32(e->args[0]->b) && fits32(e->args[1]->b)) {
+				return "vd::mulw(" + expr(e->args[0], v) + ", " + expr(e->args[1], v) + ")";
+			}
 			return "(" + expr(e->args[0], v) + " " + ops.at(e->fn) + " " + expr(e->args[1], v) + ")";
 		}
 		}
 		return "0";
+	}
+
+	static bool fits32(const Bounds& b) {
+		return b.lo >= (__int128)INT32_MIN && b.hi <= (__int128)INT32_MAX;
 	}
 
 	int A() const { return (int)p.sink.aggs.size(); }
@@ -123,22 +150,27 @@ struct PipeGen {
 		return h;
 	}
 
-	void header(const std::string& kname, int threads) {
-		o << "extern \"C\" __global__ void __launch_bounds__(" << threads << ") " << kname
-		  << "(const VcParams p) {\n";
+	/* hash that picks table positions: voila_hash chain of the raw keys (hash=voila) or
+	 * the finalizer-mixed bit-packed key (hash=mix) */
+	std::string table_hash(const std::vector<BExprP>& keys, const std::string& packed, int bits,
+		const std::string& v) {
+		if (fl.hash == "voila") {
+			return key_hash(keys, v);
+		}
+		return bits <= 32 ? "vd::mix_hash32((uint32_t)(" + packed + "))" : "vd::mix_hash64(" + packed + ")";
+	}
+
+	std::string join_slot_type(const JoinDesc& jd) {
+		return std::string("vd::JoinSlot<") + (jd.key64 ? "uint64_t" : "uint32_t") + ", " +
+			(jd.pay64 ? "uint64_t" : "uint32_t") + ">";
 	}
 
 	/* ------------------------------------------------------------ main kernel ------ */
 
-	std::string gen_main(size_t& smem_out) {
-		std::ostringstream body;
-		const int T = fl.threads;
-		smem_out = 0;
-
-		header(name + "_main", T);
+	std::string gen_main() {
+		o << "extern \"C\" __global__ void __launch_bounds__(" << T << ") " << name << "_main(const VcParams p) {\n";
 		o << "  const int64_t n = " << P((unsigned long long)p.rows) << ";\n";
 		p.err_slot = (int)params.size();
-		err_slot = params.size();
 		o << "  unsigned* const err = (unsigned*)p.v[" << params.size() << "];\n";
 		params.push_back(0); /* error word, filled by the runtime */
 		p.col_slots.clear();
@@ -149,34 +181,311 @@ struct PipeGen {
 			params.push_back(0); /* column pointer, filled by the runtime */
 		}
 		o << "  (void)err;\n";
-
-		sink_prologue(smem_out);
-
+		o << "  extern __shared__ __align__(128) unsigned char vd_smem[];\n";
+		plan_phases();
+		sink_prologue();
 		o << "  const int64_t tile = (int64_t)" << T << " * " << V << ";\n";
 		o << "  const int64_t ntiles = (n + tile - 1) / tile;\n";
-		o << "  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {\n";
-		o << "    const int64_t r0 = t * tile + (int64_t)threadIdx.x * " << V << ";\n";
-		o << "    bool act[" << V << "];\n";
-		o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) { act[v] = r0 + v < n; }\n";
+
+		emit_compaction_smem();
+		bool any_eager = false;
 		for (size_t c = 0; c < p.cols.size(); c++) {
-			o << "    " << ctype(p.cols[c].type) << " x" << c << "[" << V << "];\n";
-			o << "    vd::load_rows<" << ctype(p.cols[c].type) << ", " << V << ">(c" << c << ", r0, n, x" << c << ");\n";
+			any_eager = any_eager || eager[c];
 		}
-		/* ops, op-major */
-		for (size_t i = 0; i < p.ops.size(); i++) {
+		const bool tma = fl.load == "tma" && any_eager;
+		if (tma) {
+			gen_tma_loop();
+		} else if (fl.prefetch && any_eager) {
+			/* register double buffering: the next tile's eager columns are in flight while
+			 * this tile's probes and aggregation run */
+			o << "  {\n";
+			for (size_t c = 0; c < p.cols.size(); c++) {
+				if (eager[c]) {
+					o << "  " << ctype(p.cols[c].type) << " pf" << c << "[" << V << "];\n";
+				}
+			}
+			o << "  int64_t t = blockIdx.x;\n";
+			o << "  if (t < ntiles) {\n    const int64_t r0p = t * tile + (int64_t)threadIdx.x * " << V << ";\n";
+			emit_load_cols("ldg", "pf", "r0p");
+			o << "  }\n";
+			o << "  for (; t < ntiles; t += gridDim.x) {\n";
+			emit_decl_cols(true, V);
+			for (size_t c = 0; c < p.cols.size(); c++) {
+				if (eager[c]) {
+					o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) { x" << c << "[v] = pf" << c << "[v]; }\n";
+				}
+			}
+			o << "    {\n    const int64_t tn = t + gridDim.x;\n";
+			o << "    if (tn < ntiles) {\n    const int64_t r0p = tn * tile + (int64_t)threadIdx.x * " << V << ";\n";
+			emit_load_cols("ldg", "pf", "r0p");
+			o << "    }\n    }\n";
+			emit_body("pre");
+			o << "  }\n  }\n";
+		} else {
+			o << "  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {\n";
+			emit_body("ldg");
+			o << "  }\n";
+		}
+		sink_epilogue();
+		o << "}\n\n";
+		smem_total = std::max(smem_total, smem_sink);
+		return o.str();
+	}
+
+	/* tile bytes of all columns, each region 16-byte aligned */
+	size_t tile_region(size_t c) {
+		size_t off = 0;
+		for (size_t i = 0; i < c; i++) {
+			if (!eager[i]) {
+				continue;
+			}
+			off += (size_t)T * V * type_bytes(p.cols[i].type);
+			off = (off + 15) & ~(size_t)15;
+		}
+		return off;
+	}
+
+	void gen_tma_loop() {
+		const int S = fl.stages;
+		const size_t tile_bytes = tile_region(p.cols.size());
+		size_t base = (smem_sink + 127) & ~(size_t)127;
+		const size_t bar_off = base + (size_t)S * tile_bytes;
+		smem_total = bar_off + 8 * (size_t)S;
+		o << "  unsigned char* const stages = vd_smem + " << base << ";\n";
+		o << "  uint64_t* const full = (uint64_t*)(vd_smem + " << bar_off << ");\n";
+		o << "  const int64_t nfull = n / tile;\n";
+		o << "  if (threadIdx.x == 0) {\n";
+		o << "    for (int s = 0; s < " << S << "; s++) { vd::mbar_init(&full[s], 1); }\n";
+		o << "    vd::mbar_init_fence();\n";
+		o << "  }\n  __syncthreads();\n";
+		/* issue helper as a lambda */
+		o << "  auto issue = [&](int64_t j) {\n";
+		o << "    const int64_t tj = (int64_t)blockIdx.x + j * (int64_t)gridDim.x;\n";
+		o << "    if (tj >= nfull) { return; }\n";
+		o << "    const int s = (int)(j % " << S << ");\n";
+		o << "    unsigned char* dst = stages + (size_t)s * " << tile_bytes << ";\n";
+		o << "    vd::mbar_expect_tx(&full[s], " << tile_bytes_tx() << ");\n";
+		for (size_t c = 0; c < p.cols.size(); c++) {
+			if (!eager[c]) {
+				continue;
+			}
+			const int tb = type_bytes(p.cols[c].type);
+			o << "    vd::bulk_load(dst + " << tile_region(c) << ", c" << c << " + tj * tile, " << (size_t)T * V * tb
+			  << "u, &full[s]);\n";
+		}
+		o << "  };\n";
+		o << "  if (threadIdx.x == 0) {\n";
+		o << "    vd::fence_proxy_async();\n";
+		o << "    for (int j = 0; j < " << S - 1 << "; j++) { issue(j); }\n";
+		o << "  }\n";
+		o << "  bool timed_out = false;\n";
+		o << "  int64_t i = 0;\n";
+		o << "  for (;; i++) {\n";
+		o << "    const int64_t t = (int64_t)blockIdx.x + i * (int64_t)gridDim.x;\n";
+		o << "    if (t >= nfull) { break; }\n";
+		o << "    if (threadIdx.x == 0) { vd::fence_proxy_async(); issue(i + " << S - 1 << "); }\n";
+		o << "    const int s = (int)(i % " << S << ");\n";
+		o << "    const bool ok = vd::mbar_wait(&full[s], (uint32_t)((i / " << S << ") & 1));\n";
+		o << "    if (__syncthreads_or(!ok)) { timed_out = true; break; }\n";
+		o << "    const unsigned char* stage = stages + (size_t)s * " << tile_bytes << ";\n";
+		emit_body("smem");
+		o << "    __syncthreads();\n";
+		o << "  }\n";
+		o << "  if (timed_out) {\n";
+		o << "    if (threadIdx.x == 0) {\n";
+		o << "      atomicOr(err, VD_ERR_WAIT_TIMEOUT);\n";
+		o << "      for (int64_t j = i; j < i + " << S - 1 << "; j++) {\n";
+		o << "        if ((int64_t)blockIdx.x + j * (int64_t)gridDim.x < nfull) {\n";
+		o << "          vd::mbar_wait(&full[j % " << S << "], (uint32_t)((j / " << S << ") & 1), 100000000ull);\n";
+		o << "        }\n      }\n    }\n";
+		o << "    __syncthreads();\n";
+		o << "  } else if (nfull < ntiles && (int64_t)blockIdx.x == nfull % (int64_t)gridDim.x) {\n";
+		o << "    const int64_t t = nfull;\n";
+		emit_body("ldg");
+		o << "  }\n";
+	}
+
+	size_t tile_bytes_tx() {
+		size_t b = 0;
+		for (size_t c = 0; c < p.cols.size(); c++) {
+			if (eager[c]) {
+				b += (size_t)T * V * type_bytes(p.cols[c].type);
+			}
+		}
+		return b;
+	}
+
+	/* ------------------------------------------------------------ column phases ---- */
+
+	int compact_at = -1;              /* op index after which survivors are compacted */
+	std::vector<bool> eager;          /* column loaded with the tile (else gathered after compaction) */
+	std::vector<std::pair<int, int>> carried; /* (probe op, payload) values carried through compaction */
+
+	static void cols_of(const BExprP& e, std::vector<bool>& used) {
+		if (e->kind == BExpr::Col) {
+			used[e->col] = true;
+		}
+		for (auto& a : e->args) {
+			cols_of(a, used);
+		}
+	}
+	static void payloads_of(const BExprP& e, std::vector<std::pair<int, int>>& out) {
+		if (e->kind == BExpr::ProbeOut) {
+			std::pair<int, int> k(e->probe, e->pidx);
+			if (std::find(out.begin(), out.end(), k) == out.end()) {
+				out.push_back(k);
+			}
+		}
+		for (auto& a : e->args) {
+			payloads_of(a, out);
+		}
+	}
+	std::vector<BExprP> sink_exprs() {
+		std::vector<BExprP> r;
+		for (auto& k : p.sink.keys) r.push_back(k);
+		for (auto& k : p.sink.pay) r.push_back(k);
+		for (auto& a : p.sink.aggs) if (a.arg) r.push_back(a.arg);
+		for (auto& k : p.sink.outs) r.push_back(k);
+		return r;
+	}
+
+	void plan_phases() {
+		compact_at = fl.compact;
+		if (compact_at == -2) {
+			/* auto: after the first probe when more probes follow */
+			compact_at = -1;
+			for (size_t i = 0; i < p.ops.size(); i++) {
+				if (p.ops[i].kind == Op::Probe) {
+					for (size_t j = i + 1; j < p.ops.size(); j++) {
+						if (p.ops[j].kind == Op::Probe) {
+							compact_at = (int)i;
+						}
+					}
+					break;
+				}
+			}
+		}
+		if (compact_at >= (int)p.ops.size()) {
+			compact_at = -1;
+		}
+		eager.assign(p.cols.size(), compact_at < 0);
+		carried.clear();
+		if (compact_at < 0) {
+			return;
+		}
+		for (int i = 0; i <= compact_at; i++) {
+			const Op& op = p.ops[i];
+			if (op.pred) cols_of(op.pred, eager);
+			for (auto& k : op.keys) cols_of(k, eager);
+		}
+		std::vector<BExprP> later = sink_exprs();
+		for (size_t i = compact_at + 1; i < p.ops.size(); i++) {
+			if (p.ops[i].pred) later.push_back(p.ops[i].pred);
+			for (auto& k : p.ops[i].keys) later.push_back(k);
+		}
+		for (auto& e : later) {
+			payloads_of(e, carried);
+		}
+		carried.erase(std::remove_if(carried.begin(), carried.end(),
+			[&](const std::pair<int, int>& c) { return c.first > compact_at; }), carried.end());
+	}
+
+	void emit_decl_cols(bool only_eager, int rows) {
+		for (size_t c = 0; c < p.cols.size(); c++) {
+			if (only_eager && !eager[c]) {
+				continue;
+			}
+			o << "    " << ctype(p.cols[c].type) << " x" << c << "[" << rows << "];\n";
+		}
+	}
+
+	void emit_load_cols(const std::string& src, const std::string& dst, const std::string& r0) {
+		for (size_t c = 0; c < p.cols.size(); c++) {
+			if (!eager[c]) {
+				continue;
+			}
+			const char* ct = ctype(p.cols[c].type);
+			if (src == "smem") {
+				o << "    vd::load_rows_smem<" << ct << ", " << V << ">((const " << ct << "*)(stage + " << tile_region(c)
+				  << ") + threadIdx.x * " << V << ", " << dst << c << ");\n";
+			} else {
+				o << "    vd::load_rows<" << ct << ", " << V << ">(c" << c << ", " << r0 << ", n, " << dst << c << ");\n";
+			}
+		}
+	}
+
+	void emit_ops(int from, int to) {
+		for (int i = from; i < to; i++) {
 			const Op& op = p.ops[i];
 			if (op.kind == Op::Filter) {
 				o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) { act[v] = act[v] && "
 				  << expr(op.pred, "v") << "; }\n";
 			} else {
-				gen_probe((int)i, op);
+				gen_probe(i, op);
 			}
 		}
+	}
+
+	/* one tile's work for the tile index `t`: loads (mode "ldg", "smem" or "pre" = the
+	 * eager columns are already in x<c>), ops, sink */
+	void emit_body(const std::string& mode) {
+		o << "    {\n";
+		o << "    const int64_t r0 = t * tile + (int64_t)threadIdx.x * " << V << ";\n";
+		o << "    bool act[" << V << "];\n";
+		o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) { act[v] = r0 + v < n; }\n";
+		if (mode != "pre") {
+			emit_decl_cols(true, V);
+			emit_load_cols(mode, "x", "r0");
+		}
+		if (compact_at < 0) {
+			emit_ops(0, (int)p.ops.size());
+			sink_row();
+			o << "    }\n";
+			return;
+		}
+		emit_ops(0, compact_at + 1);
+		/* selection vector: survivors' tile offsets (and carried payloads) in shared memory */
+		o << "    const int nsel = vd::block_compact<" << V << ">(act, (int)(threadIdx.x * " << V
+		  << "), csel, cscan, csel_pos);\n";
+		for (size_t k = 0; k < carried.size(); k++) {
+			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) { if (act[v]) { ccar" << k
+			  << "[csel_pos[v]] = pay" << carried[k].first << "_" << carried[k].second << "[v]; } }\n";
+		}
+		o << "    __syncthreads();\n";
+		o << "    for (int base = 0; base < nsel; base += " << T << ") {\n";
+		o << "      const int ci = base + (int)threadIdx.x;\n";
+		o << "      const bool live = ci < nsel;\n";
+		o << "      const int64_t row = t * tile + (live ? csel[ci] : 0);\n";
+		const int saveV = V;
+		V = 1;
+		o << "      bool act[1] = {live};\n";
+		for (size_t c = 0; c < p.cols.size(); c++) {
+			const char* ct = ctype(p.cols[c].type);
+			o << "      " << ct << " x" << c << "[1] = {live ? vd::load_one(c" << c << ", row) : (" << ct << ")0};\n";
+		}
+		for (size_t k = 0; k < carried.size(); k++) {
+			o << "      int64_t pay" << carried[k].first << "_" << carried[k].second << "[1] = {live ? ccar" << k
+			  << "[ci] : 0};\n";
+		}
+		emit_ops(compact_at + 1, (int)p.ops.size());
 		sink_row();
-		o << "  }\n";
-		sink_epilogue();
-		o << "}\n\n";
-		return o.str();
+		V = saveV;
+		o << "    }\n";
+		o << "    __syncthreads();\n";
+		o << "    }\n";
+	}
+
+	/* shared-memory selection vector for compaction (declared once per kernel) */
+	void emit_compaction_smem() {
+		if (compact_at < 0) {
+			return;
+		}
+		o << "  __shared__ int csel[" << T * V << "];\n";
+		o << "  __shared__ int cscan[33];\n";
+		o << "  int csel_pos[" << V << "];\n";
+		for (size_t k = 0; k < carried.size(); k++) {
+			o << "  __shared__ int64_t ccar" << k << "[" << T * V << "];\n";
+		}
 	}
 
 	void gen_probe(int opi, const Op& op) {
@@ -186,15 +495,18 @@ struct PipeGen {
 		}
 		const std::string KT = jd.key64 ? "uint64_t" : "uint32_t";
 		const std::string PT = jd.pay64 ? "uint64_t" : "uint32_t";
-		const std::string S = "vd::JoinSlot<" + KT + ", " + PT + ">";
+		const std::string S = join_slot_type(jd);
 		const std::string j = std::to_string(opi);
 		for (int k = 0; k < op.npay; k++) {
 			o << "    int64_t pay" << j << "_" << k << "[" << V << "];\n";
 		}
 		o << "    {\n";
 		o << "      const " << S << "* __restrict__ jt = " << Pptr(jd.table, "const " + S + "*") << ";\n";
-		o << "      const uint64_t bmask = ((const unsigned long long*)" << Pptr(jd.words, "const void*")
-		  << ")[1];\n";
+		if (jd.direct) {
+			o << "      const uint64_t bmask = " << Pu(jd.direct_bmask) << ";\n";
+		} else {
+			o << "      const uint64_t bmask = ((const unsigned long long*)" << Pptr(jd.words, "const void*") << ")[1];\n";
+		}
 		o << "      int st[" << V << "]; uint64_t bk[" << V << "]; " << KT << " key[" << V << "]; " << PT
 		  << " raw[" << V << "];\n";
 		o << "#pragma unroll\n      for (int v = 0; v < " << V << "; v++) {\n";
@@ -203,13 +515,15 @@ struct PipeGen {
 		for (size_t k = 0; k < op.keys.size(); k++) {
 			const std::string kv = expr(op.keys[k], "v");
 			const std::string lo = P((unsigned long long)(int64_t)jd.key_b[k].lo);
-			const std::string hi = P((unsigned long long)(int64_t)jd.key_b[k].hi);
-			inrange += " && " + kv + " >= " + lo + " && " + kv + " <= " + hi;
+			const std::string span = Pu((unsigned long long)(int64_t)(jd.key_b[k].hi - jd.key_b[k].lo));
+			/* keys outside the build side's domain cannot match (and must not alias) */
+			inrange += " && (uint64_t)(" + kv + " - " + lo + ") <= " + span;
 			packed += " | ((uint64_t)(" + kv + " - " + lo + ") << " + P((unsigned long long)jd.key_shift[k]) + ")";
 		}
 		o << "        const bool ok = " << inrange << ";\n";
-		o << "        key[v] = (" << KT << ")((" << packed << ") + 1ull);\n";
-		o << "        bk[v] = " << key_hash(op.keys, "v") << " & bmask;\n";
+		o << "        const uint64_t pk = " << packed << ";\n";
+		o << "        key[v] = (" << KT << ")(pk + 1ull);\n";
+		o << "        bk[v] = " << table_hash(op.keys, "pk", jd.key_bits, "v") << " & bmask;\n";
 		o << "        raw[v] = 0; st[v] = 0;\n";
 		o << "        if (ok) { st[v] = vd::join_probe_bucket(jt, bk[v], key[v], raw[v]); }\n";
 		o << "      }\n";
@@ -234,7 +548,7 @@ struct PipeGen {
 
 	/* ------------------------------------------------------------ sinks ------------ */
 
-	void sink_prologue(size_t& smem) {
+	void sink_prologue() {
 		Sink& s = p.sink;
 		switch (s.kind) {
 		case Sink::AggGlobal:
@@ -243,27 +557,52 @@ struct PipeGen {
 			break;
 		case Sink::AggDense: {
 			const int64_t D = (int64_t)s.domain;
-			const bool in_smem = D * A() * 8 <= 96 * 1024;
-			if (in_smem) {
-				smem = (size_t)(D * A() * 8);
-				o << "  extern __shared__ __align__(16) unsigned char vd_smem[];\n";
-				o << "  unsigned long long* const sacc = (unsigned long long*)vd_smem;\n";
-				o << "  for (int64_t i = threadIdx.x; i < " << P((unsigned long long)(D * A()))
-				  << "; i += blockDim.x) { sacc[i] = 0ull; }\n";
+			const int64_t warps = T / 32;
+			replicas = fl.lowcard == "atomic" && D * A() * 8 * warps <= 96 * 1024 ? (int)warps : 1;
+			dense_in_smem = D * A() * 8 * replicas <= 96 * 1024;
+			if (dense_in_smem) {
+				smem_sink = (size_t)(D * A() * 8 * replicas);
+				o << "  unsigned long long* const sacc0 = (unsigned long long*)vd_smem;\n";
+				o << "  for (int64_t i = threadIdx.x; i < " << P((unsigned long long)(D * A() * replicas))
+				  << "; i += blockDim.x) { sacc0[i] = 0ull; }\n";
 				o << "  __syncthreads();\n";
+				if (replicas > 1) {
+					o << "  unsigned long long* const sacc = sacc0 + (threadIdx.x >> 5) * " << P((unsigned long long)(D * A()))
+					  << ";\n";
+				} else {
+					o << "  unsigned long long* const sacc = sacc0;\n";
+				}
 			} else {
-				o << "  unsigned long long* const sacc = " << Pptr(s_dev(), "unsigned long long*") << ";\n";
+				o << "  unsigned long long* const sacc = " << Pptr(st.sink_dev, "unsigned long long*") << ";\n";
 			}
-			dense_in_smem = in_smem;
+			/* per-thread private accumulators for up to kGmax slots seen by the block */
+			const size_t priv_bytes = (size_t)kGmax * A() * T * 8;
+			const size_t dict_bytes = ((size_t)D * 4 + 4 * (kGmax + 1) + 15) & ~(size_t)15;
+			private_acc = fl.lowcard == "private" && dense_in_smem && replicas == 1 &&
+				smem_sink + priv_bytes + dict_bytes <= 160 * 1024;
+			if (private_acc) {
+				const size_t priv_off = (smem_sink + 15) & ~(size_t)15;
+				const size_t dict_off = priv_off + priv_bytes;
+				smem_sink = dict_off + dict_bytes;
+				o << "  int64_t* const priv = (int64_t*)(vd_smem + " << priv_off << ");\n";
+				o << "  int* const pdict = (int*)(vd_smem + " << dict_off << ");\n";
+				o << "  int* const pcodes = pdict + " << P((unsigned long long)D) << ";\n";
+				o << "  int* const pncodes = pcodes + " << kGmax << ";\n";
+				o << "  for (int64_t i = threadIdx.x; i < " << P((unsigned long long)D)
+				  << "; i += blockDim.x) { pdict[i] = -1; }\n";
+				o << "  if (threadIdx.x == 0) { *pncodes = 0; }\n";
+				o << "#pragma unroll\n  for (int i = 0; i < " << kGmax * A() << "; i++) { priv[i * " << T
+				  << " + threadIdx.x] = 0; }\n";
+				o << "  __syncthreads();\n";
+			}
 			break;
 		}
 		case Sink::AggHash:
-			o << "  unsigned long long* const gtab = " << Pptr(s_dev(), "unsigned long long*") << ";\n";
-			o << "  const uint64_t gmask = " << Pu((unsigned long long)(s_cap() - 1)) << ";\n";
+			o << "  unsigned long long* const gtab = " << Pptr(st.sink_dev, "unsigned long long*") << ";\n";
+			o << "  const uint64_t gmask = " << Pu((unsigned long long)(st.sink_cap - 1)) << ";\n";
 			if (fl.aggr == "cache") {
 				const int S = (int)pow2_at_least(std::max(32, fl.cache_slots));
-				smem = (size_t)S * (1 + A()) * 8;
-				o << "  extern __shared__ __align__(16) unsigned char vd_smem[];\n";
+				smem_sink = (size_t)S * (1 + A()) * 8;
 				o << "  unsigned long long* const scache = (unsigned long long*)vd_smem;\n";
 				o << "  for (int i = threadIdx.x; i < " << S * (1 + A()) << "; i += blockDim.x) { scache[i] = 0ull; }\n";
 				o << "  __syncthreads();\n";
@@ -272,20 +611,38 @@ struct PipeGen {
 			break;
 		case Sink::JoinBuild: {
 			JoinDesc& jd = plan.joins[s.join];
-			o << "  unsigned long long* const words = " << Pptr(jd.words, "unsigned long long*") << ";\n";
-			o << "  " << (jd.key64 ? "uint64_t" : "uint32_t") << "* const skeys = "
-			  << Pptr(jd.stage_keys, jd.key64 ? "uint64_t*" : "uint32_t*") << ";\n";
-			o << "  " << (jd.pay64 ? "uint64_t" : "uint32_t") << "* const spay = "
-			  << Pptr(jd.stage_pay, jd.pay64 ? "uint64_t*" : "uint32_t*") << ";\n";
-			o << "  uint64_t* const shash = " << Pptr(stage_hash(jd), "uint64_t*") << ";\n";
+			const std::string S = join_slot_type(jd);
+			if (jd.direct) {
+				o << "  " << S << "* const jt = " << Pptr(jd.table, S + "*") << ";\n";
+				o << "  const uint64_t bmask = " << Pu(jd.direct_bmask) << ";\n";
+			} else {
+				o << "  __shared__ unsigned long long app[33];\n";
+				o << "  unsigned long long* const words = " << Pptr(jd.words, "unsigned long long*") << ";\n";
+				o << "  " << (jd.key64 ? "uint64_t" : "uint32_t") << "* const skeys = "
+				  << Pptr(jd.stage_keys, jd.key64 ? "uint64_t*" : "uint32_t*") << ";\n";
+				o << "  " << (jd.pay64 ? "uint64_t" : "uint32_t") << "* const spay = "
+				  << Pptr(jd.stage_pay, jd.pay64 ? "uint64_t*" : "uint32_t*") << ";\n";
+				o << "  uint64_t* const shash = " << Pptr(st.stage_hash, "uint64_t*") << ";\n";
+			}
 			break;
 		}
 		case Sink::Emit:
-			o << "  int64_t* const out = " << Pptr(plan_out, "int64_t*") << ";\n";
-			o << "  const int64_t ocap = " << P((unsigned long long)plan_out_cap) << ";\n";
-			o << "  unsigned long long* const ocount = " << Pptr(out_count(), "unsigned long long*") << ";\n";
+			o << "  __shared__ unsigned long long app[33];\n";
+			o << "  int64_t* const out = " << Pptr(qs.out, "int64_t*") << ";\n";
+			o << "  const int64_t ocap = " << P((unsigned long long)qs.out_cap) << ";\n";
+			o << "  unsigned long long* const ocount = " << Pptr(qs.out_count, "unsigned long long*") << ";\n";
 			break;
 		}
+	}
+
+	std::string packed_key(const std::vector<BExprP>& keys, const std::vector<Bounds>& b, const std::vector<int>& shift,
+		const std::string& v) {
+		std::string pk = "0ull";
+		for (size_t k = 0; k < keys.size(); k++) {
+			pk += " | ((uint64_t)(" + expr(keys[k], v) + " - " + P((unsigned long long)(int64_t)b[k].lo) + ") << " +
+				P((unsigned long long)shift[k]) + ")";
+		}
+		return pk;
 	}
 
 	void sink_row() {
@@ -306,24 +663,38 @@ struct PipeGen {
 			}
 			o << "      const int64_t slot = act[v] ? (" << slot << ") : 0;\n";
 			o << "      " << agg_vals("v") << "\n";
-			o << "      if (vd::warp_combine<" << A() << ">((uint64_t)slot, act[v], vals)) {\n";
+			if (private_acc) {
+				o << "      if (act[v]) {\n";
+				o << "        const int code = vd::dict_code(pdict, pcodes, pncodes, slot, " << kGmax << ");\n";
+				o << "        if (code >= 0) {\n";
+				o << "#pragma unroll\n          for (int a = 0; a < " << A() << "; a++) { priv[(code * " << A() << " + a) * "
+				  << T << " + threadIdx.x] += vals[a]; }\n";
+				o << "        } else {\n";
+				o << "#pragma unroll\n          for (int a = 0; a < " << A() << "; a++) { atomicAdd(&sacc[slot * " << A()
+				  << " + a], (unsigned long long)vals[a]); }\n";
+				o << "        }\n      }\n    }\n";
+				break;
+			}
+			if (replicas > 1) {
+				o << "      if (act[v]) {\n";
+			} else {
+				o << "      if (vd::warp_combine<" << A() << ">((uint64_t)slot, act[v], vals)) {\n";
+			}
 			o << "#pragma unroll\n        for (int a = 0; a < " << A() << "; a++) { atomicAdd(&sacc[slot * "
 			  << A() << " + a], (unsigned long long)vals[a]); }\n";
 			o << "      }\n    }\n";
 			break;
 		}
 		case Sink::AggHash: {
-			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
-			std::string packed = "0ull";
-			for (size_t k = 0; k < s.keys.size(); k++) {
-				packed += " | ((uint64_t)(" + expr(s.keys[k], "v") + " - " +
-					P((unsigned long long)(int64_t)s.keys[k]->b.lo) + ") << " +
-					P((unsigned long long)s.key_shift[k]) + ")";
+			std::vector<Bounds> kb;
+			for (auto& k : s.keys) {
+				kb.push_back(k->b);
 			}
-			o << "      const uint64_t pk = act[v] ? (" << packed << ") : 0ull;\n";
+			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
+			o << "      const uint64_t pk = act[v] ? (" << packed_key(s.keys, kb, s.key_shift, "v") << ") : 0ull;\n";
 			o << "      " << agg_vals("v") << "\n";
 			o << "      if (vd::warp_combine<" << A() << ">(pk, act[v], vals)) {\n";
-			o << "        const uint64_t h = " << key_hash(s.keys, "v") << ";\n";
+			o << "        const uint64_t h = " << table_hash(s.keys, "pk", s.key_bits, "v") << ";\n";
 			if (fl.aggr == "cache") {
 				o << "        if (!vd::cache_add<" << A() << ">(scache, " << cache_slots << ", h, pk + 1ull, vals)) {\n";
 				o << "          vd::group_add<" << A() << ">(gtab, gmask, h, pk + 1ull, vals, err);\n";
@@ -336,28 +707,30 @@ struct PipeGen {
 		}
 		case Sink::JoinBuild: {
 			JoinDesc& jd = plan.joins[s.join];
+			const std::string KT = jd.key64 ? "uint64_t" : "uint32_t";
+			const std::string PT = jd.pay64 ? "uint64_t" : "uint32_t";
 			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
-			o << "      const int64_t pos = vd::warp_append(&words[0], act[v]);\n";
-			o << "      if (act[v]) {\n";
-			std::string pk = "0ull";
-			for (size_t k = 0; k < s.keys.size(); k++) {
-				pk += " | ((uint64_t)(" + expr(s.keys[k], "v") + " - " + P((unsigned long long)(int64_t)jd.key_b[k].lo) +
-					") << " + P((unsigned long long)jd.key_shift[k]) + ")";
+			const std::string pk = packed_key(s.keys, jd.key_b, jd.key_shift, "v");
+			const std::string pp = s.pay.empty() ? std::string("0ull") : packed_key(s.pay, jd.pay_b, jd.pay_shift, "v");
+			if (jd.direct) {
+				o << "      if (act[v]) {\n";
+				o << "        const uint64_t pkb = " << pk << ";\n";
+				o << "        vd::join_insert(jt, bmask, " << table_hash(s.keys, "pkb", jd.key_bits, "v") << ", (" << KT
+				  << ")(pkb + 1ull), (" << PT << ")(" << pp << "), err);\n";
+				o << "      }\n    }\n";
+			} else {
+				o << "      const int64_t pos = vd::block_append(&words[0], act[v], app);\n";
+				o << "      if (act[v]) {\n";
+				o << "        const uint64_t pkb = " << pk << ";\n        skeys[pos] = (" << KT << ")(pkb + 1ull);\n";
+				o << "        spay[pos] = (" << PT << ")(" << pp << ");\n";
+				o << "        shash[pos] = " << table_hash(s.keys, "pkb", jd.key_bits, "v") << ";\n";
+				o << "      }\n    }\n";
 			}
-			std::string pp = "0ull";
-			for (size_t k = 0; k < s.pay.size(); k++) {
-				pp += " | ((uint64_t)(" + expr(s.pay[k], "v") + " - " + P((unsigned long long)(int64_t)jd.pay_b[k].lo) +
-					") << " + P((unsigned long long)jd.pay_shift[k]) + ")";
-			}
-			o << "        skeys[pos] = (" << (jd.key64 ? "uint64_t" : "uint32_t") << ")((" << pk << ") + 1ull);\n";
-			o << "        spay[pos] = (" << (jd.pay64 ? "uint64_t" : "uint32_t") << ")(" << pp << ");\n";
-			o << "        shash[pos] = " << key_hash(s.keys, "v") << ";\n";
-			o << "      }\n    }\n";
 			break;
 		}
 		case Sink::Emit: {
 			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
-			o << "      const int64_t pos = vd::warp_append(ocount, act[v]);\n";
+			o << "      const int64_t pos = vd::block_append(ocount, act[v], app);\n";
 			o << "      if (act[v]) {\n";
 			o << "        if (pos < ocap) {\n";
 			for (size_t c = 0; c < s.outs.size(); c++) {
@@ -370,28 +743,83 @@ struct PipeGen {
 		}
 	}
 
+	/* the last CTA writes the result rows of a global or dense aggregation */
+	void publish_slots(const std::string& g, int64_t nslots_val) {
+		Sink& s = p.sink;
+		o << "  __shared__ int last_flag;\n";
+		o << "  if (vd::last_block_done(" << Pptr(st.done, "unsigned long long*") << ", &last_flag)) {\n";
+		o << "    int64_t* const out = " << Pptr(qs.out, "int64_t*") << ";\n";
+		o << "    const int64_t ocap = " << P((unsigned long long)qs.out_cap) << ";\n";
+		o << "    unsigned long long* const ocount = " << Pptr(qs.out_count, "unsigned long long*") << ";\n";
+		o << "    const int64_t nslots = " << P((unsigned long long)nslots_val) << ";\n";
+		o << "    for (int64_t base = (threadIdx.x & ~31); base < nslots; base += blockDim.x) {\n";
+		o << "      const int64_t i = base + (threadIdx.x & 31);\n";
+		o << "      const bool take = i < nslots && (int64_t)__ldcg(&" << g << "[i * " << A() << " + " << s.count_idx
+		  << "]) > 0;\n";
+		o << "      const int64_t pos = vd::warp_append(ocount, take);\n";
+		o << "      if (take && pos < ocap) {\n";
+		int col = 0;
+		for (size_t k = 0; k < s.keys.size(); k++, col++) {
+			const int64_t range = (int64_t)(s.keys[k]->b.hi - s.keys[k]->b.lo + 1);
+			o << "        out[" << col << " * ocap + pos] = " << P((unsigned long long)(int64_t)s.keys[k]->b.lo)
+			  << " + (i / " << P((unsigned long long)s.key_radix[k]) << ") % " << P((unsigned long long)range) << ";\n";
+		}
+		for (int a = 0; a < A(); a++) {
+			if (!s.aggs[a].visible) {
+				continue;
+			}
+			o << "        out[" << col << " * ocap + pos] = (int64_t)__ldcg(&" << g << "[i * " << A() << " + " << a
+			  << "]);\n";
+			col++;
+		}
+		o << "      }\n    }\n  }\n";
+	}
+
 	void sink_epilogue() {
 		Sink& s = p.sink;
 		switch (s.kind) {
 		case Sink::AggGlobal:
 			o << "  __shared__ int64_t red[32 * " << A() << "];\n";
 			o << "  vd::block_sum<" << A() << ">(acc, red);\n";
+			o << "  unsigned long long* const g = " << Pptr(st.sink_dev, "unsigned long long*") << ";\n";
 			o << "  if (threadIdx.x == 0) {\n";
-			o << "    unsigned long long* g = " << Pptr(s_dev(), "unsigned long long*") << ";\n";
 			o << "#pragma unroll\n    for (int a = 0; a < " << A() << "; a++) { if (acc[a]) atomicAdd(&g[a], (unsigned long long)acc[a]); }\n";
 			o << "  }\n";
+			publish_slots("g", 1);
 			break;
 		case Sink::AggDense:
+			o << "  unsigned long long* const g = " << Pptr(st.sink_dev, "unsigned long long*") << ";\n";
+			if (private_acc) {
+				/* fold the private accumulators into the block's slot array: one warp per
+				 * (code, aggregate) pair, lanes striding over the threads' copies */
+				o << "  __syncthreads();\n";
+				o << "  {\n    const int ng = min(*pncodes, " << kGmax << ");\n";
+				o << "    for (int pr = (int)(threadIdx.x >> 5); pr < ng * " << A() << "; pr += (int)(blockDim.x >> 5)) {\n";
+				o << "      int64_t sum = 0;\n";
+				o << "      for (int t2 = (int)(threadIdx.x & 31); t2 < " << T << "; t2 += 32) { sum += priv[pr * " << T
+				  << " + t2]; }\n";
+				o << "#pragma unroll\n      for (int o2 = 16; o2 > 0; o2 >>= 1) { sum += (int64_t)__shfl_xor_sync(0xffffffffu, "
+				     "(unsigned long long)sum, o2); }\n";
+				o << "      if ((threadIdx.x & 31) == 0 && sum) { atomicAdd(&sacc[(int64_t)pcodes[pr / " << A() << "] * " << A()
+				  << " + pr % " << A() << "], (unsigned long long)sum); }\n";
+				o << "    }\n  }\n";
+			}
 			if (dense_in_smem) {
 				const int64_t D = (int64_t)s.domain;
 				o << "  __syncthreads();\n";
-				o << "  {\n    unsigned long long* g = " << Pptr(s_dev(), "unsigned long long*") << ";\n";
-				o << "    for (int64_t i = threadIdx.x; i < " << P((unsigned long long)D) << "; i += blockDim.x) {\n";
-				o << "      if (sacc[i * " << A() << " + " << s.count_idx << "]) {\n";
-				o << "#pragma unroll\n        for (int a = 0; a < " << A() << "; a++) { atomicAdd(&g[i * " << A()
-				  << " + a], sacc[i * " << A() << " + a]); }\n";
-				o << "      }\n    }\n  }\n";
+				o << "  for (int64_t i = threadIdx.x; i < " << P((unsigned long long)D) << "; i += blockDim.x) {\n";
+				o << "    unsigned long long sum[" << A() << "];\n";
+				o << "#pragma unroll\n    for (int a = 0; a < " << A() << "; a++) { sum[a] = 0ull; }\n";
+				o << "    for (int r = 0; r < " << replicas << "; r++) {\n";
+				o << "#pragma unroll\n      for (int a = 0; a < " << A() << "; a++) { sum[a] += sacc0[(r * "
+				  << P((unsigned long long)D) << " + i) * " << A() << " + a]; }\n";
+				o << "    }\n";
+				o << "    if (sum[" << s.count_idx << "]) {\n";
+				o << "#pragma unroll\n      for (int a = 0; a < " << A() << "; a++) { atomicAdd(&g[i * " << A()
+				  << " + a], sum[a]); }\n";
+				o << "    }\n  }\n";
 			}
+			publish_slots("g", (int64_t)s.domain);
 			break;
 		case Sink::AggHash:
 			if (fl.aggr == "cache") {
@@ -402,7 +830,6 @@ struct PipeGen {
 				o << "      int64_t vals[" << A() << "];\n";
 				o << "#pragma unroll\n      for (int a = 0; a < " << A() << "; a++) { vals[a] = (int64_t)scache[i * "
 				  << (1 + A()) << " + 1 + a]; }\n";
-				/* recompute the hash of the raw key values from the packed key */
 				o << "      const uint64_t pk = sk - 1ull;\n";
 				std::string h;
 				for (size_t k = 0; k < s.keys.size(); k++) {
@@ -411,6 +838,9 @@ struct PipeGen {
 					const std::string kv = "(" + P((unsigned long long)(int64_t)s.keys[k]->b.lo) + " + (int64_t)((pk >> " +
 						P((unsigned long long)s.key_shift[k]) + ") & " + Pu(mask) + "))";
 					h = k == 0 ? "vd::hash(" + kv + ")" : "vd::rehash(" + h + ", " + kv + ")";
+				}
+				if (fl.hash != "voila") {
+					h = s.key_bits <= 32 ? "vd::mix_hash32((uint32_t)pk)" : "vd::mix_hash64(pk)";
 				}
 				o << "      vd::group_add<" << A() << ">(gtab, gmask, " << h << ", sk, vals, err);\n";
 				o << "    }\n  }\n";
@@ -423,12 +853,12 @@ struct PipeGen {
 
 	/* ------------------------------------------------------------ extra kernels ---- */
 
-	/* join build: clear the table for the materialised count, then insert */
+	/* staged join build: clear the table for the materialised count, then insert */
 	std::string gen_join_build() {
 		JoinDesc& jd = plan.joins[p.sink.join];
 		const std::string KT = jd.key64 ? "uint64_t" : "uint32_t";
 		const std::string PT = jd.pay64 ? "uint64_t" : "uint32_t";
-		const std::string S = "vd::JoinSlot<" + KT + ", " + PT + ">";
+		const std::string S = join_slot_type(jd);
 		std::ostringstream k;
 		const std::string words = Pptr(jd.words, "unsigned long long*");
 		const std::string table = Pptr(jd.table, S + "*");
@@ -445,8 +875,8 @@ struct PipeGen {
 		k << "  " << S << "* const jt = " << table << ";\n";
 		k << "  const " << KT << "* const skeys = " << Pptr(jd.stage_keys, "const " + KT + "*") << ";\n";
 		k << "  const " << PT << "* const spay = " << Pptr(jd.stage_pay, "const " + PT + "*") << ";\n";
-		k << "  const uint64_t* const shash = " << Pptr(stage_hash(jd), "const uint64_t*") << ";\n";
-		k << "  unsigned* const err = (unsigned*)p.v[" << err_slot << "];\n";
+		k << "  const uint64_t* const shash = " << Pptr(st.stage_hash, "const uint64_t*") << ";\n";
+		k << "  unsigned* const err = (unsigned*)p.v[" << p.err_slot << "];\n";
 		k << "  const uint64_t cnt = words[0];\n";
 		k << "  const uint64_t bmask = vd::join_buckets<" << S << ">(cnt) - 1;\n";
 		k << "  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (uint64_t)gridDim.x * blockDim.x) {\n";
@@ -454,78 +884,57 @@ struct PipeGen {
 		return k.str();
 	}
 
-	/* group extraction: rows with count > 0, keys unpacked, visible aggregates */
+	/* hash-group extraction: rows with count > 0, keys unpacked, visible aggregates */
 	std::string gen_extract() {
 		Sink& s = p.sink;
 		std::ostringstream k;
 		k << "extern \"C\" __global__ void __launch_bounds__(256) " << name << "_extract(const VcParams p) {\n";
-		k << "  int64_t* const out = " << Pptr(plan_out, "int64_t*") << ";\n";
-		k << "  const int64_t ocap = " << P((unsigned long long)plan_out_cap) << ";\n";
-		k << "  unsigned long long* const ocount = " << Pptr(out_count(), "unsigned long long*") << ";\n";
-		k << "  const unsigned long long* const g = " << Pptr(s_dev(), "const unsigned long long*") << ";\n";
-		const int W = s.kind == Sink::AggHash ? 1 + A() : A();
-		const int off = s.kind == Sink::AggHash ? 1 : 0;
-		int64_t nslots = s.kind == Sink::AggGlobal ? 1 : s.kind == Sink::AggDense ? (int64_t)s.domain : s_cap();
-		k << "  const int64_t nslots = " << P((unsigned long long)nslots) << ";\n";
-		k << "  const int64_t stride = (int64_t)gridDim.x * blockDim.x;\n";
-		k << "  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < nslots; base += stride) {\n";
-		k << "    const int64_t i = base + (threadIdx.x & 31);\n";
-		k << "    bool take = false;\n";
-		k << "    if (i < nslots) {\n";
-		if (s.kind == Sink::AggHash) {
-			k << "      take = g[i * " << W << "] != 0ull && (int64_t)g[i * " << W << " + 1 + " << s.count_idx << "] > 0;\n";
-		} else {
-			k << "      take = (int64_t)g[i * " << W << " + " << s.count_idx << "] > 0;\n";
-		}
+		k << "  int64_t* const out = " << Pptr(qs.out, "int64_t*") << ";\n";
+		k << "  const int64_t ocap = " << P((unsigned long long)qs.out_cap) << ";\n";
+		k << "  unsigned long long* const ocount = " << Pptr(qs.out_count, "unsigned long long*") << ";\n";
+		k << "  const unsigned long long* const g = " << Pptr(st.sink_dev, "const unsigned long long*") << ";\n";
+		const int W = 1 + A();
+		k << "  const int64_t nslots = " << P((unsigned long long)st.sink_cap) << ";\n";
+		/* each warp covers kExtractK groups of 32 slots per step: all their key and count
+		 * words are loaded before any is used */
+		k << "  const int64_t stride = (int64_t)gridDim.x * blockDim.x * " << kExtractK << ";\n";
+		k << "  for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * " << kExtractK
+		  << "; base < nslots; base += stride) {\n";
+		k << "    unsigned long long kw[" << kExtractK << "]; long long cw[" << kExtractK << "];\n";
+		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
+		k << "      const int64_t i = base + q * 32 + (threadIdx.x & 31);\n";
+		k << "      kw[q] = i < nslots ? __ldcs(&g[i * " << W << "]) : 0ull;\n";
+		k << "      cw[q] = i < nslots ? (long long)__ldcs(&g[i * " << W << " + 1 + " << s.count_idx << "]) : 0;\n";
 		k << "    }\n";
+		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
+		k << "    const int64_t i = base + q * 32 + (threadIdx.x & 31);\n";
+		k << "    const bool take = kw[q] != 0ull && cw[q] > 0;\n";
 		k << "    const int64_t pos = vd::warp_append(ocount, take);\n";
 		k << "    if (take && pos < ocap) {\n";
 		int col = 0;
 		for (size_t kk = 0; kk < s.keys.size(); kk++, col++) {
 			const std::string lo = P((unsigned long long)(int64_t)s.keys[kk]->b.lo);
-			if (s.kind == Sink::AggDense) {
-				const int64_t range = (int64_t)(s.keys[kk]->b.hi - s.keys[kk]->b.lo + 1);
-				k << "      out[" << col << " * ocap + pos] = " << lo << " + (i / " << P((unsigned long long)s.key_radix[kk])
-				  << ") % " << P((unsigned long long)range) << ";\n";
-			} else {
-				const int bits = (kk + 1 < s.keys.size() ? s.key_shift[kk + 1] : s.key_bits) - s.key_shift[kk];
-				const unsigned long long mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
-				k << "      out[" << col << " * ocap + pos] = " << lo << " + (int64_t)(((g[i * " << W << "] - 1ull) >> "
-				  << P((unsigned long long)s.key_shift[kk]) << ") & " << Pu(mask) << ");\n";
-			}
+			const int bits = (kk + 1 < s.keys.size() ? s.key_shift[kk + 1] : s.key_bits) - s.key_shift[kk];
+			const unsigned long long mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
+			k << "      out[" << col << " * ocap + pos] = " << lo << " + (int64_t)(((kw[q] - 1ull) >> "
+			  << P((unsigned long long)s.key_shift[kk]) << ") & " << Pu(mask) << ");\n";
 		}
 		for (int a = 0; a < A(); a++) {
 			if (!s.aggs[a].visible) {
 				continue;
 			}
-			k << "      out[" << col << " * ocap + pos] = (int64_t)g[i * " << W << " + " << off + a << "];\n";
+			k << "      out[" << col << " * ocap + pos] = (int64_t)g[i * " << W << " + " << 1 + a << "];\n";
 			col++;
 		}
-		k << "    }\n  }\n}\n\n";
+		k << "    }\n    }\n  }\n}\n\n";
 		return k.str();
 	}
-
-	/* state accessors, set by the runtime before generation */
-	void* s_dev_ptr = nullptr;
-	int64_t s_cap_val = 0;
-	void* stage_hash_ptr = nullptr;
-	unsigned long long* out_count_ptr = nullptr;
-	void* plan_out = nullptr;
-	int64_t plan_out_cap = 0;
-	size_t err_slot = 1;
-	bool dense_in_smem = false;
-	int cache_slots = 0;
-
-	void* s_dev() { return s_dev_ptr; }
-	int64_t s_cap() { return s_cap_val; }
-	void* stage_hash(JoinDesc&) { return stage_hash_ptr; }
-	unsigned long long* out_count() { return out_count_ptr; }
 };
 
 } // namespace
 
 GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<PipeDeviceState>& st,
-	void* out, int64_t out_cap, unsigned long long* out_count, std::vector<std::vector<unsigned long long>>& params)
+	const QueryDeviceState& qs, std::vector<std::vector<unsigned long long>>& params)
 {
 	GeneratedCode gc;
 	std::ostringstream src;
@@ -533,19 +942,12 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 	params.assign(plan.pipes.size(), {});
 	for (auto& p : plan.pipes) {
 		auto& prm = params[p.id];
-		PipeGen g(p, plan, fl, prm);
-		g.s_dev_ptr = st[p.id].sink_dev;
-		g.s_cap_val = st[p.id].sink_cap;
-		g.stage_hash_ptr = st[p.id].stage_hash;
-		g.out_count_ptr = out_count;
-		g.plan_out = out;
-		g.plan_out_cap = out_cap;
-		size_t smem = 0;
-		std::string main = g.gen_main(smem);
+		PipeGen g(p, plan, fl, st[p.id], qs, prm);
+		std::string main = g.gen_main();
 		std::string extra;
-		if (p.sink.kind == Sink::JoinBuild) {
+		if (p.sink.kind == Sink::JoinBuild && !plan.joins[p.sink.join].direct) {
 			extra = g.gen_join_build();
-		} else if (p.sink.kind == Sink::AggGlobal || p.sink.kind == Sink::AggDense || p.sink.kind == Sink::AggHash) {
+		} else if (p.sink.kind == Sink::AggHash) {
 			extra = g.gen_extract();
 		}
 		src << "#define VcParams VcParams" << p.id << "\n";
@@ -557,13 +959,17 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 		m.kernel = g.name + "_main";
 		m.pipe = p.id;
 		m.stage = 0;
-		m.smem = smem;
+		m.smem = g.smem_total;
 		m.threads = fl.threads;
 		const int64_t tile = (int64_t)fl.threads * fl.rows;
-		m.grid_items = (p.rows + tile - 1) / tile;
+		m.grid_items = std::max<int64_t>((p.rows + tile - 1) / tile, 1);
 		m.dominant = p.id == plan.result_pipe;
-		if (p.sink.kind == Sink::JoinBuild) {
-			gc.launches.push_back(m);
+		if (p.sink.kind == Sink::AggGlobal || p.sink.kind == Sink::AggDense) {
+			/* the last-block publication needs every launched block to count itself */
+			m.grid_items = std::max<int64_t>(m.grid_items, 1);
+		}
+		gc.launches.push_back(m);
+		if (p.sink.kind == Sink::JoinBuild && !plan.joins[p.sink.join].direct) {
 			Launch c;
 			c.kernel = g.name + "_clear";
 			c.pipe = p.id;
@@ -575,19 +981,14 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 			ins.kernel = g.name + "_insert";
 			ins.stage = 2;
 			gc.launches.push_back(ins);
-		} else {
-			gc.launches.push_back(m);
-			if (p.sink.kind != Sink::Emit) {
-				Launch e;
-				e.kernel = g.name + "_extract";
-				e.pipe = p.id;
-				e.stage = 1;
-				e.threads = 256;
-				const int64_t nslots = p.sink.kind == Sink::AggGlobal ? 1
-					: p.sink.kind == Sink::AggDense ? (int64_t)p.sink.domain : st[p.id].sink_cap;
-				e.grid_items = (nslots + 255) / 256;
-				gc.launches.push_back(e);
-			}
+		} else if (p.sink.kind == Sink::AggHash) {
+			Launch e;
+			e.kernel = g.name + "_extract";
+			e.pipe = p.id;
+			e.stage = 1;
+			e.threads = 256;
+			e.grid_items = (st[p.id].sink_cap + 256 * 4 - 1) / (256 * 4);
+			gc.launches.push_back(e);
 		}
 	}
 	gc.source = src.str();

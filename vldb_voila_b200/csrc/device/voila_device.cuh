@@ -63,6 +63,34 @@ __device__ __forceinline__ uint64_t rehash(uint64_t h, int64_t v)
 	return hash(v) ^ (h * 2654435761ull);
 }
 
+/* Table hash of a bit-packed key (flavor hash=mix): the 32-bit finalizer of MurmurHash3
+ * (A. Appleby, public domain) for keys of up to 32 bits and the SplitMix64 output function
+ * for wider ones.  Both avalanche into the low bits that index the tables and use 32-bit
+ * multiplies where they can.  Table positions never reach results, so this cheaper hash
+ * may replace voila_hash; both sides of a table use the same one. */
+__device__ __forceinline__ uint64_t mix_hash32(uint32_t h)
+{
+	h ^= h >> 16;
+	h *= 0x85ebca6bu;
+	h ^= h >> 13;
+	h *= 0xc2b2ae35u;
+	h ^= h >> 16;
+	return (uint64_t)h;
+}
+
+__device__ __forceinline__ uint64_t mix_hash64(uint64_t z)
+{
+	z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+	z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+	return z ^ (z >> 31);
+}
+
+/* product of two values whose ranges fit int32, as one 32x32->64 multiply */
+__device__ __forceinline__ int64_t mulw(int64_t a, int64_t b)
+{
+	return (int64_t)(int32_t)a * (int64_t)(int32_t)b;
+}
+
 /* ---------------------------------------------------------------- loads ---------- */
 
 /* Loads rows [r0, r0+V) of a column into registers.  Whole tiles use vector loads through
@@ -116,6 +144,115 @@ __device__ __forceinline__ T load_one(const T* __restrict__ col, int64_t row)
 	return __ldg(col + row);
 }
 
+/* Reads this thread's V consecutive rows of a column tile staged in shared memory. */
+template <typename T, int V>
+__device__ __forceinline__ void load_rows_smem(const T* s, T (&out)[V])
+{
+	constexpr int bytes = V * (int)sizeof(T);
+	if constexpr (bytes % 16 == 0) {
+#pragma unroll
+		for (int i = 0; i < bytes / 16; i++) {
+			const uint4 tmp = reinterpret_cast<const uint4*>(s)[i];
+#pragma unroll
+			for (int j = 0; j < 16 / (int)sizeof(T); j++) {
+				out[i * (16 / (int)sizeof(T)) + j] = reinterpret_cast<const T*>(&tmp)[j];
+			}
+		}
+	} else if constexpr (bytes == 8) {
+		const uint2 tmp = *reinterpret_cast<const uint2*>(s);
+#pragma unroll
+		for (int i = 0; i < V; i++) {
+			out[i] = reinterpret_cast<const T*>(&tmp)[i];
+		}
+	} else if constexpr (bytes == 4) {
+		const unsigned int tmp = *reinterpret_cast<const unsigned int*>(s);
+#pragma unroll
+		for (int i = 0; i < V; i++) {
+			out[i] = reinterpret_cast<const T*>(&tmp)[i];
+		}
+	} else {
+#pragma unroll
+		for (int i = 0; i < V; i++) {
+			out[i] = s[i];
+		}
+	}
+}
+
+/* ---------------------------------------------------------------- TMA staging ---- */
+
+/*
+ * Column tiles are staged into shared memory with bulk asynchronous copies (the untiled
+ * cp.async.bulk form of TMA; no cluster multicast) that complete on an mbarrier.  One
+ * thread issues copies S-1 tiles ahead of the tile the block is working on, so HBM
+ * streaming overlaps the dependent hash-table loads of the current tile.
+ */
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+	return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence()
+{
+	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+		: "memory");
+}
+
+/* generic-proxy reads of a stage are ordered before the async-proxy refill of it */
+__device__ __forceinline__ void fence_proxy_async()
+{
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+/* global -> shared bulk copy; dst, src 16-byte aligned, bytes a multiple of 16 */
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+		::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+		: "memory");
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns()
+{
+	uint64_t t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
+/* Waits for the barrier's phase with the given parity.  Gives up after `limit_ns` of
+ * wall time (returns false) instead of spinning forever. */
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns = 2000000000ull)
+{
+	const uint32_t a = smem_addr(bar);
+	uint64_t start = 0;
+	for (uint32_t it = 0;; it++) {
+		uint32_t done;
+		asm volatile(
+			"{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+			: "=r"(done)
+			: "r"(a), "r"(parity)
+			: "memory");
+		if (done) {
+			return true;
+		}
+		if (it == 0) {
+			start = globaltimer_ns();
+		} else if ((it & 63u) == 0 && globaltimer_ns() - start > limit_ns) {
+			return false;
+		}
+	}
+}
+
 /* ---------------------------------------------------------------- warp helpers --- */
 
 __device__ __forceinline__ unsigned lane_id()
@@ -163,6 +300,128 @@ __device__ __forceinline__ int64_t warp_append(unsigned long long* cursor, bool 
 	}
 	base = __shfl_sync(0xffffffffu, base, leader);
 	return (int64_t)base + __popc(mask & ((1u << lane) - 1u));
+}
+
+/* Block-aggregated append: one atomic per block and call.  All threads of the block must
+ * call it; `scratch` holds at least 33 words of shared memory. */
+__device__ __forceinline__ int64_t block_append(unsigned long long* cursor, bool take, unsigned long long* scratch)
+{
+	const unsigned mask = __ballot_sync(0xffffffffu, take);
+	const unsigned lane = lane_id(), warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+	if (lane == 0) {
+		scratch[warp] = __popc(mask);
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		unsigned long long total = 0;
+		for (unsigned w = 0; w < nw; w++) {
+			const unsigned long long c = scratch[w];
+			scratch[w] = total;
+			total += c;
+		}
+		scratch[32] = total ? atomicAdd(cursor, total) : 0ull;
+	}
+	__syncthreads();
+	const int64_t pos = (int64_t)(scratch[32] + scratch[warp]) + __popc(mask & ((1u << lane) - 1u));
+	__syncthreads();
+	return pos;
+}
+
+/* Selection vector of the block's active rows (seltrue + compaction, kernel_generator.py
+ * :617-631): every thread passes its V row flags and its first row's tile offset; active
+ * rows get consecutive positions pos[v] (-1 otherwise) and sel[pos] = tile offset.  Returns
+ * the number of active rows.  All threads call it; `scan` holds 33 ints of shared memory. */
+template <int V>
+__device__ __forceinline__ int block_compact(const bool (&act)[V], int off, int* sel, int* scan, int (&pos)[V])
+{
+	int cnt = 0;
+#pragma unroll
+	for (int v = 0; v < V; v++) {
+		cnt += act[v] ? 1 : 0;
+	}
+	const unsigned lane = lane_id(), warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+	int x = cnt;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const int y = __shfl_up_sync(0xffffffffu, x, o);
+		if ((int)lane >= o) {
+			x += y;
+		}
+	}
+	if (lane == 31) {
+		scan[warp] = x;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		int run = 0;
+		for (unsigned w = 0; w < nw; w++) {
+			const int c = scan[w];
+			scan[w] = run;
+			run += c;
+		}
+		scan[32] = run;
+	}
+	__syncthreads();
+	int base = scan[warp] + x - cnt;
+#pragma unroll
+	for (int v = 0; v < V; v++) {
+		if (act[v]) {
+			pos[v] = base;
+			sel[base] = off + v;
+			base++;
+		} else {
+			pos[v] = -1;
+		}
+	}
+	return scan[32];
+}
+
+/* Block dictionary of group slots for per-thread private accumulators: returns the dense
+ * code (< gmax) of `slot`, assigning the next code on first sight, or -1 when the block has
+ * run out of codes (or another thread's assignment did not become visible within a bounded
+ * wait); the caller then falls back to shared-memory atomics, so results never depend on it.
+ * dict holds -1 (unseen), -2 (being assigned), -3 (no code) or the code. */
+__device__ __forceinline__ int dict_code(int* dict, int* codes, int* ncodes, int64_t slot, int gmax)
+{
+	int c = *(volatile int*)&dict[slot];
+	if (c >= 0) {
+		return c;
+	}
+	if (c == -1) {
+		const int old = atomicCAS(&dict[slot], -1, -2);
+		if (old == -1) {
+			const int k = atomicAdd(ncodes, 1);
+			const int code = k < gmax ? k : -3;
+			if (k < gmax) {
+				codes[k] = (int)slot;
+			}
+			__threadfence_block();
+			atomicExch(&dict[slot], code);
+			return code >= 0 ? code : -1;
+		}
+		c = old;
+	}
+	for (int spin = 0; c == -2 && spin < 1024; spin++) {
+		c = *(volatile int*)&dict[slot];
+	}
+	return c >= 0 ? c : -1;
+}
+
+/* True in every thread of the block that finishes last (all blocks call it once, after
+ * their global updates); that block then publishes the final result. */
+__device__ __forceinline__ bool last_block_done(unsigned long long* counter, int* flag_smem)
+{
+	__threadfence();
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		*flag_smem = atomicAdd(counter, 1ull) == (unsigned long long)(gridDim.x - 1);
+	}
+	__syncthreads();
+	const bool last = *flag_smem != 0;
+	if (last) {
+		__threadfence();
+	}
+	return last;
 }
 
 /* Block-wide int64 sum (all threads call; result valid in every thread). */
@@ -272,18 +531,18 @@ __device__ __forceinline__ bool join_insert(JoinSlot<KeyT, PayT>* __restrict__ s
 		JoinSlot<KeyT, PayT>* bucket = slots + b * SPB;
 #pragma unroll
 		for (int s = 0; s < SPB; s++) {
+			/* CAS first: one round trip when the slot is free; a failed CAS observes the
+			 * occupant like a read would, and occupied slots stay a prefix of the bucket */
 			KeyT* kp = &bucket[s].key;
-			if (*(volatile KeyT*)kp == 0) {
-				KeyT prev;
-				if (sizeof(KeyT) == 4) {
-					prev = (KeyT)atomicCAS((unsigned int*)kp, 0u, (unsigned int)key);
-				} else {
-					prev = (KeyT)atomicCAS((unsigned long long*)kp, 0ull, (unsigned long long)key);
-				}
-				if (prev == 0) {
-					bucket[s].pay = pay;
-					return true;
-				}
+			KeyT prev;
+			if constexpr (sizeof(KeyT) == 4) {
+				prev = (KeyT)atomicCAS((unsigned int*)kp, 0u, (unsigned int)key);
+			} else {
+				prev = (KeyT)atomicCAS((unsigned long long*)kp, 0ull, (unsigned long long)key);
+			}
+			if (prev == 0) {
+				bucket[s].pay = pay;
+				return true;
 			}
 		}
 		b = (b + 1) & bucket_mask;

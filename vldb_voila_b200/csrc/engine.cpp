@@ -39,7 +39,16 @@ static int64_t pow2_at_least(int64_t x)
 std::string Flavor::str() const
 {
 	std::ostringstream o;
-	o << "cuda(threads=" << threads << ",rows=" << rows << ",aggr=" << aggr << ",cache=" << cache_slots
+	o << "cuda(threads=" << threads << ",rows=" << rows << ",load=" << load;
+	if (load == "tma") {
+		o << ",stages=" << stages;
+	}
+	else {
+		o << ",prefetch=" << (prefetch ? 1 : 0);
+	}
+	o << ",compact=" << (compact == -2 ? std::string("auto") : std::to_string(compact));
+	o << ",aggr=" << aggr << ",lowcard=" << lowcard << ",hash=" << hash << ",fill=" << fill << ",cache=" << cache_slots
+	  << ",build=" << build
 	  << ",grid=" << grid << ",dense=" << dense_limit << ",graph=" << (graph ? 1 : 0) << ")";
 	return o.str();
 }
@@ -104,6 +113,34 @@ Flavor Flavor::parse(const std::string& s0)
 			f.dense_limit = num(1, 1 << 22);
 		} else if (k == "graph") {
 			f.graph = num(0, 1) != 0;
+		} else if (k == "load") {
+			if (v != "ldg" && v != "tma") {
+				throw Error(1, "load must be ldg or tma");
+			}
+			f.load = v;
+		} else if (k == "stages") {
+			f.stages = num(2, 8);
+		} else if (k == "prefetch") {
+			f.prefetch = num(0, 1) != 0;
+		} else if (k == "compact") {
+			f.compact = v == "auto" ? -2 : num(-1, 64);
+		} else if (k == "lowcard") {
+			if (v != "combine" && v != "atomic" && v != "private") {
+				throw Error(1, "lowcard must be combine, atomic or private");
+			}
+			f.lowcard = v;
+		} else if (k == "hash") {
+			if (v != "mix" && v != "voila") {
+				throw Error(1, "hash must be mix or voila");
+			}
+			f.hash = v;
+		} else if (k == "fill") {
+			f.fill = num(10, 90);
+		} else if (k == "build") {
+			if (v != "auto" && v != "direct" && v != "staged") {
+				throw Error(1, "build must be auto, direct or staged");
+			}
+			f.build = v;
 		} else {
 			throw Error(1, "unknown flavor knob '" + k + "'");
 		}
@@ -189,10 +226,21 @@ void query_prepare(Query& q)
 	QueryState& st = state_of(q);
 	st.pipes.assign(plan.pipes.size(), PipeDeviceState());
 
-	q.err = (unsigned*)dev_alloc(q, 256);
-	q.out_count = (unsigned long long*)dev_alloc(q, 256);
-	st.memsets.push_back({q.err, 256});
-	st.memsets.push_back({q.out_count, 256});
+	/* Small per-run state (error word, result count, last-block counters, join counters,
+	 * global and small dense accumulators) lives in one arena cleared by one memset. */
+	const size_t arena_cap = 1 << 20;
+	char* arena = (char*)dev_alloc(q, arena_cap);
+	size_t arena_used = 0;
+	auto arena_take = [&](size_t bytes) -> void* {
+		size_t off = (arena_used + 255) & ~(size_t)255;
+		if (off + bytes > arena_cap) {
+			return nullptr;
+		}
+		arena_used = off + bytes;
+		return arena + off;
+	};
+	q.err = (unsigned*)arena_take(8);
+	q.out_count = (unsigned long long*)arena_take(8);
 
 	for (auto& jd : plan.joins) {
 		const int64_t rows = std::max<int64_t>(jd.build_rows, 1);
@@ -200,19 +248,29 @@ void query_prepare(Query& q)
 		const int spb = std::max(1, 32 / sb);
 		const int64_t slots = std::max<int64_t>(pow2_at_least(2 * rows), 2 * spb);
 		jd.max_buckets = slots / spb;
-		jd.table = dev_alloc(q, (size_t)slots * sb);
-		jd.stage_keys = dev_alloc(q, (size_t)rows * (jd.key64 ? 8 : 4));
-		jd.stage_pay = dev_alloc(q, (size_t)rows * (jd.pay64 ? 8 : 4));
-		jd.words = (unsigned long long*)dev_alloc(q, 256);
-		st.memsets.push_back({jd.words, 256});
+		jd.table_bytes = (size_t)slots * sb;
+		const std::string& bm = q.flavor.build;
+		jd.direct = bm == "direct" || (bm == "auto" && (int64_t)jd.table_bytes <= q.flavor.direct_limit);
+		jd.direct_bmask = (uint64_t)(jd.max_buckets - 1);
+		jd.table = dev_alloc(q, jd.table_bytes);
+		jd.words = (unsigned long long*)arena_take(32);
+		if (jd.direct) {
+			st.memsets.push_back({jd.table, jd.table_bytes});
+		} else {
+			jd.stage_keys = dev_alloc(q, (size_t)rows * (jd.key64 ? 8 : 4));
+			jd.stage_pay = dev_alloc(q, (size_t)rows * (jd.pay64 ? 8 : 4));
+		}
 	}
 	Pipeline& rp = plan.pipes[plan.result_pipe];
 	for (auto& p : plan.pipes) {
 		PipeDeviceState& ps = st.pipes[p.id];
 		const int A = (int)p.sink.aggs.size();
+		ps.done = (unsigned long long*)arena_take(8);
 		switch (p.sink.kind) {
 		case Sink::JoinBuild:
-			ps.stage_hash = dev_alloc(q, (size_t)std::max<int64_t>(plan.joins[p.sink.join].build_rows, 1) * 8);
+			if (!plan.joins[p.sink.join].direct) {
+				ps.stage_hash = dev_alloc(q, (size_t)std::max<int64_t>(plan.joins[p.sink.join].build_rows, 1) * 8);
+			}
 			break;
 		case Sink::AggGlobal:
 			ps.sink_cap = 1;
@@ -223,17 +281,22 @@ void query_prepare(Query& q)
 			ps.sink_bytes = (size_t)p.sink.domain * A * 8;
 			break;
 		case Sink::AggHash:
-			ps.sink_cap = std::max<int64_t>(pow2_at_least(2 * std::max<int64_t>(p.sink.groups_bound, 1)), 1024);
+			ps.sink_cap = std::max<int64_t>(
+				pow2_at_least((std::max<int64_t>(p.sink.groups_bound, 1) * 100 + q.flavor.fill - 1) / q.flavor.fill), 1024);
 			ps.sink_bytes = (size_t)ps.sink_cap * (1 + A) * 8;
 			break;
 		case Sink::Emit:
 			break;
 		}
 		if (ps.sink_bytes) {
-			ps.sink_dev = dev_alloc(q, ps.sink_bytes);
-			st.memsets.push_back({ps.sink_dev, ps.sink_bytes});
+			ps.sink_dev = ps.sink_bytes <= (64 << 10) ? arena_take(ps.sink_bytes) : nullptr;
+			if (!ps.sink_dev) {
+				ps.sink_dev = dev_alloc(q, ps.sink_bytes);
+				st.memsets.push_back({ps.sink_dev, ps.sink_bytes});
+			}
 		}
 	}
+	st.memsets.insert(st.memsets.begin(), {arena, arena_used});
 	switch (rp.sink.kind) {
 	case Sink::AggGlobal: q.out_cap = 1; break;
 	case Sink::AggDense: q.out_cap = (int64_t)rp.sink.domain; break;
@@ -241,7 +304,11 @@ void query_prepare(Query& q)
 	}
 	q.out = (int64_t*)dev_alloc(q, (size_t)q.out_cap * plan.result_cols * 8);
 
-	q.code = generate_cuda(plan, q.flavor, st.pipes, q.out, q.out_cap, q.out_count, q.params);
+	QueryDeviceState qs;
+	qs.out = q.out;
+	qs.out_cap = q.out_cap;
+	qs.out_count = q.out_count;
+	q.code = generate_cuda(plan, q.flavor, st.pipes, qs, q.params);
 	std::string log;
 	if (e.offline) {
 		jit_cubin(q.code.source, &log);
@@ -254,7 +321,8 @@ void query_prepare(Query& q)
 	for (auto& l : q.code.launches) {
 		cudaKernel_t k;
 		VC_CHECK_CUDA(cudaLibraryGetKernel(&k, q.mod->lib, l.kernel.c_str()));
-		if (l.smem > 48 * 1024) {
+		if (l.smem > 0) {
+			/* static + dynamic shared memory above 48 KiB needs the opt-in */
 			VC_CHECK_CUDA(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem));
 		}
 		int occ = 0;
@@ -292,7 +360,7 @@ static void refresh_column_params(Query& q)
 	}
 }
 
-static void launch_all(Query& q, cudaStream_t stream)
+static void launch_all(Query& q, cudaStream_t stream, bool capturing = false)
 {
 	QueryState& st = state_of(q);
 	for (auto& m : st.memsets) {
@@ -319,12 +387,12 @@ static void launch_all(Query& q, cudaStream_t stream)
 		grid = std::max<int64_t>(grid, 1);
 		void* args[] = {q.params[l.pipe].data()};
 		if (q.profile) {
-			VC_CHECK_CUDA(cudaEventRecord(q.ev[2 * i], stream));
+			VC_CHECK_CUDA(cudaEventRecordWithFlags(q.ev[2 * i], stream, capturing ? cudaEventRecordExternal : 0));
 		}
 		VC_CHECK_CUDA(cudaLaunchKernel((const void*)st.kernels[i], dim3((unsigned)grid), dim3((unsigned)l.threads), args,
 			l.smem, stream));
 		if (q.profile) {
-			VC_CHECK_CUDA(cudaEventRecord(q.ev[2 * i + 1], stream));
+			VC_CHECK_CUDA(cudaEventRecordWithFlags(q.ev[2 * i + 1], stream, capturing ? cudaEventRecordExternal : 0));
 		}
 	}
 }
@@ -360,7 +428,7 @@ void query_launch(Query& q, cudaStream_t stream)
 			cudaGraph_t g;
 			VC_CHECK_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
 			try {
-				launch_all(q, cs);
+				launch_all(q, cs, true);
 			} catch (...) {
 				cudaStreamEndCapture(cs, &g);
 				cudaStreamDestroy(cs);

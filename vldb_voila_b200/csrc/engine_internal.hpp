@@ -122,6 +122,9 @@ struct JoinDesc {
 	void* stage_pay = nullptr;       /* materialised packed payloads */
 	unsigned long long* words = nullptr; /* [0] materialised count, [1] bucket mask */
 	int64_t max_buckets = 0;
+	bool direct = false;             /* build inserts directly into a table sized for build_rows */
+	uint64_t direct_bmask = 0;       /* bucket mask of the direct table */
+	size_t table_bytes = 0;
 	int slot_bytes() const { return (key64 || pay64) ? 16 : 8; }
 };
 
@@ -181,6 +184,16 @@ struct Flavor {
 	int grid = 0;             /* CTAs per SM (0 = occupancy) */
 	int dense_limit = 4096;   /* largest dense key domain */
 	bool graph = true;        /* replay the query's launches from a CUDA graph */
+	std::string load = "ldg"; /* column tiles: ldg (vector loads) | tma (bulk copies into a smem ring) */
+	int stages = 4;           /* tma ring depth */
+	std::string build = "auto"; /* join build: auto | direct | staged */
+	bool prefetch = true;     /* ldg: load the next tile while the current one is processed */
+	int compact = -2;         /* compact survivors after op k (-1 never, -2 auto) */
+	std::string lowcard = "combine"; /* dense aggregation: combine (warp pre-sum) | atomic (per-warp replicas)
+	                                  * | private (per-thread accumulators behind a block dictionary) */
+	std::string hash = "mix"; /* table positions: mix (finalizer of the packed key) | voila (runtime.hpp hash) */
+	int fill = 50;            /* largest load factor (percent) of group tables */
+	int64_t direct_limit = 64ll << 20; /* auto: direct when the upper-bound table fits this many bytes */
 
 	std::string str() const;
 	static Flavor parse(const std::string& s);
@@ -217,14 +230,22 @@ struct GeneratedCode {
 
 /* device state of one pipeline's sink, allocated before code generation */
 struct PipeDeviceState {
-	void* sink_dev = nullptr;
+	void* sink_dev = nullptr;            /* aggregation state (global sums, dense slots, group table) */
 	int64_t sink_cap = 0;
 	size_t sink_bytes = 0;
-	void* stage_hash = nullptr;
+	void* stage_hash = nullptr;          /* staged join build: materialised hashes */
+	unsigned long long* done = nullptr;  /* last-block counter */
 };
 
-GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<PipeDeviceState>& st, void* out,
-	int64_t out_cap, unsigned long long* out_count, std::vector<std::vector<unsigned long long>>& params);
+/* query-wide device state the generated kernels write to */
+struct QueryDeviceState {
+	int64_t* out = nullptr;              /* result_cols x out_cap, column-major */
+	int64_t out_cap = 0;
+	unsigned long long* out_count = nullptr;
+};
+
+GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<PipeDeviceState>& st,
+	const QueryDeviceState& qs, std::vector<std::vector<unsigned long long>>& params);
 
 /* ------------------------------------------------------------------ JIT ---------------- */
 

@@ -161,6 +161,36 @@ int vc_query_source(vc_query* q, char* buf, size_t cap, size_t* len);
 /* Per-launch device times of the last run, in launch order (enable first with
  * vc_query_profile).  `names` receives kernel names separated by '\n'. */
 int vc_query_profile(vc_query* q, int enable);
+
+/* Runs the query `reps` times on `stream` and stores each run's device time (CUDA events
+ * around the run) in ms_out[0..reps); with flush_l2 a 256 MiB buffer is written before every
+ * run so inputs come from HBM.  The timing primitive of the autotuner (the reference's
+ * timed hot repetitions, compiler.cpp:521-575). */
+int vc_query_time(vc_query* q, int reps, int flush_l2, void* stream, float* ms_out, int cap);
+
+/* ---------------------------------------------------------------- flavor chooser ------ */
+
+/* A small multi-layer perceptron (in -> hidden -> hidden -> out, ReLU), trained and run on
+ * the GPU by the library's own kernels.  It maps a pipeline's features to the predicted
+ * relative time of every candidate flavor; the caller picks the argmin.  It stands beside
+ * the exhaustive search over blends that the reference's explorer performs
+ * (explorer.cpp:111-134, :352-426), which remains the fallback and judge. */
+typedef struct vc_mlp vc_mlp;
+
+/* Glorot-uniform weights from `seed`, zero biases. */
+int vc_mlp_create(int device, int n_in, int n_hidden, int n_out, uint64_t seed, vc_mlp** out);
+int vc_mlp_free(vc_mlp* m);
+int vc_mlp_num_params(vc_mlp* m, int64_t* n);
+/* Parameters flattened as W1[in][hidden], b1, W2[hidden][hidden], b2, W3[hidden][out], b3. */
+int vc_mlp_get_params(vc_mlp* m, float* out, int64_t cap);
+int vc_mlp_set_params(vc_mlp* m, const float* in, int64_t n);
+/* Masked mean squared error of (X[n][in] -> targets T[n][out]) and its gradient with respect
+ * to every parameter (same layout as the parameters).  mask may be NULL (all ones). */
+int vc_mlp_loss_grad(vc_mlp* m, const float* X, const float* T, const float* mask, int n, float* loss, float* grads);
+/* Adam training, shuffled mini-batches; *final_loss = loss over all n samples after training. */
+int vc_mlp_train(vc_mlp* m, const float* X, const float* T, const float* mask, int n, int epochs, int batch, float lr,
+	uint64_t seed, float* final_loss);
+int vc_mlp_predict(vc_mlp* m, const float* X, int n, float* Y);
 int vc_query_timings(vc_query* q, float* ms, int cap, int* n, char* names, size_t names_cap);
 
 #ifdef __cplusplus

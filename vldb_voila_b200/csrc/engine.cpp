@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cinttypes>
 #include <cstring>
+#include <functional>
 #include <sstream>
 
 #include "engine_internal.hpp"
@@ -541,6 +542,14 @@ static int guarded(F&& f)
 	}
 }
 
+namespace vc {
+/* status-code guard shared with the other translation units of the C ABI */
+int abi_guard_mlp(const std::function<void()>& f)
+{
+	return guarded(f);
+}
+} // namespace vc
+
 static int copy_out(const std::string& s, char* buf, size_t cap, size_t* len)
 {
 	if (len) {
@@ -1000,6 +1009,44 @@ int vc_query_source(vc_query* q, char* buf, size_t cap, size_t* len)
 			throw Error(VC_ERR_INVALID, "null query");
 		}
 		copy_out(q->q.code.source, buf, cap, len);
+	});
+}
+
+int vc_query_time(vc_query* q, int reps, int flush_l2, void* stream, float* ms_out, int cap)
+{
+	return guarded([&] {
+		if (!q || reps < 1 || !ms_out || cap < reps) {
+			throw Error(VC_ERR_INVALID, "bad arguments");
+		}
+		Query& qq = q->q;
+		if (qq.eng->offline) {
+			throw Error(VC_ERR_NO_DEVICE, "an offline engine only generates and compiles code");
+		}
+		VC_CHECK_CUDA(cudaSetDevice(qq.eng->device));
+		cudaStream_t s = (cudaStream_t)stream;
+		static thread_local void* flush = nullptr;
+		static thread_local int flush_dev = -1;
+		const size_t flush_bytes = 256ull << 20; /* larger than the 126 MiB L2 */
+		if (flush_l2 && (flush == nullptr || flush_dev != qq.eng->device)) {
+			VC_CHECK_CUDA(cudaMalloc(&flush, flush_bytes));
+			flush_dev = qq.eng->device;
+		}
+		cudaEvent_t a, b;
+		VC_CHECK_CUDA(cudaEventCreate(&a));
+		VC_CHECK_CUDA(cudaEventCreate(&b));
+		for (int r = 0; r < reps; r++) {
+			if (flush_l2) {
+				VC_CHECK_CUDA(cudaMemsetAsync(flush, r & 0xff, flush_bytes, s));
+			}
+			VC_CHECK_CUDA(cudaEventRecord(a, s));
+			query_launch(qq, s);
+			VC_CHECK_CUDA(cudaEventRecord(b, s));
+			VC_CHECK_CUDA(cudaEventSynchronize(b));
+			VC_CHECK_CUDA(cudaEventElapsedTime(&ms_out[r], a, b));
+		}
+		cudaEventDestroy(a);
+		cudaEventDestroy(b);
+		query_fetch(qq); /* surfaces device errors of the timed runs */
 	});
 }
 

@@ -75,6 +75,16 @@ def lib():
         "vc_query_info": (c.c_int, [P, P, c.c_size_t, c.POINTER(c.c_size_t)]),
         "vc_query_source": (c.c_int, [P, P, c.c_size_t, c.POINTER(c.c_size_t)]),
         "vc_query_profile": (c.c_int, [P, c.c_int]),
+        "vc_query_time": (c.c_int, [P, c.c_int, c.c_int, P, c.POINTER(c.c_float), c.c_int]),
+        "vc_mlp_create": (c.c_int, [c.c_int, c.c_int, c.c_int, c.c_int, c.c_uint64, c.POINTER(P)]),
+        "vc_mlp_free": (c.c_int, [P]),
+        "vc_mlp_num_params": (c.c_int, [P, c.POINTER(c.c_int64)]),
+        "vc_mlp_get_params": (c.c_int, [P, P, c.c_int64]),
+        "vc_mlp_set_params": (c.c_int, [P, P, c.c_int64]),
+        "vc_mlp_loss_grad": (c.c_int, [P, P, P, P, c.c_int, c.POINTER(c.c_float), P]),
+        "vc_mlp_train": (c.c_int, [P, P, P, P, c.c_int, c.c_int, c.c_int, c.c_float, c.c_uint64,
+                                   c.POINTER(c.c_float)]),
+        "vc_mlp_predict": (c.c_int, [P, P, c.c_int, P]),
         "vc_query_timings": (c.c_int, [P, c.POINTER(c.c_float), c.c_int, c.POINTER(c.c_int), P, c.c_size_t]),
     }
     for name, (res, args) in sigs.items():
@@ -354,6 +364,12 @@ class Query:
     def profile(self, enable=True):
         check(lib().vc_query_profile(self._h, 1 if enable else 0))
 
+    def time(self, reps=5, flush_l2=True, stream=None):
+        """Device time (ms) of each of `reps` runs, L2 flushed before each."""
+        ms = (ctypes.c_float * reps)()
+        check(lib().vc_query_time(self._h, reps, 1 if flush_l2 else 0, _stream_ptr(stream), ms, reps))
+        return [float(x) for x in ms]
+
     def timings(self):
         ms = (ctypes.c_float * 256)()
         n = ctypes.c_int()
@@ -361,3 +377,63 @@ class Query:
         check(lib().vc_query_timings(self._h, ms, 256, ctypes.byref(n), names, len(names)))
         kn = names.value.decode().split("\n")
         return [(kn[i], float(ms[i])) for i in range(n.value)]
+
+
+class Mlp:
+    """The chooser's perceptron, trained and evaluated by the library's GPU kernels."""
+
+    def __init__(self, n_in, n_hidden, n_out, seed=1, device=0):
+        h = ctypes.c_void_p()
+        check(lib().vc_mlp_create(device, n_in, n_hidden, n_out, seed, ctypes.byref(h)))
+        self._h = h
+        self.shape = (n_in, n_hidden, n_out)
+
+    def close(self):
+        if self._h:
+            check(lib().vc_mlp_free(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def num_params(self):
+        n = ctypes.c_int64()
+        check(lib().vc_mlp_num_params(self._h, ctypes.byref(n)))
+        return n.value
+
+    def get_params(self):
+        out = np.empty(self.num_params(), dtype=np.float32)
+        check(lib().vc_mlp_get_params(self._h, out.ctypes.data, out.size))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        check(lib().vc_mlp_set_params(self._h, p.ctypes.data, p.size))
+
+    @staticmethod
+    def _f32(a):
+        return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+    def loss_grad(self, X, T, mask=None):
+        X, T, M = self._f32(X), self._f32(T), self._f32(mask)
+        loss = ctypes.c_float()
+        g = np.empty(self.num_params(), dtype=np.float32)
+        check(lib().vc_mlp_loss_grad(self._h, X.ctypes.data, T.ctypes.data, None if M is None else M.ctypes.data,
+                                     X.shape[0], ctypes.byref(loss), g.ctypes.data))
+        return float(loss.value), g
+
+    def train(self, X, T, mask=None, epochs=200, batch=64, lr=1e-3, seed=1):
+        X, T, M = self._f32(X), self._f32(T), self._f32(mask)
+        loss = ctypes.c_float()
+        check(lib().vc_mlp_train(self._h, X.ctypes.data, T.ctypes.data, None if M is None else M.ctypes.data,
+                                 X.shape[0], epochs, batch, lr, seed, ctypes.byref(loss)))
+        return float(loss.value)
+
+    def predict(self, X):
+        X = self._f32(X)
+        Y = np.empty((X.shape[0], self.shape[2]), dtype=np.float32)
+        check(lib().vc_mlp_predict(self._h, X.ctypes.data, X.shape[0], Y.ctypes.data))
+        return Y

@@ -168,6 +168,27 @@ int vc_query_profile(vc_query* q, int enable);
  * timed hot repetitions, compiler.cpp:521-575). */
 int vc_query_time(vc_query* q, int reps, int flush_l2, void* stream, float* ms_out, int cap);
 
+/* ---------------------------------------------------------------- batches ------------- */
+
+/* Many queries in one persistent kernel driven by a device work queue, launched from a
+ * captured CUDA graph.  The reference runs queries one at a time, each pipeline fanned out
+ * over threads (runtime_framework.cpp:166-198); a batch instead fuses every pipeline of every
+ * query (each with its own flavor; threads per CTA shared) into one launch whose CTAs pull
+ * tile ranges in dependency order (join builds before their probes, group tables before
+ * their extraction).  The queries keep their device state and results: after
+ * vc_batch_run + vc_batch_wait, vc_query_result_* read each query's rows.  The queries must
+ * outlive the batch.  flavors may be NULL (each query's own) or hold one flavor per query
+ * (NULL entries = the query's own).  tiles_per_item: tiles of a pipeline per work item. */
+typedef struct vc_batch vc_batch;
+int vc_batch_new(vc_query** queries, int n, const char** flavors, int threads, int64_t tiles_per_item, vc_batch** out);
+int vc_batch_run(vc_batch* b, void* stream);
+/* Waits for the run; VC_ERR_TIMEOUT if a bounded dependency wait gave up. */
+int vc_batch_wait(vc_batch* b);
+/* Completion time of each query, in microseconds since the batch kernel started. */
+int vc_batch_latencies(vc_batch* b, double* us, int n);
+int vc_batch_info(vc_batch* b, char* buf, size_t cap, size_t* len);
+int vc_batch_free(vc_batch* b);
+
 /* ---------------------------------------------------------------- flavor chooser ------ */
 
 /* A small multi-layer perceptron (in -> hidden -> hidden -> out, ReLU), trained and run on

@@ -1,0 +1,54 @@
+"""The batched persistent kernel: every query of a mixed batch gets exactly the result it
+gets on its own (and the oracle's), over repeated graph replays."""
+import numpy as np
+import pytest
+
+from oracle.voila_oracle import result_lines, run_plan
+from vldb_voila_b200 import Engine, generate_workload_host, workload
+from vldb_voila_b200.engine import Batch, batch_specs
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(specs, flavor_of=lambda s: ""):
+    engines, queries, expect = [], [], []
+    for s in specs:
+        w = workload(s)
+        data = generate_workload_host(w)
+        e = Engine(0)
+        e.load_workload(w, data=data)
+        engines.append(e)
+        queries.append(e.query(w.plan, flavor_of(s)))
+        expect.append(result_lines(run_plan(w.plan, data)))
+    return engines, queries, expect
+
+
+def test_mixed_batch_matches_oracle_and_is_repeatable():
+    specs = batch_specs(24, seed=3, min_rows=1_000, max_rows=400_000)
+    specs += ["star:rows=50000,custs=3000,supps=200,parts=14000,seed=9", "groupby:rows=0,keys=10,seed=1",
+              "sel_aggr:rows=1,seed=2", "join_aggr:build=0,probe=100,seed=3"]
+    engines, queries, expect = _setup(specs)
+    b = Batch(queries, tiles_per_item=2)
+    assert b.info()["work_items"] >= len(specs)
+    for _ in range(3):
+        b.run()
+        b.wait()
+        for q, e in zip(queries, expect):
+            assert q.result_lines() == e
+    lat = b.latencies_us()
+    assert all(x >= 0 for x in lat)
+    # the same queries still run on their own afterwards
+    for q, e in zip(queries[:4], expect[:4]):
+        q.run()
+        assert q.result_lines() == e
+
+
+def test_batch_with_per_query_flavors():
+    specs = batch_specs(12, seed=4, min_rows=10_000, max_rows=200_000)
+    choice = ["cuda(lowcard=private)", "cuda(aggr=cache,cache=128)", "cuda(prefetch=0,rows=2)", ""]
+    engines, queries, expect = _setup(specs)
+    b = Batch(queries, flavors=[choice[i % 4] for i in range(len(specs))], threads=128, tiles_per_item=4)
+    b.run()
+    b.wait()
+    for q, e in zip(queries, expect):
+        assert q.result_lines() == e

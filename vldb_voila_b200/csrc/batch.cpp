@@ -1,0 +1,274 @@
+/*
+ * Batched execution: many queries (pipelines of uneven sizes) in one persistent kernel.
+ *
+ * The reference runs one query at a time and, inside it, one pipeline at a time with
+ * tbb::parallel_for over threads (runtime_framework.cpp:166-198).  Small pipelines leave
+ * most of a GPU idle and every launch costs microseconds, so a batch instead fuses all
+ * pipelines of all its queries into one launch: a persistent grid (one wave of CTAs) pulls
+ * work items -- state clears, tile ranges of pipelines, slot ranges of group extraction --
+ * from a device work queue in dependency order (see generate_batch).  The launch (clears
+ * included) is captured once into a CUDA graph and replayed.
+ *
+ * Waits on dependencies are bounded (2 s); a wait that gives up records VD_ERR_WAIT_TIMEOUT
+ * in the batch's error word and the item is skipped, so a stuck batch ends with an error
+ * instead of a hang.
+ */
+#include <algorithm>
+#include <cstring>
+#include <functional>
+#include <sstream>
+
+#include "engine_internal.hpp"
+#include "../../include/voila_cuda.h"
+
+struct vc_query;
+
+namespace vc {
+
+int abi_guard_mlp(const std::function<void()>& f);
+void query_mark_external_run(Query& q, cudaStream_t s);
+Query* vc_query_internal(vc_query* q);
+
+Batch::~Batch()
+{
+	if (eng) {
+		cudaSetDevice(eng->device);
+	}
+	if (graph) {
+		cudaGraphExecDestroy(graph);
+	}
+	for (void* p : allocations) {
+		cudaFree(p);
+	}
+}
+
+static void* balloc(Batch& b, size_t bytes)
+{
+	void* p = nullptr;
+	VC_CHECK_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 256)));
+	b.allocations.push_back(p);
+	return p;
+}
+
+static void batch_prepare(Batch& b, const std::vector<Flavor>& flavors, int64_t tiles_per_item)
+{
+	VC_CHECK_CUDA(cudaSetDevice(b.eng->device));
+	BatchCode bc = generate_batch(b.queries, flavors, b.flavor.threads, tiles_per_item);
+
+	/* clear items: every query's per-run state, in chunks of at most 8 MiB */
+	std::vector<BatchItem> clears;
+	const int64_t chunk = 8ll << 20;
+	for (Query* q : b.queries) {
+		for (auto& m : state_of(*q).memsets) {
+			const int64_t bytes = (int64_t)((m.second + 15) & ~(size_t)15); /* allocations are 256-byte granular */
+			const int64_t poff = (int64_t)bc.params.size();
+			bc.params.push_back((unsigned long long)(uintptr_t)m.first);
+			for (int64_t off = 0; off < bytes; off += chunk) {
+				BatchItem it;
+				it.shape = -1;
+				it.dep = -1;
+				it.params = poff;
+				it.begin = off;
+				it.end = std::min(off + chunk, bytes);
+				it.nitems = 1;
+				it.dep_target = 0;
+				it.done = 1;
+				it.finish = -1;
+				clears.push_back(it);
+			}
+		}
+	}
+	for (auto& it : bc.items) {
+		if (it.dep_target == -2) {
+			it.dep_target = (int64_t)clears.size();
+		}
+	}
+	bc.items.insert(bc.items.begin(), clears.begin(), clears.end());
+	b.nitems = (int64_t)bc.items.size();
+	b.source = bc.source;
+	std::string log;
+	b.mod = jit_compile(bc.source, &log);
+	VC_CHECK_CUDA(cudaLibraryGetKernel(&b.kernel, b.mod->lib, "vc_batch"));
+	b.smem = bc.smem;
+	if (b.smem > 0) {
+		VC_CHECK_CUDA(cudaFuncSetAttribute((const void*)b.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.smem));
+	}
+	VC_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b.occupancy, (const void*)b.kernel, b.flavor.threads,
+		b.smem));
+	if (b.occupancy < 1) {
+		throw Error(VC_ERR_UNSUPPORTED, "the batch kernel cannot be resident with its shared memory");
+	}
+	/* one wave only: every CTA is resident, so a CTA waiting on a dependency never waits
+	 * for a CTA that cannot run */
+	b.grid = b.eng->sms * b.occupancy;
+
+	b.items = (BatchItem*)balloc(b, sizeof(BatchItem) * bc.items.size());
+	VC_CHECK_CUDA(cudaMemcpy(b.items, bc.items.data(), sizeof(BatchItem) * bc.items.size(), cudaMemcpyHostToDevice));
+	b.params = (unsigned long long*)balloc(b, sizeof(unsigned long long) * std::max<size_t>(bc.params.size(), 1));
+	VC_CHECK_CUDA(cudaMemcpy(b.params, bc.params.data(), sizeof(unsigned long long) * bc.params.size(),
+		cudaMemcpyHostToDevice));
+	b.counters_bytes = sizeof(unsigned long long) * (size_t)bc.ncounters;
+	b.counters = (unsigned long long*)balloc(b, b.counters_bytes + sizeof(unsigned long long) * (b.queries.size() + 1) + 64);
+	b.finish = b.counters + bc.ncounters;
+	b.err = (unsigned*)(b.finish + b.queries.size() + 1);
+}
+
+static void batch_launch_all(Batch& b, cudaStream_t s)
+{
+	const size_t book = b.counters_bytes + sizeof(unsigned long long) * (b.queries.size() + 1) + 64;
+	VC_CHECK_CUDA(cudaMemsetAsync(b.counters, 0, book, s));
+	long long nwork = b.nitems;
+	int nq = (int)b.queries.size();
+	void* args[] = {&b.items, &nwork, &b.counters, &b.params, &b.finish, &nq, &b.err};
+	VC_CHECK_CUDA(cudaLaunchKernel((const void*)b.kernel, dim3((unsigned)b.grid), dim3((unsigned)b.flavor.threads), args,
+		b.smem, s));
+}
+
+static void batch_run(Batch& b, cudaStream_t s)
+{
+	VC_CHECK_CUDA(cudaSetDevice(b.eng->device));
+	if (!b.graph) {
+		cudaStream_t cs;
+		VC_CHECK_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+		cudaGraph_t g;
+		VC_CHECK_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+		try {
+			batch_launch_all(b, cs);
+		} catch (...) {
+			cudaStreamEndCapture(cs, &g);
+			cudaStreamDestroy(cs);
+			throw;
+		}
+		VC_CHECK_CUDA(cudaStreamEndCapture(cs, &g));
+		VC_CHECK_CUDA(cudaGraphInstantiate(&b.graph, g, 0));
+		cudaGraphDestroy(g);
+		cudaStreamDestroy(cs);
+	}
+	VC_CHECK_CUDA(cudaGraphLaunch(b.graph, s));
+	b.stream = s;
+	for (Query* q : b.queries) {
+		query_mark_external_run(*q, s);
+	}
+}
+
+} // namespace vc
+
+using namespace vc;
+
+struct vc_batch {
+	Batch b;
+};
+
+extern "C" {
+
+int vc_batch_new(vc_query** queries, int n, const char** flavors, int threads, int64_t tiles_per_item, vc_batch** out)
+{
+	vc_batch* h = nullptr;
+	int rc = abi_guard_mlp([&] {
+		if (!queries || n < 1 || !out || threads < 32 || threads > 1024 || threads % 32 || tiles_per_item < 1) {
+			throw Error(VC_ERR_INVALID, "bad batch arguments");
+		}
+		h = new vc_batch();
+		std::vector<Flavor> fls;
+		for (int i = 0; i < n; i++) {
+			if (!queries[i]) {
+				throw Error(VC_ERR_INVALID, "null query in batch");
+			}
+			Query* q = vc_query_internal(queries[i]);
+			if (h->b.eng && h->b.eng->device != q->eng->device) {
+				throw Error(VC_ERR_INVALID, "batched queries must live on one device");
+			}
+			if (q->eng->offline) {
+				throw Error(VC_ERR_NO_DEVICE, "offline queries cannot be batched");
+			}
+			h->b.eng = q->eng;
+			h->b.queries.push_back(q);
+			fls.push_back(flavors && flavors[i] ? Flavor::parse(flavors[i]) : q->flavor);
+		}
+		h->b.flavor.threads = threads;
+		batch_prepare(h->b, fls, tiles_per_item);
+		*out = h;
+	});
+	if (rc != VC_OK && h) {
+		delete h; /* the error message of the failed call stays in place */
+	}
+	return rc;
+}
+
+int vc_batch_run(vc_batch* h, void* stream)
+{
+	return abi_guard_mlp([&] {
+		if (!h) {
+			throw Error(VC_ERR_INVALID, "null batch");
+		}
+		batch_run(h->b, (cudaStream_t)stream);
+	});
+}
+
+int vc_batch_wait(vc_batch* h)
+{
+	return abi_guard_mlp([&] {
+		if (!h) {
+			throw Error(VC_ERR_INVALID, "null batch");
+		}
+		Batch& b = h->b;
+		VC_CHECK_CUDA(cudaSetDevice(b.eng->device));
+		VC_CHECK_CUDA(cudaStreamSynchronize(b.stream));
+		unsigned err = 0;
+		VC_CHECK_CUDA(cudaMemcpy(&err, b.err, sizeof(err), cudaMemcpyDeviceToHost));
+		if (err & 2u) {
+			throw Error(VC_ERR_TIMEOUT, "a batch dependency wait gave up");
+		}
+		if (err) {
+			throw Error(VC_ERR_CAPACITY, "batch error bits " + std::to_string(err));
+		}
+	});
+}
+
+int vc_batch_latencies(vc_batch* h, double* us, int n)
+{
+	return abi_guard_mlp([&] {
+		if (!h || !us || n < (int)h->b.queries.size()) {
+			throw Error(VC_ERR_INVALID, "bad arguments");
+		}
+		Batch& b = h->b;
+		std::vector<unsigned long long> f(b.queries.size() + 1);
+		VC_CHECK_CUDA(cudaSetDevice(b.eng->device));
+		VC_CHECK_CUDA(cudaStreamSynchronize(b.stream));
+		VC_CHECK_CUDA(cudaMemcpy(f.data(), b.finish, sizeof(unsigned long long) * f.size(), cudaMemcpyDeviceToHost));
+		const unsigned long long start = f.back();
+		for (size_t i = 0; i < b.queries.size(); i++) {
+			us[i] = f[i] >= start ? (double)(f[i] - start) / 1000.0 : -1.0;
+		}
+	});
+}
+
+int vc_batch_info(vc_batch* h, char* buf, size_t cap, size_t* len)
+{
+	return abi_guard_mlp([&] {
+		if (!h) {
+			throw Error(VC_ERR_INVALID, "null batch");
+		}
+		Batch& b = h->b;
+		std::ostringstream o;
+		o << "{\"queries\": " << b.queries.size() << ", \"work_items\": " << b.nitems << ", \"grid\": " << b.grid
+		  << ", \"threads\": " << b.flavor.threads << ", \"smem\": " << b.smem << ", \"occupancy\": " << b.occupancy
+		  << ", \"source_bytes\": " << b.source.size() << "}";
+		const std::string s = o.str();
+		if (len) {
+			*len = s.size();
+		}
+		if (buf && cap) {
+			const size_t k = std::min(cap - 1, s.size());
+			std::memcpy(buf, s.data(), k);
+			buf[k] = 0;
+		}
+	});
+}
+
+int vc_batch_free(vc_batch* h)
+{
+	return abi_guard_mlp([&] { delete h; });
+}
+
+} // extern "C"

@@ -167,8 +167,29 @@ struct PipeGen {
 
 	/* ------------------------------------------------------------ main kernel ------ */
 
+	/* item mode: the pipeline body becomes a device function over a tile range [t_begin,
+	 * t_end) that the persistent batch kernel calls; parameters come from a pool in global
+	 * memory instead of the kernel parameter space */
+	bool item = false;
+	std::string tstart() const { return item ? "t_begin" : "(int64_t)blockIdx.x"; }
+	std::string tstep() const { return item ? "1" : "(int64_t)gridDim.x"; }
+	std::string tend() const { return item ? "tlim" : "ntiles"; }
+	std::string blocks_total() const { return item ? "(unsigned long long)nitems" : "(unsigned long long)gridDim.x"; }
+
+	void fn_header(const std::string& suffix) {
+		if (item) {
+			o << "__device__ __noinline__ void " << name << suffix
+			  << "(const unsigned long long* __restrict__ pv, int64_t t_begin, int64_t t_end, int64_t nitems) {\n";
+			o << "  const struct { const unsigned long long* __restrict__ v; } p = {pv};\n";
+			o << "  (void)nitems;\n";
+		} else {
+			o << "extern \"C\" __global__ void __launch_bounds__(" << T << ") " << name << suffix
+			  << "(const VcParams p) {\n";
+		}
+	}
+
 	std::string gen_main() {
-		o << "extern \"C\" __global__ void __launch_bounds__(" << T << ") " << name << "_main(const VcParams p) {\n";
+		fn_header("_main");
 		o << "  const int64_t n = " << P((unsigned long long)p.rows) << ";\n";
 		p.err_slot = (int)params.size();
 		o << "  unsigned* const err = (unsigned*)p.v[" << params.size() << "];\n";
@@ -186,13 +207,16 @@ struct PipeGen {
 		sink_prologue();
 		o << "  const int64_t tile = (int64_t)" << T << " * " << V << ";\n";
 		o << "  const int64_t ntiles = (n + tile - 1) / tile;\n";
+		if (item) {
+			o << "  const int64_t tlim = t_end < ntiles ? t_end : ntiles;\n";
+		}
 
 		emit_compaction_smem();
 		bool any_eager = false;
 		for (size_t c = 0; c < p.cols.size(); c++) {
 			any_eager = any_eager || eager[c];
 		}
-		const bool tma = fl.load == "tma" && any_eager;
+		const bool tma = fl.load == "tma" && any_eager && !item;
 		if (tma) {
 			gen_tma_loop();
 		} else if (fl.prefetch && any_eager) {
@@ -204,25 +228,25 @@ struct PipeGen {
 					o << "  " << ctype(p.cols[c].type) << " pf" << c << "[" << V << "];\n";
 				}
 			}
-			o << "  int64_t t = blockIdx.x;\n";
-			o << "  if (t < ntiles) {\n    const int64_t r0p = t * tile + (int64_t)threadIdx.x * " << V << ";\n";
+			o << "  int64_t t = " << tstart() << ";\n";
+			o << "  if (t < " << tend() << ") {\n    const int64_t r0p = t * tile + (int64_t)threadIdx.x * " << V << ";\n";
 			emit_load_cols("ldg", "pf", "r0p");
 			o << "  }\n";
-			o << "  for (; t < ntiles; t += gridDim.x) {\n";
+			o << "  for (; t < " << tend() << "; t += " << tstep() << ") {\n";
 			emit_decl_cols(true, V);
 			for (size_t c = 0; c < p.cols.size(); c++) {
 				if (eager[c]) {
 					o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) { x" << c << "[v] = pf" << c << "[v]; }\n";
 				}
 			}
-			o << "    {\n    const int64_t tn = t + gridDim.x;\n";
-			o << "    if (tn < ntiles) {\n    const int64_t r0p = tn * tile + (int64_t)threadIdx.x * " << V << ";\n";
+			o << "    {\n    const int64_t tn = t + " << tstep() << ";\n";
+			o << "    if (tn < " << tend() << ") {\n    const int64_t r0p = tn * tile + (int64_t)threadIdx.x * " << V << ";\n";
 			emit_load_cols("ldg", "pf", "r0p");
 			o << "    }\n    }\n";
 			emit_body("pre");
 			o << "  }\n  }\n";
 		} else {
-			o << "  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {\n";
+			o << "  for (int64_t t = " << tstart() << "; t < " << tend() << "; t += " << tstep() << ") {\n";
 			emit_body("ldg");
 			o << "  }\n";
 		}
@@ -747,7 +771,8 @@ struct PipeGen {
 	void publish_slots(const std::string& g, int64_t nslots_val) {
 		Sink& s = p.sink;
 		o << "  __shared__ int last_flag;\n";
-		o << "  if (vd::last_block_done(" << Pptr(st.done, "unsigned long long*") << ", &last_flag)) {\n";
+		o << "  if (vd::last_block_done(" << Pptr(st.done, "unsigned long long*") << ", " << blocks_total()
+		  << ", &last_flag)) {\n";
 		o << "    int64_t* const out = " << Pptr(qs.out, "int64_t*") << ";\n";
 		o << "    const int64_t ocap = " << P((unsigned long long)qs.out_cap) << ";\n";
 		o << "    unsigned long long* const ocount = " << Pptr(qs.out_count, "unsigned long long*") << ";\n";
@@ -888,7 +913,14 @@ struct PipeGen {
 	std::string gen_extract() {
 		Sink& s = p.sink;
 		std::ostringstream k;
-		k << "extern \"C\" __global__ void __launch_bounds__(256) " << name << "_extract(const VcParams p) {\n";
+		if (item) {
+			k << "__device__ __noinline__ void " << name
+			  << "_extract(const unsigned long long* __restrict__ pv, int64_t t_begin, int64_t t_end, int64_t nitems) {\n";
+			k << "  const struct { const unsigned long long* __restrict__ v; } p = {pv};\n";
+			k << "  (void)nitems;\n";
+		} else {
+			k << "extern \"C\" __global__ void __launch_bounds__(256) " << name << "_extract(const VcParams p) {\n";
+		}
 		k << "  int64_t* const out = " << Pptr(qs.out, "int64_t*") << ";\n";
 		k << "  const int64_t ocap = " << P((unsigned long long)qs.out_cap) << ";\n";
 		k << "  unsigned long long* const ocount = " << Pptr(qs.out_count, "unsigned long long*") << ";\n";
@@ -896,15 +928,23 @@ struct PipeGen {
 		const int W = 1 + A();
 		k << "  const int64_t nslots = " << P((unsigned long long)st.sink_cap) << ";\n";
 		/* each warp covers kExtractK groups of 32 slots per step: all their key and count
-		 * words are loaded before any is used */
-		k << "  const int64_t stride = (int64_t)gridDim.x * blockDim.x * " << kExtractK << ";\n";
-		k << "  for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * " << kExtractK
-		  << "; base < nslots; base += stride) {\n";
+		 * words are loaded (from L2, coherent) before any is used */
+		if (item) {
+			/* one item = slot groups [t_begin, t_end) of blockDim.x * kExtractK slots */
+			k << "  const int64_t stride = (int64_t)blockDim.x * " << kExtractK << ";\n";
+			k << "  const int64_t slim = t_end * stride < nslots ? t_end * stride : nslots;\n";
+			k << "  for (int64_t base = t_begin * stride + (int64_t)(threadIdx.x & ~31) * " << kExtractK
+			  << "; base < slim; base += stride) {\n";
+		} else {
+			k << "  const int64_t stride = (int64_t)gridDim.x * blockDim.x * " << kExtractK << ";\n";
+			k << "  for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * " << kExtractK
+			  << "; base < nslots; base += stride) {\n";
+		}
 		k << "    unsigned long long kw[" << kExtractK << "]; long long cw[" << kExtractK << "];\n";
 		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
 		k << "      const int64_t i = base + q * 32 + (threadIdx.x & 31);\n";
-		k << "      kw[q] = i < nslots ? __ldcs(&g[i * " << W << "]) : 0ull;\n";
-		k << "      cw[q] = i < nslots ? (long long)__ldcs(&g[i * " << W << " + 1 + " << s.count_idx << "]) : 0;\n";
+		k << "      kw[q] = i < nslots ? __ldcg(&g[i * " << W << "]) : 0ull;\n";
+		k << "      cw[q] = i < nslots ? (long long)__ldcg(&g[i * " << W << " + 1 + " << s.count_idx << "]) : 0;\n";
 		k << "    }\n";
 		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
 		k << "    const int64_t i = base + q * 32 + (threadIdx.x & 31);\n";
@@ -993,6 +1033,184 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 	}
 	gc.source = src.str();
 	return gc;
+}
+
+/*
+ * Batch code: every pipeline of every query becomes a device item function (deduplicated by
+ * generated text, so instances of one shape share code) and a list of work items over its
+ * tiles.  Items are ordered by phase -- phase 0: join builds and pipelines without inputs
+ * from other pipelines, phase 1: probes that read a built table, phase 2: group extraction --
+ * and carry the done-counter they must wait for, so the persistent kernel's queue runs them
+ * in dependency order.  Phase-0 items wait for the state clears the runtime prepends
+ * (dep_target -2 is patched with their count).  Counter 0 is the queue head, counter 1
+ * counts finished clears.
+ */
+BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>& flavors, int threads,
+	int64_t tiles_per_item)
+{
+	BatchCode bc;
+	std::map<std::string, int> shape_of;
+	std::vector<std::string> shape_fn;
+	std::ostringstream funcs;
+	std::vector<BatchItem> phases[3];
+	int ncounters = 2;
+	auto add_shape = [&](const std::string& text, const std::string& suffix) -> int {
+		auto it = shape_of.find(text);
+		if (it != shape_of.end()) {
+			return it->second;
+		}
+		const int id = (int)shape_fn.size();
+		const std::string fname = "vc_s" + std::to_string(id);
+		std::string t = text;
+		for (size_t pos = t.find("VCSHAPE"); pos != std::string::npos; pos = t.find("VCSHAPE", pos)) {
+			t.replace(pos, 7, fname);
+		}
+		funcs << t;
+		shape_fn.push_back(fname + suffix);
+		shape_of[text] = id;
+		return id;
+	};
+	for (size_t qi = 0; qi < queries.size(); qi++) {
+		Query& q = *queries[qi];
+		QueryState& st = state_of(q);
+		Flavor fl = flavors[qi];
+		fl.threads = threads;
+		fl.load = "ldg";
+		QueryDeviceState qs;
+		qs.out = q.out;
+		qs.out_cap = q.out_cap;
+		qs.out_count = q.out_count;
+		int build_counter = -1;
+		int64_t build_items = 0;
+		for (auto& p : q.plan.pipes) {
+			if (p.sink.kind == Sink::JoinBuild && !q.plan.joins[p.sink.join].direct) {
+				throw Error(6, "batched queries need direct join builds (build=staged is not batchable)");
+			}
+			std::vector<unsigned long long> prm;
+			PipeGen g(p, q.plan, fl, st.pipes[p.id], qs, prm);
+			g.item = true;
+			g.name = "VCSHAPE";
+			const std::string main_src = g.gen_main();
+			const std::string extract_src = p.sink.kind == Sink::AggHash ? g.gen_extract() : std::string();
+			bc.smem = std::max(bc.smem, g.smem_total);
+			prm[p.err_slot] = (unsigned long long)(uintptr_t)q.err;
+			for (size_t c = 0; c < p.cols.size(); c++) {
+				Column* col = q.eng->tables.at(p.cols[c].table).find(p.cols[c].name);
+				prm[p.col_slots[c]] = (unsigned long long)(uintptr_t)col->dev;
+			}
+			const int64_t poff = (int64_t)bc.params.size();
+			bc.params.insert(bc.params.end(), prm.begin(), prm.end());
+
+			const int sid = add_shape(main_src, "_main");
+			const int64_t tile = (int64_t)fl.threads * fl.rows;
+			const int64_t ntiles = std::max<int64_t>((p.rows + tile - 1) / tile, 1);
+			const int64_t nit = (ntiles + tiles_per_item - 1) / tiles_per_item;
+			const bool is_build = p.sink.kind == Sink::JoinBuild;
+			int counter;
+			if (is_build) {
+				if (build_counter < 0) {
+					build_counter = ncounters++;
+				}
+				counter = build_counter;
+			} else {
+				counter = ncounters++;
+			}
+			const int phase = is_build ? 0 : (build_counter >= 0 ? 1 : 0);
+			for (int64_t k = 0; k < nit; k++) {
+				BatchItem it;
+				it.shape = sid;
+				it.params = poff;
+				it.begin = k * tiles_per_item;
+				it.end = std::min((k + 1) * tiles_per_item, ntiles);
+				it.nitems = nit;
+				it.dep = phase == 0 ? 1 : build_counter;
+				it.dep_target = phase == 0 ? -2 : build_items;
+				it.done = counter;
+				it.finish = (!is_build && p.sink.kind != Sink::AggHash) ? (int)qi : -1;
+				phases[phase].push_back(it);
+			}
+			if (is_build) {
+				build_items += nit;
+			}
+			if (p.sink.kind == Sink::AggHash) {
+				const int sid2 = add_shape(extract_src, "_extract");
+				const int64_t group = (int64_t)threads * 4;
+				const int64_t ngroups = std::max<int64_t>((st.pipes[p.id].sink_cap + group - 1) / group, 1);
+				const int64_t per = std::max<int64_t>(tiles_per_item / 4, 1);
+				const int64_t nit2 = (ngroups + per - 1) / per;
+				const int counter2 = ncounters++;
+				for (int64_t k = 0; k < nit2; k++) {
+					BatchItem it;
+					it.shape = sid2;
+					it.params = poff;
+					it.begin = k * per;
+					it.end = std::min((k + 1) * per, ngroups);
+					it.nitems = nit2;
+					it.dep = counter;
+					it.dep_target = nit;
+					it.done = counter2;
+					it.finish = (int)qi;
+					phases[std::min(phase + 1, 2)].push_back(it);
+				}
+			}
+		}
+	}
+	for (auto& ph : phases) {
+		bc.items.insert(bc.items.end(), ph.begin(), ph.end());
+	}
+	bc.ncounters = ncounters;
+
+	std::ostringstream src;
+	src << "#define VD_COHERENT_TABLES 1\n#include \"voila_device.cuh\"\n";
+	src << "struct VcBatchItem { int shape; int dep; long long params; long long begin; long long end; "
+		"long long nitems; long long dep_target; int done; int finish; };\n\n";
+	src << funcs.str();
+	src << "extern \"C\" __global__ void __launch_bounds__(" << threads << ") vc_batch(const VcBatchItem* __restrict__ items, "
+		"long long nwork, unsigned long long* counters, const unsigned long long* __restrict__ pool, "
+		"unsigned long long* finish_ns, int nq, unsigned* err) {\n";
+	src << "  __shared__ long long s_w;\n  __shared__ int s_ok;\n";
+	src << "  if (threadIdx.x == 0) { atomicCAS(&finish_ns[nq], 0ull, (unsigned long long)vd::globaltimer_ns()); }\n";
+	src << "  for (;;) {\n";
+	src << "    if (threadIdx.x == 0) { s_w = (long long)atomicAdd(&counters[0], 1ull); }\n";
+	src << "    __syncthreads();\n";
+	src << "    const long long w = s_w;\n";
+	src << "    if (w >= nwork) { break; }\n";
+	src << "    const VcBatchItem it = items[w];\n";
+	src << "    if (threadIdx.x == 0) {\n";
+	src << "      int ok = 1;\n";
+	src << "      if (it.dep >= 0) {\n";
+	src << "        uint64_t t0 = 0;\n";
+	src << "        for (unsigned spin = 0; *(volatile unsigned long long*)&counters[it.dep] < (unsigned long long)it.dep_target; spin++) {\n";
+	src << "          if (spin == 0) { t0 = vd::globaltimer_ns(); }\n";
+	src << "          else if ((spin & 255u) == 0 && vd::globaltimer_ns() - t0 > 2000000000ull) { ok = 0; break; }\n";
+	src << "          __nanosleep(100);\n";
+	src << "        }\n";
+	src << "        __threadfence();\n";
+	src << "      }\n";
+	src << "      s_ok = ok;\n";
+	src << "    }\n";
+	src << "    __syncthreads();\n";
+	src << "    if (s_ok) {\n";
+	src << "      switch (it.shape) {\n";
+	src << "      case -1: {\n";
+	src << "        unsigned char* base = (unsigned char*)pool[it.params];\n";
+	src << "        for (long long off = it.begin + (long long)threadIdx.x * 16; off < it.end; off += (long long)blockDim.x * 16) {\n";
+	src << "          *(uint4*)(base + off) = make_uint4(0u, 0u, 0u, 0u);\n";
+	src << "        }\n        break;\n      }\n";
+	for (size_t s = 0; s < shape_fn.size(); s++) {
+		src << "      case " << s << ": " << shape_fn[s] << "(pool + it.params, it.begin, it.end, it.nitems); break;\n";
+	}
+	src << "      default: break;\n      }\n";
+	src << "    } else if (threadIdx.x == 0) {\n      atomicOr(err, VD_ERR_WAIT_TIMEOUT);\n    }\n";
+	src << "    __syncthreads();\n";
+	src << "    if (threadIdx.x == 0) {\n";
+	src << "      __threadfence();\n";
+	src << "      const unsigned long long old = atomicAdd(&counters[it.done], 1ull);\n";
+	src << "      if (it.finish >= 0 && old + 1ull == (unsigned long long)it.nitems) { finish_ns[it.finish] = vd::globaltimer_ns(); }\n";
+	src << "    }\n";
+	src << "  }\n}\n";
+	bc.source = src.str();
+	return bc;
 }
 
 } // namespace vc

@@ -409,12 +409,12 @@ __device__ __forceinline__ int dict_code(int* dict, int* codes, int* ncodes, int
 
 /* True in every thread of the block that finishes last (all blocks call it once, after
  * their global updates); that block then publishes the final result. */
-__device__ __forceinline__ bool last_block_done(unsigned long long* counter, int* flag_smem)
+__device__ __forceinline__ bool last_block_done(unsigned long long* counter, unsigned long long total, int* flag_smem)
 {
 	__threadfence();
 	__syncthreads();
 	if (threadIdx.x == 0) {
-		*flag_smem = atomicAdd(counter, 1ull) == (unsigned long long)(gridDim.x - 1);
+		*flag_smem = atomicAdd(counter, 1ull) == total - 1ull;
 	}
 	__syncthreads();
 	const bool last = *flag_smem != 0;
@@ -498,8 +498,14 @@ __device__ __forceinline__ int join_probe_bucket(const JoinSlot<KeyT, PayT>* __r
 	const S* bk = slots + b * SPB;
 	S s[SPB];
 	if constexpr (sizeof(S) * SPB == 32) {
+#ifdef VD_COHERENT_TABLES
+		/* the table was built earlier in the same (persistent) kernel: read it from L2 */
+		uint4 lo = __ldcg(reinterpret_cast<const uint4*>(bk));
+		uint4 hi = __ldcg(reinterpret_cast<const uint4*>(bk) + 1);
+#else
 		uint4 lo = __ldg(reinterpret_cast<const uint4*>(bk));
 		uint4 hi = __ldg(reinterpret_cast<const uint4*>(bk) + 1);
+#endif
 		reinterpret_cast<uint4*>(s)[0] = lo;
 		reinterpret_cast<uint4*>(s)[1] = hi;
 	} else {

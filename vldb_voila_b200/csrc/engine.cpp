@@ -199,17 +199,10 @@ Query::~Query()
 	}
 }
 
-struct QueryState {
-	std::vector<PipeDeviceState> pipes;
-	std::vector<cudaKernel_t> kernels;
-	std::vector<int> occupancy;
-	std::vector<std::pair<void*, size_t>> memsets;
-};
-
 static std::map<Query*, QueryState> g_state;
 static std::mutex g_state_mu;
 
-static QueryState& state_of(Query& q)
+QueryState& state_of(Query& q)
 {
 	std::lock_guard<std::mutex> g(g_state_mu);
 	return g_state[&q];
@@ -547,6 +540,20 @@ namespace vc {
 int abi_guard_mlp(const std::function<void()>& f)
 {
 	return guarded(f);
+}
+
+Query* vc_query_internal(vc_query* q)
+{
+	return &q->q;
+}
+
+/* the query's kernels ran inside a batch on stream s: results are read as after vc_query_run */
+void query_mark_external_run(Query& q, cudaStream_t s)
+{
+	q.stream = s;
+	q.ran = true;
+	q.result_rows = -1;
+	q.profile = false;
 }
 } // namespace vc
 

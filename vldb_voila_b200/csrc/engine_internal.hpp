@@ -296,6 +296,65 @@ struct Query {
 	~Query();
 };
 
+/* device-side bookkeeping of one query (kept beside Query so batches can reuse it) */
+struct QueryState {
+	std::vector<PipeDeviceState> pipes;
+	std::vector<cudaKernel_t> kernels;
+	std::vector<int> occupancy;
+	std::vector<std::pair<void*, size_t>> memsets;
+};
+
+QueryState& state_of(Query& q);
+
+/* ------------------------------------------------------------------ batches ------------ */
+
+/* One unit of work of the persistent batch kernel (layout shared with the device code). */
+struct BatchItem {
+	int32_t shape;          /* which generated item function runs it */
+	int32_t dep;            /* done-counter that must reach dep_target first, -1 = none */
+	int64_t params;         /* offset of the pipeline's parameters in the parameter pool */
+	int64_t begin, end;     /* tile (or slot-group) range */
+	int64_t nitems;         /* items of this pipeline stage (last-item publication) */
+	int64_t dep_target;
+	int32_t done;           /* done-counter incremented when the item finishes */
+	int32_t finish;         /* query whose completion time this item may record, -1 = none */
+};
+
+struct Batch {
+	Engine* eng = nullptr;
+	std::vector<Query*> queries;
+	Flavor flavor;
+	std::string source;
+	std::shared_ptr<JitModule> mod;
+	cudaKernel_t kernel = nullptr;
+	int occupancy = 0;
+	size_t smem = 0;
+	int64_t nitems = 0;
+	std::vector<void*> allocations;
+	BatchItem* items = nullptr;
+	unsigned long long* counters = nullptr; /* [0] queue head, [1..] done counters */
+	size_t counters_bytes = 0;
+	unsigned long long* params = nullptr;
+	unsigned long long* finish = nullptr;   /* per query: completion globaltimer ns; [n] = start */
+	unsigned* err = nullptr;
+	std::vector<std::pair<void*, size_t>> memsets;
+	cudaGraphExec_t graph = nullptr;
+	cudaStream_t stream = nullptr;
+	int grid = 0;
+	~Batch();
+};
+
+struct BatchCode {
+	std::string source;
+	size_t smem = 0;
+	std::vector<BatchItem> items;
+	std::vector<unsigned long long> params;
+	int ncounters = 0;
+};
+
+BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>& flavors, int threads,
+	int64_t tiles_per_item);
+
 void query_prepare(Query& q);
 void query_launch(Query& q, cudaStream_t stream);
 void query_fetch(Query& q);

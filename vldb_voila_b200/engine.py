@@ -85,6 +85,12 @@ def lib():
         "vc_mlp_train": (c.c_int, [P, P, P, P, c.c_int, c.c_int, c.c_int, c.c_float, c.c_uint64,
                                    c.POINTER(c.c_float)]),
         "vc_mlp_predict": (c.c_int, [P, P, c.c_int, P]),
+        "vc_batch_new": (c.c_int, [c.POINTER(P), c.c_int, c.POINTER(c.c_char_p), c.c_int, c.c_int64, c.POINTER(P)]),
+        "vc_batch_run": (c.c_int, [P, P]),
+        "vc_batch_wait": (c.c_int, [P]),
+        "vc_batch_latencies": (c.c_int, [P, c.POINTER(c.c_double), c.c_int]),
+        "vc_batch_info": (c.c_int, [P, P, c.c_size_t, c.POINTER(c.c_size_t)]),
+        "vc_batch_free": (c.c_int, [P]),
         "vc_query_timings": (c.c_int, [P, c.POINTER(c.c_float), c.c_int, c.POINTER(c.c_int), P, c.c_size_t]),
     }
     for name, (res, args) in sigs.items():
@@ -377,6 +383,47 @@ class Query:
         check(lib().vc_query_timings(self._h, ms, 256, ctypes.byref(n), names, len(names)))
         kn = names.value.decode().split("\n")
         return [(kn[i], float(ms[i])) for i in range(n.value)]
+
+
+class Batch:
+    """Many queries in one persistent kernel (vc_batch_*); the queries keep their results."""
+
+    def __init__(self, queries, flavors=None, threads=256, tiles_per_item=64):
+        self.queries = list(queries)  # the queries must outlive the batch
+        arr = (ctypes.c_void_p * len(self.queries))(*[q._h.value for q in self.queries])
+        fl = None
+        if flavors is not None:
+            fl = (ctypes.c_char_p * len(self.queries))(*[_b(f) if f else None for f in flavors])
+        h = ctypes.c_void_p()
+        check(lib().vc_batch_new(arr, len(self.queries), fl, threads, tiles_per_item, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            check(lib().vc_batch_free(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, stream=None):
+        check(lib().vc_batch_run(self._h, _stream_ptr(stream)))
+        return self
+
+    def wait(self):
+        check(lib().vc_batch_wait(self._h))
+
+    def latencies_us(self):
+        out = (ctypes.c_double * len(self.queries))()
+        check(lib().vc_batch_latencies(self._h, out, len(self.queries)))
+        return [float(x) for x in out]
+
+    def info(self):
+        import json
+        return json.loads(_text_call(lib().vc_batch_info, self._h))
 
 
 class Mlp:

@@ -63,6 +63,21 @@ def test_bad_or_unsupported_plans_fail_with_status(plan, code):
     assert ex.value.code == code
 
 
+def test_batch_module_compiles_and_dedups_shapes():
+    from vldb_voila_b200.engine import Batch, batch_specs
+    specs = batch_specs(9, seed=3, min_rows=1000, max_rows=400000) + ["star:rows=5000,seed=9"]
+    engines, queries = [], []
+    for s in specs:
+        w, e = offline(s)
+        engines.append(e)
+        queries.append(e.query(w.plan))
+    one = Batch(queries[:1])
+    many = Batch(queries)
+    # one persistent kernel; shapes shared: far less code than one copy per query
+    assert many.info()["source_bytes"] < 4 * one.info()["source_bytes"] * 3
+    assert many.info()["work_items"] >= len(specs)
+
+
 @pytest.mark.parametrize("flavor", ["cuda(rows=3)", "cuda(threads=100)", "cuda(aggr=magic)", "gpu(x=1)", "cuda(nokey=1)"])
 def test_bad_flavors_are_rejected(flavor):
     w, e = offline("sel_aggr:rows=1000")

@@ -31,6 +31,9 @@ Query* vc_query_internal(vc_query* q);
 
 Batch::~Batch()
 {
+	if (eng && eng->offline) {
+		return;
+	}
 	if (eng) {
 		cudaSetDevice(eng->device);
 	}
@@ -52,6 +55,16 @@ static void* balloc(Batch& b, size_t bytes)
 
 static void batch_prepare(Batch& b, const std::vector<Flavor>& flavors, int64_t tiles_per_item)
 {
+	if (b.eng->offline) {
+		/* compile-only engines: generate and compile the batch module, nothing more */
+		BatchCode bc = generate_batch(b.queries, flavors, b.flavor.threads, tiles_per_item);
+		b.source = bc.source;
+		b.nitems = (int64_t)bc.items.size();
+		b.smem = bc.smem;
+		std::string log;
+		jit_cubin(bc.source, &log);
+		return;
+	}
 	VC_CHECK_CUDA(cudaSetDevice(b.eng->device));
 	BatchCode bc = generate_batch(b.queries, flavors, b.flavor.threads, tiles_per_item);
 
@@ -178,8 +191,8 @@ int vc_batch_new(vc_query** queries, int n, const char** flavors, int threads, i
 			if (h->b.eng && h->b.eng->device != q->eng->device) {
 				throw Error(VC_ERR_INVALID, "batched queries must live on one device");
 			}
-			if (q->eng->offline) {
-				throw Error(VC_ERR_NO_DEVICE, "offline queries cannot be batched");
+			if (h->b.eng && h->b.eng->offline != q->eng->offline) {
+				throw Error(VC_ERR_INVALID, "a batch cannot mix offline and device queries");
 			}
 			h->b.eng = q->eng;
 			h->b.queries.push_back(q);
@@ -200,6 +213,9 @@ int vc_batch_run(vc_batch* h, void* stream)
 	return abi_guard_mlp([&] {
 		if (!h) {
 			throw Error(VC_ERR_INVALID, "null batch");
+		}
+		if (h->b.eng->offline) {
+			throw Error(VC_ERR_NO_DEVICE, "an offline engine only generates and compiles code");
 		}
 		batch_run(h->b, (cudaStream_t)stream);
 	});

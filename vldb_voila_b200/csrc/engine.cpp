@@ -175,7 +175,8 @@ static void* dev_alloc(Query& q, size_t bytes)
 		q.eng->fake_next += ((bytes + 255) / 256 + 1) * 256;
 		return p;
 	}
-	VC_CHECK_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 256)));
+	/* whole 256-byte granules: bulk clears may round a region up to 16 bytes */
+	VC_CHECK_CUDA(cudaMalloc(&p, std::max<size_t>((bytes + 255) & ~(size_t)255, 256)));
 	q.allocations.push_back(p);
 	return p;
 }

@@ -74,6 +74,7 @@ struct PipeGen {
 	int cache_slots = 0;
 	bool dense_in_smem = false;
 	int replicas = 1;          /* per-warp copies of the dense slot array (lowcard=atomic) */
+	std::map<const BExpr*, int> const_slot; /* parameter slot of each constant node */
 	bool private_acc = false;  /* per-thread private accumulators (lowcard=private) */
 	static constexpr int kGmax = 8; /* distinct groups per block held in private accumulators */
 	static constexpr int kExtractK = 4; /* slot groups per warp step of the group extraction */
@@ -103,12 +104,16 @@ struct PipeGen {
 		switch (e->kind) {
 		case BExpr::Col:
 			return "((int64_t)x" + std::to_string(e->col) + "[" + v + "])";
-		case BExpr::Const:
-			if (e->param < 0) {
+		case BExpr::Const: {
+			/* one slot per constant node and generation (the plan may be generated again,
+			 * e.g. for a batch, with a different parameter layout) */
+			auto it = const_slot.find(e.get());
+			if (it == const_slot.end()) {
 				params.push_back((unsigned long long)e->cval);
-				e->param = (int)params.size() - 1;
+				it = const_slot.emplace(e.get(), (int)params.size() - 1).first;
 			}
-			return "((int64_t)p.v[" + std::to_string(e->param) + "])";
+			return "((int64_t)p.v[" + std::to_string(it->second) + "])";
+		}
 		case BExpr::ProbeOut:
 			return "pay" + std::to_string(e->probe) + "_" + std::to_string(e->pidx) + "[" + v + "]";
 		case BExpr::Fun: {
@@ -1202,6 +1207,9 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 	}
 	src << "      default: break;\n      }\n";
 	src << "    } else if (threadIdx.x == 0) {\n      atomicOr(err, VD_ERR_WAIT_TIMEOUT);\n    }\n";
+	/* every thread's stores (payloads, results) are device-visible before the item counts
+	 * as done */
+	src << "    __threadfence();\n";
 	src << "    __syncthreads();\n";
 	src << "    if (threadIdx.x == 0) {\n";
 	src << "      __threadfence();\n";

@@ -99,7 +99,6 @@ struct BExpr {
 	enum Kind { Col, Const, ProbeOut, Fun } kind;
 	int col = -1;              /* Col: index into Pipeline::cols */
 	int64_t cval = 0;          /* Const */
-	int param = -1;            /* Const: parameter slot */
 	int probe = -1, pidx = -1; /* ProbeOut: op index, payload index */
 	std::string fn;            /* Fun: lt le gt ge eq ne and or add sub mul */
 	std::vector<BExprP> args;

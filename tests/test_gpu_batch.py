@@ -28,19 +28,22 @@ def test_mixed_batch_matches_oracle_and_is_repeatable():
     specs += ["star:rows=50000,custs=3000,supps=200,parts=14000,seed=9", "groupby:rows=0,keys=10,seed=1",
               "sel_aggr:rows=1,seed=2", "join_aggr:build=0,probe=100,seed=3"]
     engines, queries, expect = _setup(specs)
+    for s, q, e in zip(specs, queries, expect):
+        q.run()
+        assert q.result_lines() == e, s
     b = Batch(queries, tiles_per_item=2)
     assert b.info()["work_items"] >= len(specs)
     for _ in range(3):
         b.run()
         b.wait()
-        for q, e in zip(queries, expect):
-            assert q.result_lines() == e
+        for s, q, e in zip(specs, queries, expect):
+            assert q.result_lines() == e, s
     lat = b.latencies_us()
     assert all(x >= 0 for x in lat)
     # the same queries still run on their own afterwards
-    for q, e in zip(queries[:4], expect[:4]):
+    for s, q, e in zip(specs, queries, expect):
         q.run()
-        assert q.result_lines() == e
+        assert q.result_lines() == e, s
 
 
 def test_batch_with_per_query_flavors():

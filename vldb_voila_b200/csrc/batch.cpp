@@ -104,7 +104,13 @@ static void batch_prepare(Batch& b, const std::vector<Flavor>& flavors, int64_t 
 	VC_CHECK_CUDA(cudaLibraryGetKernel(&b.kernel, b.mod->lib, "vc_batch"));
 	b.smem = bc.smem;
 	if (b.smem > 0) {
-		VC_CHECK_CUDA(cudaFuncSetAttribute((const void*)b.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.smem));
+		/* batches of one shape share the kernel: the limit only grows */
+		cudaFuncAttributes fa;
+		VC_CHECK_CUDA(cudaFuncGetAttributes(&fa, (const void*)b.kernel));
+		if ((size_t)fa.maxDynamicSharedSizeBytes < b.smem) {
+			VC_CHECK_CUDA(cudaFuncSetAttribute((const void*)b.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				(int)b.smem));
+		}
 	}
 	VC_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b.occupancy, (const void*)b.kernel, b.flavor.threads,
 		b.smem));

@@ -1092,6 +1092,9 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 				throw Error(6, "batched queries need direct join builds (build=staged is not batchable)");
 			}
 			std::vector<unsigned long long> prm;
+			/* the query keeps its own parameter layout for standalone runs */
+			const int saved_err = p.err_slot;
+			const std::vector<int> saved_cols = p.col_slots;
 			PipeGen g(p, q.plan, fl, st.pipes[p.id], qs, prm);
 			g.item = true;
 			g.name = "VCSHAPE";
@@ -1103,6 +1106,8 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 				Column* col = q.eng->tables.at(p.cols[c].table).find(p.cols[c].name);
 				prm[p.col_slots[c]] = (unsigned long long)(uintptr_t)col->dev;
 			}
+			p.err_slot = saved_err;
+			p.col_slots = saved_cols;
 			const int64_t poff = (int64_t)bc.params.size();
 			bc.params.insert(bc.params.end(), prm.begin(), prm.end());
 

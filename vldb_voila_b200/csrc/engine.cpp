@@ -317,8 +317,14 @@ void query_prepare(Query& q)
 		cudaKernel_t k;
 		VC_CHECK_CUDA(cudaLibraryGetKernel(&k, q.mod->lib, l.kernel.c_str()));
 		if (l.smem > 0) {
-			/* static + dynamic shared memory above 48 KiB needs the opt-in */
-			VC_CHECK_CUDA(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem));
+			/* static + dynamic shared memory above 48 KiB needs the opt-in.  Queries of one
+			 * shape share this kernel with different (runtime-sized) shared memory, so the
+			 * limit only ever grows. */
+			cudaFuncAttributes fa;
+			VC_CHECK_CUDA(cudaFuncGetAttributes(&fa, (const void*)k));
+			if ((size_t)fa.maxDynamicSharedSizeBytes < l.smem) {
+				VC_CHECK_CUDA(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem));
+			}
 		}
 		int occ = 0;
 		VC_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k, l.threads, l.smem));

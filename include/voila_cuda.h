@@ -168,6 +168,26 @@ int vc_query_profile(vc_query* q, int enable);
  * timed hot repetitions, compiler.cpp:521-575). */
 int vc_query_time(vc_query* q, int reps, int flush_l2, void* stream, float* ms_out, int cap);
 
+/* ---------------------------------------------------------------- no allocation ------- */
+
+/* The hash join + global aggregate pipeline (a join_aggr query: build rows with
+ * build_attr < attr_threshold form a Join01 table on build_key; every probe row whose
+ * probe_key is in it contributes probe_val) without any device allocation.  This entry point
+ * has no counterpart in the reference.  It is for callers that cannot call cudaMalloc --
+ * code running where allocation is forbidden or unsafe (host callbacks, allocator-owned
+ * device memory, allocation-free service paths).  All pointers are caller-owned device
+ * memory; out receives 3 int64: sum(probe_val) over matches, the match count, and error
+ * bits (0 = none).
+ * Limit: at most 2,097,152 build rows (the join table is a static 4 Mi-slot, 32 MiB device
+ * array that every GPU loading the library keeps until the process exits); larger inputs fail
+ * with VC_ERR_INVALID.  The first call on a device looks the arrays' addresses up
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All calls on a device
+ * share the arrays and the last call's contents remain (each call clears what it uses);
+ * calls that overlap on the GPU race and give wrong results. */
+int vc_join_aggr_noalloc(const int32_t* build_key, const int32_t* build_attr, int64_t build_rows,
+	int32_t attr_threshold, const int32_t* probe_key, const int64_t* probe_val, int64_t probe_rows, int64_t* out,
+	void* stream);
+
 /* ---------------------------------------------------------------- batches ------------- */
 
 /* Many queries in one persistent kernel driven by a device work queue, launched from a

@@ -254,12 +254,15 @@ def main():
     def step():
         q.run(stream)
 
+    from vldb_voila_b200.shards import merge_partials, plan_group_keys
+
+    nkeys = plan_group_keys(w.plan)
+
     def combine():
-        if world > 1 and w.template == "join_aggr":
-            part = torch.from_numpy(q.result().reshape(-1).astype(np.int64)).cuda()
-            if part.numel() == 0:
-                part = torch.zeros(2, dtype=torch.int64, device="cuda")
-            dist.all_reduce(part)
+        """Exchange step: merge the ranks' partial aggregates (vldb_voila_b200/shards.py)."""
+        if world > 1:
+            part = q.result()
+            merge_partials(part, nkeys, part.shape[1], device="cuda")
 
     for i in range(args.warmup):
         flush.fill_(i & 0xff)
@@ -390,5 +393,113 @@ def main():
     return 0
 
 
+def run_config5(args):
+    """The mixed batch: 256 seeded pipelines (sizes log-uniform 1e4..6e7 rows, selectivities
+    1-100 %, Zipf 0-1.25) run (a) one query after another with exhaustively tuned flavors and
+    (b) as one persistent-kernel batch with learned-chooser flavors.  Also reports the learned
+    choices' time against the exhaustive best on these held-out pipelines."""
+    import numpy as np
+    import torch
+
+    from vldb_voila_b200 import chooser as ch
+    from vldb_voila_b200 import Engine, workload
+    from vldb_voila_b200.engine import Batch, batch_specs
+
+    torch.cuda.set_device(0)
+    n = int(os.environ.get("VC_BATCH_N", "256"))
+    max_rows = int(float(os.environ.get("VC_BATCH_MAX_ROWS", "60000000")))
+    specs = batch_specs(n, 5, 10_000, max_rows)
+    t0 = time.time()
+    # learned chooser: trained on autotuner timings of separate seeded workloads
+    train = ch.training_specs(int(os.environ.get("VC_TRAIN_N", "48")), seed=21, min_rows=100_000, max_rows=20_000_000)
+    records = [{"spec": s, "features": ch.features(s).tolist(), "times_ms": ch.autotune(s, reps=3)} for s in train]
+    chooser = ch.Chooser()
+    loss = chooser.fit(records)
+    t_train = time.time() - t0
+
+    engines, queries_tuned, tuned, learned, records5 = [], [], [], [], []
+    for s in specs:
+        w = workload(s)
+        e = Engine(0)
+        e.load_workload(w, on_device=True)
+        times = ch.autotune(s, reps=3, engine=e)
+        best = min(times, key=times.get)
+        pick = chooser.choose(s)
+        records5.append({"spec": s, "best": best, "best_ms": times[best], "chosen": pick, "chosen_ms": times[pick],
+                         "default_ms": times[ch.DEFAULT]})
+        tuned.append(best)
+        learned.append(pick)
+        engines.append(e)
+        queries_tuned.append(e.query(w.plan, best))
+    torch.cuda.synchronize()
+    t_tune = time.time() - t0 - t_train
+
+    stream = torch.cuda.current_stream()
+    # (a) per-pipeline launches, one query after another, tuned flavors
+    for q in queries_tuned[:8]:
+        q.run(stream)
+    torch.cuda.synchronize()
+    plain_ms, plain_lat = [], []
+    for rep in range(args.steps):
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(queries_tuned) + 1)]
+        evs[0].record(stream)
+        for i, q in enumerate(queries_tuned):
+            q.run(stream)
+            evs[i + 1].record(stream)
+        evs[-1].synchronize()
+        plain_ms.append(evs[0].elapsed_time(evs[-1]))
+        plain_lat = [evs[0].elapsed_time(e) * 1000.0 for e in evs[1:]]
+    expect = [q.result_lines() for q in queries_tuned]
+
+    # (b) one persistent kernel over all pipelines, learned flavors
+    # batched pipelines build their join tables directly (one work phase per table)
+    batch_flavors = [f.replace("build=staged", "build=direct") if "build=" in f else f.replace("cuda(", "cuda(build=direct,", 1)
+                     for f in learned]
+    queries_learned = [e.query(workload(s).plan, f) for e, s, f in zip(engines, specs, batch_flavors)]
+    batch = Batch(queries_learned, threads=256, tiles_per_item=64)
+    for _ in range(2):
+        batch.run(stream)
+        batch.wait()
+    batch_ms, batch_lat = [], []
+    for rep in range(args.steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        batch.run(stream)
+        b.record(stream)
+        batch.wait()
+        batch_ms.append(a.elapsed_time(b))
+        batch_lat = batch.latencies_us()
+    exact = all(q.result_lines() == e for q, e in zip(queries_learned, expect))
+
+    ratio = [r["chosen_ms"] / r["best_ms"] for r in records5]
+    rows = sum(workload(s).fact_rows for s in specs)
+    p = lambda xs, k: float(np.percentile(xs, k))
+    line = {
+        "metric": "mixed batch of pipelines: total time, batched persistent kernel vs per-pipeline launches",
+        "value": statistics.median(plain_ms) / statistics.median(batch_ms), "unit": "x (per-pipeline / batched)",
+        "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": f"{n} pipelines batch_specs(seed=5, 1e4..{max_rows:.0e} rows)", "fact_rows": rows,
+                   "batch_info": batch.info()},
+        "batched_ms": statistics.median(batch_ms), "per_pipeline_ms": statistics.median(plain_ms),
+        "batched_rows_per_s": rows / (statistics.median(batch_ms) / 1e3),
+        "latency_us": {"batched_p50": p(batch_lat, 50), "batched_p99": p(batch_lat, 99),
+                       "per_pipeline_p50": p(plain_lat, 50), "per_pipeline_p99": p(plain_lat, 99)},
+        "results_identical": exact,
+        "chooser": {"train_workloads": len(train), "train_loss": loss, "heldout_pipelines": len(records5),
+                    "geomean_chosen_over_best": float(np.exp(np.mean(np.log(ratio)))),
+                    "max_chosen_over_best": float(np.max(ratio)),
+                    "within_10pct_fraction": float(np.mean([r <= 1.10 for r in ratio])),
+                    "sum_chosen_ms": sum(r["chosen_ms"] for r in records5),
+                    "sum_best_ms": sum(r["best_ms"] for r in records5),
+                    "sum_default_ms": sum(r["default_ms"] for r in records5)},
+        "setup_s": {"train": round(t_train, 1), "tune": round(t_tune, 1)},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 if __name__ == "__main__":
+    if "--workload" in sys.argv and sys.argv[sys.argv.index("--workload") + 1] == "config5":
+        sys.exit(run_config5(parse()))
     sys.exit(main())

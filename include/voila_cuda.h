@@ -198,7 +198,9 @@ int vc_join_aggr_noalloc(const int32_t* build_key, const int32_t* build_attr, in
  * their extraction).  The queries keep their device state and results: after
  * vc_batch_run + vc_batch_wait, vc_query_result_* read each query's rows.  The queries must
  * outlive the batch.  flavors may be NULL (each query's own) or hold one flavor per query
- * (NULL entries = the query's own).  tiles_per_item: tiles of a pipeline per work item. */
+ * (NULL entries = the query's own).  tiles_per_item: tiles of a pipeline per work item.
+ * Inside a batch, loads are plain (load=ldg), lowcard=private runs as lowcard=combine and
+ * cache= is capped at 256 slots, since every CTA reserves the largest shape's shared memory. */
 typedef struct vc_batch vc_batch;
 int vc_batch_new(vc_query** queries, int n, const char** flavors, int threads, int64_t tiles_per_item, vc_batch** out);
 int vc_batch_run(vc_batch* b, void* stream);
@@ -207,6 +209,8 @@ int vc_batch_wait(vc_batch* b);
 /* Completion time of each query, in microseconds since the batch kernel started. */
 int vc_batch_latencies(vc_batch* b, double* us, int n);
 int vc_batch_info(vc_batch* b, char* buf, size_t cap, size_t* len);
+/* The generated CUDA source of the batch's persistent kernel. */
+int vc_batch_source(vc_batch* b, char* buf, size_t cap, size_t* len);
 int vc_batch_free(vc_batch* b);
 
 /* ---------------------------------------------------------------- flavor chooser ------ */

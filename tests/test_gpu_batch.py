@@ -55,3 +55,20 @@ def test_batch_with_per_query_flavors():
     b.wait()
     for q, e in zip(queries, expect):
         assert q.result_lines() == e
+
+
+def test_batch_mixing_smem_and_probe_heavy_shapes():
+    """Dense shared-memory group-bys, the shared-memory group cache and the plain hash
+    group-by in one persistent kernel.  Warps leave the hash probe loops at different times;
+    this mix once made the warps of a CTA drift onto different work items at a block
+    barrier, so every run of it is checked against the oracle."""
+    specs = batch_specs(12, seed=4, min_rows=10_000, max_rows=200_000)
+    cache, lean = "cuda(aggr=cache,cache=128)", "cuda(prefetch=0,rows=2)"
+    choice = ["", cache, lean, ""]
+    engines, queries, expect = _setup(specs)
+    b = Batch(queries, flavors=[choice[i % 4] for i in range(len(specs))], threads=128, tiles_per_item=4)
+    for _ in range(4):
+        b.run()
+        b.wait()
+        for s, q, e in zip(specs, queries, expect):
+            assert q.result_lines() == e, s

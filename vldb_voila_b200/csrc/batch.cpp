@@ -288,6 +288,24 @@ int vc_batch_info(vc_batch* h, char* buf, size_t cap, size_t* len)
 	});
 }
 
+int vc_batch_source(vc_batch* h, char* buf, size_t cap, size_t* len)
+{
+	return abi_guard_mlp([&] {
+		if (!h) {
+			throw Error(VC_ERR_INVALID, "null batch");
+		}
+		const std::string& s = h->b.source;
+		if (len) {
+			*len = s.size();
+		}
+		if (buf && cap) {
+			const size_t k = std::min(cap - 1, s.size());
+			std::memcpy(buf, s.data(), k);
+			buf[k] = 0;
+		}
+	});
+}
+
 int vc_batch_free(vc_batch* h)
 {
 	return abi_guard_mlp([&] { delete h; });

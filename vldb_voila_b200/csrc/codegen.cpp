@@ -286,7 +286,7 @@ struct PipeGen {
 		o << "  if (threadIdx.x == 0) {\n";
 		o << "    for (int s = 0; s < " << S << "; s++) { vd::mbar_init(&full[s], 1); }\n";
 		o << "    vd::mbar_init_fence();\n";
-		o << "  }\n  __syncthreads();\n";
+		o << "  }\n  vd::block_sync();\n";
 		/* issue helper as a lambda */
 		o << "  auto issue = [&](int64_t j) {\n";
 		o << "    const int64_t tj = (int64_t)blockIdx.x + j * (int64_t)gridDim.x;\n";
@@ -315,10 +315,10 @@ struct PipeGen {
 		o << "    if (threadIdx.x == 0) { vd::fence_proxy_async(); issue(i + " << S - 1 << "); }\n";
 		o << "    const int s = (int)(i % " << S << ");\n";
 		o << "    const bool ok = vd::mbar_wait(&full[s], (uint32_t)((i / " << S << ") & 1));\n";
-		o << "    if (__syncthreads_or(!ok)) { timed_out = true; break; }\n";
+		o << "    if (vd::block_any(!ok)) { timed_out = true; break; }\n";
 		o << "    const unsigned char* stage = stages + (size_t)s * " << tile_bytes << ";\n";
 		emit_body("smem");
-		o << "    __syncthreads();\n";
+		o << "    vd::block_sync();\n";
 		o << "  }\n";
 		o << "  if (timed_out) {\n";
 		o << "    if (threadIdx.x == 0) {\n";
@@ -327,7 +327,7 @@ struct PipeGen {
 		o << "        if ((int64_t)blockIdx.x + j * (int64_t)gridDim.x < nfull) {\n";
 		o << "          vd::mbar_wait(&full[j % " << S << "], (uint32_t)((j / " << S << ") & 1), 100000000ull);\n";
 		o << "        }\n      }\n    }\n";
-		o << "    __syncthreads();\n";
+		o << "    vd::block_sync();\n";
 		o << "  } else if (nfull < ntiles && (int64_t)blockIdx.x == nfull % (int64_t)gridDim.x) {\n";
 		o << "    const int64_t t = nfull;\n";
 		emit_body("ldg");
@@ -480,7 +480,7 @@ struct PipeGen {
 			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) { if (act[v]) { ccar" << k
 			  << "[csel_pos[v]] = pay" << carried[k].first << "_" << carried[k].second << "[v]; } }\n";
 		}
-		o << "    __syncthreads();\n";
+		o << "    vd::block_sync();\n";
 		o << "    for (int base = 0; base < nsel; base += " << T << ") {\n";
 		o << "      const int ci = base + (int)threadIdx.x;\n";
 		o << "      const bool live = ci < nsel;\n";
@@ -500,7 +500,7 @@ struct PipeGen {
 		sink_row();
 		V = saveV;
 		o << "    }\n";
-		o << "    __syncthreads();\n";
+		o << "    vd::block_sync();\n";
 		o << "    }\n";
 	}
 
@@ -594,7 +594,7 @@ struct PipeGen {
 				o << "  unsigned long long* const sacc0 = (unsigned long long*)vd_smem;\n";
 				o << "  for (int64_t i = threadIdx.x; i < " << P((unsigned long long)(D * A() * replicas))
 				  << "; i += blockDim.x) { sacc0[i] = 0ull; }\n";
-				o << "  __syncthreads();\n";
+				o << "  vd::block_sync();\n";
 				if (replicas > 1) {
 					o << "  unsigned long long* const sacc = sacc0 + (threadIdx.x >> 5) * " << P((unsigned long long)(D * A()))
 					  << ";\n";
@@ -622,7 +622,7 @@ struct PipeGen {
 				o << "  if (threadIdx.x == 0) { *pncodes = 0; }\n";
 				o << "#pragma unroll\n  for (int i = 0; i < " << kGmax * A() << "; i++) { priv[i * " << T
 				  << " + threadIdx.x] = 0; }\n";
-				o << "  __syncthreads();\n";
+				o << "  vd::block_sync();\n";
 			}
 			break;
 		}
@@ -634,7 +634,7 @@ struct PipeGen {
 				smem_sink = (size_t)S * (1 + A()) * 8;
 				o << "  unsigned long long* const scache = (unsigned long long*)vd_smem;\n";
 				o << "  for (int i = threadIdx.x; i < " << S * (1 + A()) << "; i += blockDim.x) { scache[i] = 0ull; }\n";
-				o << "  __syncthreads();\n";
+				o << "  vd::block_sync();\n";
 				cache_slots = S;
 			}
 			break;
@@ -822,7 +822,7 @@ struct PipeGen {
 			if (private_acc) {
 				/* fold the private accumulators into the block's slot array: one warp per
 				 * (code, aggregate) pair, lanes striding over the threads' copies */
-				o << "  __syncthreads();\n";
+				o << "  vd::block_sync();\n";
 				o << "  {\n    const int ng = min(*pncodes, " << kGmax << ");\n";
 				o << "    for (int pr = (int)(threadIdx.x >> 5); pr < ng * " << A() << "; pr += (int)(blockDim.x >> 5)) {\n";
 				o << "      int64_t sum = 0;\n";
@@ -836,7 +836,7 @@ struct PipeGen {
 			}
 			if (dense_in_smem) {
 				const int64_t D = (int64_t)s.domain;
-				o << "  __syncthreads();\n";
+				o << "  vd::block_sync();\n";
 				o << "  for (int64_t i = threadIdx.x; i < " << P((unsigned long long)D) << "; i += blockDim.x) {\n";
 				o << "    unsigned long long sum[" << A() << "];\n";
 				o << "#pragma unroll\n    for (int a = 0; a < " << A() << "; a++) { sum[a] = 0ull; }\n";
@@ -853,7 +853,7 @@ struct PipeGen {
 			break;
 		case Sink::AggHash:
 			if (fl.aggr == "cache") {
-				o << "  __syncthreads();\n";
+				o << "  vd::block_sync();\n";
 				o << "  for (int i = threadIdx.x; i < " << cache_slots << "; i += blockDim.x) {\n";
 				o << "    const unsigned long long sk = scache[i * " << (1 + A()) << "];\n";
 				o << "    if (sk != 0ull) {\n";
@@ -1081,6 +1081,12 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 		Flavor fl = flavors[qi];
 		fl.threads = threads;
 		fl.load = "ldg";
+		/* every CTA of the persistent kernel reserves the largest shape's shared memory, so
+		 * the knobs that need much of it run as their lean equivalents inside a batch */
+		if (fl.lowcard == "private") {
+			fl.lowcard = "combine";
+		}
+		fl.cache_slots = std::min(fl.cache_slots, 256);
 		QueryDeviceState qs;
 		qs.out = q.out;
 		qs.out_cap = q.out_cap;
@@ -1165,8 +1171,33 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 			}
 		}
 	}
+	/* Within a phase, the pipelines' items are interleaved round-robin (pipelines with the
+	 * most items first), so that CTAs running at the same time work on different pipelines:
+	 * atomic-bound group-bys then overlap bandwidth-bound scans instead of the whole GPU
+	 * working through one pipeline at a time. */
 	for (auto& ph : phases) {
-		bc.items.insert(bc.items.end(), ph.begin(), ph.end());
+		std::map<int64_t, std::vector<BatchItem>> by_stage; /* key: parameter offset and done counter */
+		std::vector<int64_t> order;
+		for (auto& it : ph) {
+			const int64_t key = it.params * 4096 + it.done;
+			if (!by_stage.count(key)) {
+				order.push_back(key);
+			}
+			by_stage[key].push_back(it);
+		}
+		std::stable_sort(order.begin(), order.end(),
+			[&](int64_t a, int64_t b) { return by_stage[a].size() > by_stage[b].size(); });
+		std::vector<size_t> next(order.size(), 0);
+		for (bool any = true; any;) {
+			any = false;
+			for (size_t k = 0; k < order.size(); k++) {
+				auto& v = by_stage[order[k]];
+				if (next[k] < v.size()) {
+					bc.items.push_back(v[next[k]++]);
+					any = true;
+				}
+			}
+		}
 	}
 	bc.ncounters = ncounters;
 
@@ -1182,7 +1213,7 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 	src << "  if (threadIdx.x == 0) { atomicCAS(&finish_ns[nq], 0ull, (unsigned long long)vd::globaltimer_ns()); }\n";
 	src << "  for (;;) {\n";
 	src << "    if (threadIdx.x == 0) { s_w = (long long)atomicAdd(&counters[0], 1ull); }\n";
-	src << "    __syncthreads();\n";
+	src << "    vd::block_sync();\n";
 	src << "    const long long w = s_w;\n";
 	src << "    if (w >= nwork) { break; }\n";
 	src << "    const VcBatchItem it = items[w];\n";
@@ -1199,7 +1230,7 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 	src << "      }\n";
 	src << "      s_ok = ok;\n";
 	src << "    }\n";
-	src << "    __syncthreads();\n";
+	src << "    vd::block_sync();\n";
 	src << "    if (s_ok) {\n";
 	src << "      switch (it.shape) {\n";
 	src << "      case -1: {\n";
@@ -1215,7 +1246,7 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 	/* every thread's stores (payloads, results) are device-visible before the item counts
 	 * as done */
 	src << "    __threadfence();\n";
-	src << "    __syncthreads();\n";
+	src << "    vd::block_sync();\n";
 	src << "    if (threadIdx.x == 0) {\n";
 	src << "      __threadfence();\n";
 	src << "      const unsigned long long old = atomicAdd(&counters[it.done], 1ull);\n";

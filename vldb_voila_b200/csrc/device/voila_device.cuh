@@ -255,6 +255,30 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64
 
 /* ---------------------------------------------------------------- warp helpers --- */
 
+/* Block-wide barrier for code whose warps may arrive diverged.  __syncthreads() is the
+ * aligned form (bar.sync), which requires every warp to reach it converged; after the
+ * per-lane probe loops of the hash tables (early exits, data-dependent trip counts) lanes
+ * of a warp can arrive at different times, and on sm_100a an aligned barrier then let
+ * warps of one CTA drift onto different work items of the persistent batch kernel.  The
+ * non-aligned barrier counts every thread individually. */
+__device__ __forceinline__ void block_sync()
+{
+	asm volatile("barrier.sync 0;" ::: "memory");
+}
+
+/* block_sync() that also returns whether any thread passed `v` true (the non-aligned form
+ * of __syncthreads_or). */
+__device__ __forceinline__ bool block_any(bool v)
+{
+	unsigned r;
+	asm volatile(
+		"{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n barrier.red.or.pred q, 0, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+		: "=r"(r)
+		: "r"((unsigned)v)
+		: "memory");
+	return r != 0u;
+}
+
 __device__ __forceinline__ unsigned lane_id()
 {
 	return threadIdx.x & 31u;
@@ -311,7 +335,7 @@ __device__ __forceinline__ int64_t block_append(unsigned long long* cursor, bool
 	if (lane == 0) {
 		scratch[warp] = __popc(mask);
 	}
-	__syncthreads();
+	block_sync();
 	if (threadIdx.x == 0) {
 		unsigned long long total = 0;
 		for (unsigned w = 0; w < nw; w++) {
@@ -321,9 +345,9 @@ __device__ __forceinline__ int64_t block_append(unsigned long long* cursor, bool
 		}
 		scratch[32] = total ? atomicAdd(cursor, total) : 0ull;
 	}
-	__syncthreads();
+	block_sync();
 	const int64_t pos = (int64_t)(scratch[32] + scratch[warp]) + __popc(mask & ((1u << lane) - 1u));
-	__syncthreads();
+	block_sync();
 	return pos;
 }
 
@@ -351,7 +375,7 @@ __device__ __forceinline__ int block_compact(const bool (&act)[V], int off, int*
 	if (lane == 31) {
 		scan[warp] = x;
 	}
-	__syncthreads();
+	block_sync();
 	if (threadIdx.x == 0) {
 		int run = 0;
 		for (unsigned w = 0; w < nw; w++) {
@@ -361,7 +385,7 @@ __device__ __forceinline__ int block_compact(const bool (&act)[V], int off, int*
 		}
 		scan[32] = run;
 	}
-	__syncthreads();
+	block_sync();
 	int base = scan[warp] + x - cnt;
 #pragma unroll
 	for (int v = 0; v < V; v++) {
@@ -412,11 +436,11 @@ __device__ __forceinline__ int dict_code(int* dict, int* codes, int* ncodes, int
 __device__ __forceinline__ bool last_block_done(unsigned long long* counter, unsigned long long total, int* flag_smem)
 {
 	__threadfence();
-	__syncthreads();
+	block_sync();
 	if (threadIdx.x == 0) {
 		*flag_smem = atomicAdd(counter, 1ull) == total - 1ull;
 	}
-	__syncthreads();
+	block_sync();
 	const bool last = *flag_smem != 0;
 	if (last) {
 		__threadfence();
@@ -436,14 +460,14 @@ __device__ __forceinline__ void block_sum(int64_t (&vals)[A], int64_t* scratch /
 		}
 	}
 	const unsigned warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-	__syncthreads();
+	block_sync();
 	if (lane_id() == 0) {
 #pragma unroll
 		for (int a = 0; a < A; a++) {
 			scratch[warp * A + a] = vals[a];
 		}
 	}
-	__syncthreads();
+	block_sync();
 #pragma unroll
 	for (int a = 0; a < A; a++) {
 		int64_t s = 0;
@@ -452,7 +476,7 @@ __device__ __forceinline__ void block_sum(int64_t (&vals)[A], int64_t* scratch /
 		}
 		vals[a] = s;
 	}
-	__syncthreads();
+	block_sync();
 }
 
 /* ---------------------------------------------------------------- join tables ---- */

@@ -90,6 +90,7 @@ def lib():
         "vc_batch_wait": (c.c_int, [P]),
         "vc_batch_latencies": (c.c_int, [P, c.POINTER(c.c_double), c.c_int]),
         "vc_batch_info": (c.c_int, [P, P, c.c_size_t, c.POINTER(c.c_size_t)]),
+        "vc_batch_source": (c.c_int, [P, P, c.c_size_t, c.POINTER(c.c_size_t)]),
         "vc_batch_free": (c.c_int, [P]),
         "vc_query_timings": (c.c_int, [P, c.POINTER(c.c_float), c.c_int, c.POINTER(c.c_int), P, c.c_size_t]),
     }
@@ -424,6 +425,9 @@ class Batch:
     def info(self):
         import json
         return json.loads(_text_call(lib().vc_batch_info, self._h))
+
+    def source(self):
+        return _text_call(lib().vc_batch_source, self._h)
 
 
 class Mlp:

@@ -7,7 +7,7 @@ from vldb_voila_b200 import Engine, VoilaError, workload
 SPECS = ["sel_aggr:rows=1000", "join_aggr:build=100,probe=1000", "groupby:rows=1000,keys=100000,zipf=1.0",
          "groupby:rows=1000,keys=50", "star:rows=1000"]
 FLAVORS = ["", "cuda(load=tma,stages=2)", "cuda(lowcard=private,prefetch=0)", "cuda(aggr=cache,build=staged)",
-           "cuda(compact=0,rows=8,threads=128)", "cuda(hash=voila,compact=-1)"]
+           "cuda(compact=0,rows=8,threads=128)", "cuda(hash=voila,compact=-1)", "cuda(build=direct,prefetch=0)"]
 
 
 def offline(spec):
@@ -27,7 +27,10 @@ def test_workload_plans_compile_for_sm100a(spec, flavor):
     assert any(k["dominant"] for k in info["kernels"])
     assert "vc_p0_main" in src
     if w.template == "join_aggr":
-        assert "join_probe_bucket" in src
+        # small key spaces get a dense (direct-address) table unless a hash build is forced
+        hashed = "build=staged" in flavor or "build=direct" in flavor
+        assert ("join_probe_bucket" in src) == hashed
+        assert ("vd::dense_test" in src) == (not hashed)
     if "load=tma" in flavor and w.template != "star":
         assert "vd::bulk_load" in src and "mbar_wait" in src
 

@@ -15,7 +15,7 @@ CASES = sorted(manifest().items())
 FLAVORS = ["", "cuda(rows=8,threads=128,load=tma,stages=3)", "cuda(aggr=cache,cache=256,build=staged,compact=0)",
            "cuda(aggr=global,rows=1,threads=64,graph=0,prefetch=0,compact=-1)",
            "cuda(load=tma,build=staged,rows=2,lowcard=atomic)", "cuda(compact=0,lowcard=private,rows=8)",
-           "cuda(hash=voila,lowcard=private,threads=128,fill=75)"]
+           "cuda(hash=voila,lowcard=private,threads=128,fill=75)", "cuda(build=direct,prefetch=0)"]
 UNSUPPORTED = {"join_n"}  # JoinN probes are rejected by the CUDA flavor for now
 
 
@@ -62,7 +62,7 @@ def test_full_size_vs_oracle(spec):
     # the device generator produces the same columns; run from them (no host upload)
     e = Engine(0)
     e.load_workload(w, on_device=True)
-    for flavor in ["", "cuda(load=tma)", "cuda(build=staged,aggr=cache)"]:
+    for flavor in ["", "cuda(load=tma)", "cuda(build=staged,aggr=cache)", "cuda(build=direct)"]:
         q = e.query(w.plan, flavor)
         q.run()
         assert q.result_lines() == expect, flavor
@@ -101,7 +101,8 @@ EDGE_SPECS = [
 
 
 @pytest.mark.parametrize("spec", EDGE_SPECS)
-@pytest.mark.parametrize("flavor", ["", "cuda(rows=2,threads=32,aggr=global)", "cuda(load=tma,build=staged)"])
+@pytest.mark.parametrize("flavor", ["", "cuda(rows=2,threads=32,aggr=global)", "cuda(load=tma,build=staged)",
+                                    "cuda(build=direct,rows=1)"])
 def test_edge_cases_vs_oracle(spec, flavor):
     """Empty and ragged inputs, no matches, single keys (the reference itself asserts on
     empty base tables, codegen.cpp:445, so the oracle is the only checker there)."""

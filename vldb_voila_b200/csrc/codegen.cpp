@@ -517,6 +517,47 @@ struct PipeGen {
 		}
 	}
 
+	/* payload outputs of a probe from the packed payload `raw` */
+	void emit_payload_unpack(const Op& op, const JoinDesc& jd, const std::string& j, const std::string& raw) {
+		for (int k = 0; k < op.npay; k++) {
+			const int bits = (k + 1 < op.npay ? jd.pay_shift[k + 1] : jd.pay_bits) - jd.pay_shift[k];
+			const unsigned long long mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
+			o << "        pay" << j << "_" << k << "[v] = " << P((unsigned long long)(int64_t)jd.pay_b[k].lo)
+			  << " + (int64_t)(((uint64_t)" << raw << " >> " << P((unsigned long long)jd.pay_shift[k]) << ") & "
+			  << Pu(mask) << ");\n";
+		}
+	}
+
+	/* probe of a dense join table: the packed key indexes the table directly */
+	void gen_probe_dense(const Op& op, const JoinDesc& jd, const std::string& j) {
+		const int eb = jd.dense_entry_bytes();
+		const std::string ET = eb == 8 ? "unsigned long long" : "unsigned";
+		o << "    {\n";
+		o << "      const " << ET << "* __restrict__ jd" << j << " = " << Pptr(jd.table, "const " + ET + "*") << ";\n";
+		o << "#pragma unroll\n      for (int v = 0; v < " << V << "; v++) {\n";
+		std::string inrange = "act[v]";
+		std::string packed = "0ull";
+		for (size_t k = 0; k < op.keys.size(); k++) {
+			const std::string kv = expr(op.keys[k], "v");
+			const std::string lo = P((unsigned long long)(int64_t)jd.key_b[k].lo);
+			const std::string span = Pu((unsigned long long)(int64_t)(jd.key_b[k].hi - jd.key_b[k].lo));
+			inrange += " && (uint64_t)(" + kv + " - " + lo + ") <= " + span;
+			packed += " | ((uint64_t)(" + kv + " - " + lo + ") << " + P((unsigned long long)jd.key_shift[k]) + ")";
+		}
+		o << "        const bool ok = " << inrange << ";\n";
+		o << "        const uint64_t pk = " << packed << ";\n";
+		if (eb == 0) {
+			o << "        act[v] = ok && vd::dense_test(jd" << j << ", pk);\n";
+		} else {
+			o << "        const " << ET << " e = ok ? vd::table_ld(&jd" << j << "[pk]) : (" << ET << ")0;\n";
+			o << "        act[v] = e != 0;\n";
+			o << "        const uint64_t raw = e != 0 ? (uint64_t)e - 1ull : 0ull;\n";
+			emit_payload_unpack(op, jd, j, "raw");
+		}
+		o << "      }\n";
+		o << "    }\n";
+	}
+
 	void gen_probe(int opi, const Op& op) {
 		JoinDesc& jd = plan.joins[op.join];
 		if (!jd.join01) {
@@ -528,6 +569,10 @@ struct PipeGen {
 		const std::string j = std::to_string(opi);
 		for (int k = 0; k < op.npay; k++) {
 			o << "    int64_t pay" << j << "_" << k << "[" << V << "];\n";
+		}
+		if (jd.dense) {
+			gen_probe_dense(op, jd, j);
+			return;
 		}
 		o << "    {\n";
 		o << "      const " << S << "* __restrict__ jt = " << Pptr(jd.table, "const " + S + "*") << ";\n";
@@ -564,13 +609,7 @@ struct PipeGen {
 		o << "          st[v] = vd::join_probe_bucket(jt, bk[v], key[v], raw[v]);\n";
 		o << "        }\n";
 		o << "        act[v] = st[v] == 1;\n";
-		for (int k = 0; k < op.npay; k++) {
-			const int bits = (k + 1 < op.npay ? jd.pay_shift[k + 1] : jd.pay_bits) - jd.pay_shift[k];
-			const unsigned long long mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
-			o << "        pay" << j << "_" << k << "[v] = " << P((unsigned long long)(int64_t)jd.pay_b[k].lo)
-			  << " + (int64_t)(((uint64_t)raw[v] >> " << P((unsigned long long)jd.pay_shift[k]) << ") & "
-			  << Pu(mask) << ");\n";
-		}
+		emit_payload_unpack(op, jd, j, "raw[v]");
 		o << "      }\n";
 		o << "    }\n";
 	}
@@ -641,7 +680,10 @@ struct PipeGen {
 		case Sink::JoinBuild: {
 			JoinDesc& jd = plan.joins[s.join];
 			const std::string S = join_slot_type(jd);
-			if (jd.direct) {
+			if (jd.dense) {
+				const std::string ET = jd.dense_entry_bytes() == 8 ? "unsigned long long" : "unsigned";
+				o << "  " << ET << "* const jdt = " << Pptr(jd.table, ET + "*") << ";\n";
+			} else if (jd.direct) {
 				o << "  " << S << "* const jt = " << Pptr(jd.table, S + "*") << ";\n";
 				o << "  const uint64_t bmask = " << Pu(jd.direct_bmask) << ";\n";
 			} else {
@@ -741,7 +783,17 @@ struct PipeGen {
 			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
 			const std::string pk = packed_key(s.keys, jd.key_b, jd.key_shift, "v");
 			const std::string pp = s.pay.empty() ? std::string("0ull") : packed_key(s.pay, jd.pay_b, jd.pay_shift, "v");
-			if (jd.direct) {
+			if (jd.dense) {
+				o << "      if (act[v]) {\n";
+				o << "        const uint64_t pkb = " << pk << ";\n";
+				if (jd.dense_entry_bytes() == 0) {
+					o << "        vd::dense_set(jdt, pkb);\n";
+				} else {
+					const std::string ET = jd.dense_entry_bytes() == 8 ? "unsigned long long" : "unsigned";
+					o << "        atomicCAS(&jdt[pkb], (" << ET << ")0, (" << ET << ")(" << pp << " + 1ull));\n";
+				}
+				o << "      }\n    }\n";
+			} else if (jd.direct) {
 				o << "      if (act[v]) {\n";
 				o << "        const uint64_t pkb = " << pk << ";\n";
 				o << "        vd::join_insert(jt, bmask, " << table_hash(s.keys, "pkb", jd.key_bits, "v") << ", (" << KT

@@ -511,6 +511,32 @@ __device__ __forceinline__ uint64_t join_buckets(uint64_t count)
 	return slots / spb;
 }
 
+/* One word of a join table: from L2 when the table was built earlier in the same persistent
+ * kernel, else through the read-only path. */
+template <typename T>
+__device__ __forceinline__ T table_ld(const T* p)
+{
+#ifdef VD_COHERENT_TABLES
+	return __ldcg(p);
+#else
+	return __ldg(p);
+#endif
+}
+
+/* Dense join tables (packed build key = array index; the key space is small enough that
+ * no hashing is needed).  Without payload the table is a bitmap of keys present; with a
+ * payload each entry holds payload + 1 (0 = absent) and the first inserted row wins, as in
+ * the hash table. */
+__device__ __forceinline__ void dense_set(unsigned* bits, uint64_t pk)
+{
+	atomicOr(&bits[pk >> 5], 1u << (unsigned)(pk & 31u));
+}
+
+__device__ __forceinline__ bool dense_test(const unsigned* bits, uint64_t pk)
+{
+	return ((table_ld(&bits[pk >> 5]) >> (unsigned)(pk & 31u)) & 1u) != 0u;
+}
+
 /* Looks `key` up in bucket b: 1 = found (payload in pay), 0 = absent (an empty slot ends the
  * probe sequence), 2 = bucket full without a match (continue with the next bucket). */
 template <typename KeyT, typename PayT>

@@ -138,8 +138,8 @@ Flavor Flavor::parse(const std::string& s0)
 		} else if (k == "fill") {
 			f.fill = num(10, 90);
 		} else if (k == "build") {
-			if (v != "auto" && v != "direct" && v != "staged") {
-				throw Error(1, "build must be auto, direct or staged");
+			if (v != "auto" && v != "direct" && v != "staged" && v != "dense") {
+				throw Error(1, "build must be auto, direct, staged or dense");
 			}
 			f.build = v;
 		} else {
@@ -245,7 +245,24 @@ void query_prepare(Query& q)
 		jd.max_buckets = slots / spb;
 		jd.table_bytes = (size_t)slots * sb;
 		const std::string& bm = q.flavor.build;
-		jd.direct = bm == "direct" || (bm == "auto" && (int64_t)jd.table_bytes <= q.flavor.direct_limit);
+		/* a dense table when the packed key space is small: one access per probe and no
+		 * larger than the hash table would be (a bitmap when there is no payload) */
+		size_t dense_bytes = 0;
+		if (jd.key_bits <= 30) {
+			const uint64_t span = 1ull << jd.key_bits;
+			const int eb = jd.dense_entry_bytes();
+			dense_bytes = eb == 0 ? (size_t)std::max<uint64_t>((span + 31) / 32, 1) * 4 : (size_t)(span * eb);
+			dense_bytes = (dense_bytes + 15) & ~(size_t)15;
+		}
+		if (bm == "dense" && dense_bytes == 0) {
+			throw Error(VC_ERR_UNSUPPORTED, "build=dense needs a join key space of at most 2^30 values");
+		}
+		jd.dense = dense_bytes > 0 &&
+			(bm == "dense" || (bm == "auto" && dense_bytes <= std::max<size_t>(jd.table_bytes, 1 << 20)));
+		if (jd.dense) {
+			jd.table_bytes = dense_bytes;
+		}
+		jd.direct = jd.dense || bm == "direct" || (bm == "auto" && (int64_t)jd.table_bytes <= q.flavor.direct_limit);
 		jd.direct_bmask = (uint64_t)(jd.max_buckets - 1);
 		jd.table = dev_alloc(q, jd.table_bytes);
 		jd.words = (unsigned long long*)arena_take(32);

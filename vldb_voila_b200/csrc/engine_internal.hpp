@@ -124,7 +124,10 @@ struct JoinDesc {
 	bool direct = false;             /* build inserts directly into a table sized for build_rows */
 	uint64_t direct_bmask = 0;       /* bucket mask of the direct table */
 	size_t table_bytes = 0;
+	bool dense = false;              /* direct-address table indexed by the packed key */
 	int slot_bytes() const { return (key64 || pay64) ? 16 : 8; }
+	/* entry width of a dense table: 0 = bitmap (no payload), else 4 or 8 bytes of payload + 1 */
+	int dense_entry_bytes() const { return pay_bits == 0 ? 0 : (pay_bits <= 31 ? 4 : 8); }
 };
 
 struct Op {
@@ -185,7 +188,7 @@ struct Flavor {
 	bool graph = true;        /* replay the query's launches from a CUDA graph */
 	std::string load = "ldg"; /* column tiles: ldg (vector loads) | tma (bulk copies into a smem ring) */
 	int stages = 4;           /* tma ring depth */
-	std::string build = "auto"; /* join build: auto | direct | staged */
+	std::string build = "auto"; /* join build: auto | direct | staged | dense */
 	bool prefetch = true;     /* ldg: load the next tile while the current one is processed */
 	int compact = -2;         /* compact survivors after op k (-1 never, -2 auto) */
 	std::string lowcard = "combine"; /* dense aggregation: combine (warp pre-sum) | atomic (per-warp replicas)

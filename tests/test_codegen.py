@@ -87,3 +87,12 @@ def test_bad_flavors_are_rejected(flavor):
     with pytest.raises(VoilaError) as ex:
         e.query(w.plan, flavor)
     assert ex.value.code == 1
+
+
+def test_flavor_beyond_the_shared_memory_limit_is_rejected_at_creation():
+    # an 8-row, 512-thread TMA tile ring with 4 stages needs more than 227 KiB per CTA
+    w, e = offline("sel_aggr:rows=6000000")
+    with pytest.raises(VoilaError) as ex:
+        e.query(w.plan, "cuda(threads=512,rows=8,load=tma,stages=4)")
+    assert ex.value.code == 6
+    assert "shared memory" in str(ex.value)

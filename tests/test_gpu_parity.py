@@ -15,7 +15,8 @@ CASES = sorted(manifest().items())
 FLAVORS = ["", "cuda(rows=8,threads=128,load=tma,stages=3)", "cuda(aggr=cache,cache=256,build=staged,compact=0)",
            "cuda(aggr=global,rows=1,threads=64,graph=0,prefetch=0,compact=-1)",
            "cuda(load=tma,build=staged,rows=2,lowcard=atomic)", "cuda(compact=0,lowcard=private,rows=8)",
-           "cuda(hash=voila,lowcard=private,threads=128,fill=75)", "cuda(build=direct,prefetch=0)"]
+           "cuda(hash=voila,lowcard=private,threads=128,fill=75)", "cuda(build=direct,prefetch=0)",
+           "cuda(lowcard=redux,aggr=cache,cache=64)"]
 UNSUPPORTED = {"join_n"}  # JoinN probes are rejected by the CUDA flavor for now
 
 

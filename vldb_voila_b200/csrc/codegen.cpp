@@ -73,7 +73,8 @@ struct PipeGen {
 	size_t smem_total = 0;
 	int cache_slots = 0;
 	bool dense_in_smem = false;
-	int replicas = 1;          /* per-warp copies of the dense slot array (lowcard=atomic) */
+	int replicas = 1;          /* copies of the dense slot array (per warp or per group of warps) */
+	bool leader_plain = false; /* each warp owns a copy: group leaders update it without atomics */
 	std::map<const BExpr*, int> const_slot; /* parameter slot of each constant node */
 	bool private_acc = false;  /* per-thread private accumulators (lowcard=private) */
 	static constexpr int kGmax = 8; /* distinct groups per block held in private accumulators */
@@ -134,6 +135,36 @@ struct PipeGen {
 	}
 
 	int A() const { return (int)p.sink.aggs.size(); }
+
+	/* Warp pre-aggregation of one row per lane: the lanes holding the same group key (`key`,
+	 * a 32- or 64-bit expression that is `sentinel` on inactive lanes) form a group; each
+	 * aggregate is summed over the group with redux.sync on the value biased by its lower
+	 * bound (so it is non-negative and has a known bit width), and `lead` marks the lowest
+	 * active lane of each group, which then holds the group's sums in vals[]. */
+	void emit_group_reduce(const std::string& key) {
+		o << "      const unsigned gm = __match_any_sync(0xffffffffu, " << key << ");\n";
+		o << "      const bool lead = act[v] && (gm & vd::lanemask_lt()) == 0u;\n";
+		o << "      const uint64_t gn = (uint64_t)__popc(gm);\n";
+		for (int a = 0; a < A(); a++) {
+			const auto& ag = p.sink.aggs[a];
+			if (ag.count) {
+				o << "      vals[" << a << "] = (int64_t)gn;\n";
+				continue;
+			}
+			const __int128 span = ag.arg->b.hi - ag.arg->b.lo;
+			int bits = 64;
+			if (span >= 0 && span < ((__int128)1 << 64)) {
+				bits = 0;
+				for (unsigned __int128 x = (unsigned __int128)span; x; x >>= 1) {
+					bits++;
+				}
+				bits = std::max(bits, 1);
+			}
+			const std::string lo = P((unsigned long long)(int64_t)ag.arg->b.lo);
+			o << "      vals[" << a << "] = (int64_t)(vd::group_sum_u<" << bits << ">(gm, (uint64_t)vals[" << a
+			  << "] - (uint64_t)" << lo << ") + (uint64_t)" << lo << " * gn);\n";
+		}
+	}
 
 	std::string agg_vals(const std::string& v) {
 		std::ostringstream s;
@@ -626,8 +657,22 @@ struct PipeGen {
 		case Sink::AggDense: {
 			const int64_t D = (int64_t)s.domain;
 			const int64_t warps = T / 32;
-			replicas = fl.lowcard == "atomic" && D * A() * 8 * warps <= 96 * 1024 ? (int)warps : 1;
-			dense_in_smem = D * A() * 8 * replicas <= 96 * 1024;
+			const int64_t slot_bytes = D * A() * 8;
+			if (fl.lowcard == "atomic") {
+				replicas = slot_bytes * warps <= 96 * 1024 ? (int)warps : 1;
+			} else if (fl.lowcard == "redux") {
+				/* one copy of the slots per warp (or per group of warps) within 64 KiB: the
+				 * group leaders of a warp then update their own copy */
+				replicas = (int)std::max<int64_t>(1, std::min<int64_t>(warps, (64 * 1024) / std::max<int64_t>(slot_bytes, 1)));
+			} else {
+				replicas = 1;
+			}
+			dense_in_smem = slot_bytes * replicas <= 96 * 1024;
+			if (!dense_in_smem) {
+				replicas = 1;
+			}
+			/* every warp owns its copy: leaders (distinct slots within a warp) add without atomics */
+			leader_plain = fl.lowcard == "redux" && dense_in_smem && replicas == warps;
 			if (dense_in_smem) {
 				smem_sink = (size_t)(D * A() * 8 * replicas);
 				o << "  unsigned long long* const sacc0 = (unsigned long long*)vd_smem;\n";
@@ -635,8 +680,8 @@ struct PipeGen {
 				  << "; i += blockDim.x) { sacc0[i] = 0ull; }\n";
 				o << "  vd::block_sync();\n";
 				if (replicas > 1) {
-					o << "  unsigned long long* const sacc = sacc0 + (threadIdx.x >> 5) * " << P((unsigned long long)(D * A()))
-					  << ";\n";
+					o << "  unsigned long long* const sacc = sacc0 + ((threadIdx.x >> 5) % " << replicas << ") * "
+					  << P((unsigned long long)(D * A())) << ";\n";
 				} else {
 					o << "  unsigned long long* const sacc = sacc0;\n";
 				}
@@ -746,13 +791,21 @@ struct PipeGen {
 				o << "        }\n      }\n    }\n";
 				break;
 			}
-			if (replicas > 1) {
+			if (fl.lowcard == "atomic") {
 				o << "      if (act[v]) {\n";
+			} else if (fl.lowcard == "redux") {
+				emit_group_reduce("act[v] ? (unsigned)slot : 0xffffffffu");
+				o << "      if (lead) {\n";
 			} else {
 				o << "      if (vd::warp_combine<" << A() << ">((uint64_t)slot, act[v], vals)) {\n";
 			}
-			o << "#pragma unroll\n        for (int a = 0; a < " << A() << "; a++) { atomicAdd(&sacc[slot * "
-			  << A() << " + a], (unsigned long long)vals[a]); }\n";
+			if (leader_plain) {
+				o << "#pragma unroll\n        for (int a = 0; a < " << A() << "; a++) { sacc[slot * " << A()
+				  << " + a] += (unsigned long long)vals[a]; }\n";
+			} else {
+				o << "#pragma unroll\n        for (int a = 0; a < " << A() << "; a++) { atomicAdd(&sacc[slot * "
+				  << A() << " + a], (unsigned long long)vals[a]); }\n";
+			}
 			o << "      }\n    }\n";
 			break;
 		}
@@ -764,7 +817,12 @@ struct PipeGen {
 			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
 			o << "      const uint64_t pk = act[v] ? (" << packed_key(s.keys, kb, s.key_shift, "v") << ") : 0ull;\n";
 			o << "      " << agg_vals("v") << "\n";
-			o << "      if (vd::warp_combine<" << A() << ">(pk, act[v], vals)) {\n";
+			if (s.key_bits < 64) {
+				emit_group_reduce("act[v] ? (unsigned long long)pk : ~0ull");
+				o << "      if (lead) {\n";
+			} else {
+				o << "      if (vd::warp_combine<" << A() << ">(pk, act[v], vals)) {\n";
+			}
 			o << "        const uint64_t h = " << table_hash(s.keys, "pk", s.key_bits, "v") << ";\n";
 			if (fl.aggr == "cache") {
 				o << "        if (!vd::cache_add<" << A() << ">(scache, " << cache_slots << ", h, pk + 1ull, vals)) {\n";

@@ -311,6 +311,30 @@ __device__ __forceinline__ bool warp_combine(uint64_t key, bool valid, int64_t (
 	return leader;
 }
 
+/* Bits below the lane: the lanes of a __match_any_sync group whose bit is not set here
+ * are the group's lowest lane (its leader). */
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+	return (1u << lane_id()) - 1u;
+}
+
+/* Sum of u over the lanes of `mask`, a group found by __match_any_sync (every lane of the
+ * group calls with the same mask; the warp's other groups run their own sums in the same
+ * instruction).  u has at most BITS significant bits; redux.sync adds 27-bit chunks, which
+ * 32 lanes cannot overflow in 32 bits. */
+template <int BITS>
+__device__ __forceinline__ uint64_t group_sum_u(unsigned mask, uint64_t u)
+{
+	uint64_t s = __reduce_add_sync(mask, (unsigned)(u & 0x7ffffffu));
+	if constexpr (BITS > 27) {
+		s += (uint64_t)__reduce_add_sync(mask, (unsigned)((u >> 27) & 0x7ffffffu)) << 27;
+	}
+	if constexpr (BITS > 54) {
+		s += (uint64_t)__reduce_add_sync(mask, (unsigned)(u >> 54)) << 54;
+	}
+	return s;
+}
+
 /* Warp-aggregated append: every lane with `take` gets a distinct position in [0, *cursor),
  * reserved with one atomic per warp. */
 __device__ __forceinline__ int64_t warp_append(unsigned long long* cursor, bool take)

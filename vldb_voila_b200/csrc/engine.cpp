@@ -126,8 +126,8 @@ Flavor Flavor::parse(const std::string& s0)
 		} else if (k == "compact") {
 			f.compact = v == "auto" ? -2 : num(-1, 64);
 		} else if (k == "lowcard") {
-			if (v != "combine" && v != "atomic" && v != "private") {
-				throw Error(1, "lowcard must be combine, atomic or private");
+			if (v != "combine" && v != "atomic" && v != "private" && v != "redux") {
+				throw Error(1, "lowcard must be combine, atomic, private or redux");
 			}
 			f.lowcard = v;
 		} else if (k == "hash") {
@@ -321,6 +321,18 @@ void query_prepare(Query& q)
 	qs.out_cap = q.out_cap;
 	qs.out_count = q.out_count;
 	q.code = generate_cuda(plan, q.flavor, st.pipes, qs, q.params);
+	/* a flavor whose shared memory (TMA ring + sink) exceeds the per-CTA opt-in limit is
+	 * rejected here rather than failing at launch */
+	int smem_optin = 232448; /* sm_100 */
+	if (!e.offline) {
+		VC_CHECK_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, e.device));
+	}
+	for (auto& l : q.code.launches) {
+		if (l.smem + 1024 > (size_t)smem_optin) {
+			throw Error(VC_ERR_UNSUPPORTED, "flavor needs " + std::to_string(l.smem) + " bytes of shared memory per CTA in " +
+				l.kernel + "; the device allows " + std::to_string(smem_optin));
+		}
+	}
 	std::string log;
 	if (e.offline) {
 		jit_cubin(q.code.source, &log);

@@ -452,9 +452,9 @@ def run_config5(args):
     expect = [q.result_lines() for q in queries_tuned]
 
     # (b) one persistent kernel over all pipelines, learned flavors
-    # batched pipelines build their join tables directly (one work phase per table)
-    batch_flavors = [f.replace("build=staged", "build=direct") if "build=" in f else f.replace("cuda(", "cuda(build=direct,", 1)
-                     for f in learned]
+    # batched pipelines build their join tables in place (dense or direct hash; one work
+    # phase per table): a staged build becomes the automatic choice
+    batch_flavors = [f.replace("build=staged", "build=auto") for f in learned]
     queries_learned = [e.query(workload(s).plan, f) for e, s, f in zip(engines, specs, batch_flavors)]
     batch = Batch(queries_learned, threads=256, tiles_per_item=64)
     for _ in range(2):

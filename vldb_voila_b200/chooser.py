@@ -38,6 +38,10 @@ CANDIDATES = [
     "cuda(aggr=cache,cache=128,fill=75,prefetch=0)",
     "cuda(build=staged,prefetch=0)",
     "cuda(compact=-1,prefetch=0)",
+    "cuda(threads=128)",
+    "cuda(aggr=cache,cache=256,fill=75,prefetch=0)",
+    "cuda(aggr=cache,cache=2048,fill=75,prefetch=0,threads=512)",
+    "cuda(build=direct)",
 ]
 
 DEFAULT = "cuda()"

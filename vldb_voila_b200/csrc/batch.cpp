@@ -103,10 +103,11 @@ static void batch_prepare(Batch& b, const std::vector<Flavor>& flavors, int64_t 
 	b.mod = jit_compile(bc.source, &log);
 	VC_CHECK_CUDA(cudaLibraryGetKernel(&b.kernel, b.mod->lib, "vc_batch"));
 	b.smem = bc.smem;
+	cudaFuncAttributes fa;
+	VC_CHECK_CUDA(cudaFuncGetAttributes(&fa, (const void*)b.kernel));
+	b.regs = fa.numRegs;
 	if (b.smem > 0) {
 		/* batches of one shape share the kernel: the limit only grows */
-		cudaFuncAttributes fa;
-		VC_CHECK_CUDA(cudaFuncGetAttributes(&fa, (const void*)b.kernel));
 		if ((size_t)fa.maxDynamicSharedSizeBytes < b.smem) {
 			VC_CHECK_CUDA(cudaFuncSetAttribute((const void*)b.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 				(int)b.smem));
@@ -274,7 +275,8 @@ int vc_batch_info(vc_batch* h, char* buf, size_t cap, size_t* len)
 		Batch& b = h->b;
 		std::ostringstream o;
 		o << "{\"queries\": " << b.queries.size() << ", \"work_items\": " << b.nitems << ", \"grid\": " << b.grid
-		  << ", \"threads\": " << b.flavor.threads << ", \"smem\": " << b.smem << ", \"occupancy\": " << b.occupancy
+		  << ", \"threads\": " << b.flavor.threads << ", \"smem\": " << b.smem << ", \"regs\": " << b.regs
+		  << ", \"occupancy\": " << b.occupancy
 		  << ", \"source_bytes\": " << b.source.size() << "}";
 		const std::string s = o.str();
 		if (len) {

@@ -658,16 +658,18 @@ struct PipeGen {
 			const int64_t D = (int64_t)s.domain;
 			const int64_t warps = T / 32;
 			const int64_t slot_bytes = D * A() * 8;
+			const int64_t cap = std::min<int64_t>(96 * 1024, fl.sink_smem);
 			if (fl.lowcard == "atomic") {
-				replicas = slot_bytes * warps <= 96 * 1024 ? (int)warps : 1;
+				replicas = slot_bytes * warps <= cap ? (int)warps : 1;
 			} else if (fl.lowcard == "redux") {
 				/* one copy of the slots per warp (or per group of warps) within 64 KiB: the
 				 * group leaders of a warp then update their own copy */
-				replicas = (int)std::max<int64_t>(1, std::min<int64_t>(warps, (64 * 1024) / std::max<int64_t>(slot_bytes, 1)));
+				replicas = (int)std::max<int64_t>(1, std::min<int64_t>(warps, std::min<int64_t>(64 * 1024, cap) /
+					std::max<int64_t>(slot_bytes, 1)));
 			} else {
 				replicas = 1;
 			}
-			dense_in_smem = slot_bytes * replicas <= 96 * 1024;
+			dense_in_smem = slot_bytes * replicas <= cap;
 			if (!dense_in_smem) {
 				replicas = 1;
 			}
@@ -1197,6 +1199,7 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 			fl.lowcard = "combine";
 		}
 		fl.cache_slots = std::min(fl.cache_slots, 256);
+		fl.sink_smem = std::min(fl.sink_smem, 16 * 1024);
 		QueryDeviceState qs;
 		qs.out = q.out;
 		qs.out_cap = q.out_cap;
@@ -1281,10 +1284,9 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 			}
 		}
 	}
-	/* Within a phase, the pipelines' items are interleaved round-robin (pipelines with the
-	 * most items first), so that CTAs running at the same time work on different pipelines:
-	 * atomic-bound group-bys then overlap bandwidth-bound scans instead of the whole GPU
-	 * working through one pipeline at a time. */
+	/* Within a phase, each pipeline's items stay together (its hash table stays in L2 while
+	 * its items run; interleaving all pipelines' items thrashed L2 and slowed the group-bys
+	 * by a third), largest pipelines first so the small ones fill the tail of the phase. */
 	for (auto& ph : phases) {
 		std::map<int64_t, std::vector<BatchItem>> by_stage; /* key: parameter offset and done counter */
 		std::vector<int64_t> order;
@@ -1297,16 +1299,8 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 		}
 		std::stable_sort(order.begin(), order.end(),
 			[&](int64_t a, int64_t b) { return by_stage[a].size() > by_stage[b].size(); });
-		std::vector<size_t> next(order.size(), 0);
-		for (bool any = true; any;) {
-			any = false;
-			for (size_t k = 0; k < order.size(); k++) {
-				auto& v = by_stage[order[k]];
-				if (next[k] < v.size()) {
-					bc.items.push_back(v[next[k]++]);
-					any = true;
-				}
-			}
+		for (int64_t k : order) {
+			bc.items.insert(bc.items.end(), by_stage[k].begin(), by_stage[k].end());
 		}
 	}
 	bc.ncounters = ncounters;
@@ -1316,7 +1310,11 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 	src << "struct VcBatchItem { int shape; int dep; long long params; long long begin; long long end; "
 		"long long nitems; long long dep_target; int done; int finish; };\n\n";
 	src << funcs.str();
-	src << "extern \"C\" __global__ void __launch_bounds__(" << threads << ") vc_batch(const VcBatchItem* __restrict__ items, "
+	/* the kernel holds every shape, so its register count is the largest shape's: bound it so
+	 * that 32 warps per SM stay resident (the heaviest shapes spill a little instead) */
+	const int min_blocks = std::max(1, 1024 / threads);
+	src << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", " << min_blocks
+		<< ") vc_batch(const VcBatchItem* __restrict__ items, "
 		"long long nwork, unsigned long long* counters, const unsigned long long* __restrict__ pool, "
 		"unsigned long long* finish_ns, int nq, unsigned* err) {\n";
 	src << "  __shared__ long long s_w;\n  __shared__ int s_ok;\n";

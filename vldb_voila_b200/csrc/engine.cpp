@@ -50,7 +50,11 @@ std::string Flavor::str() const
 	o << ",compact=" << (compact == -2 ? std::string("auto") : std::to_string(compact));
 	o << ",aggr=" << aggr << ",lowcard=" << lowcard << ",hash=" << hash << ",fill=" << fill << ",cache=" << cache_slots
 	  << ",build=" << build
-	  << ",grid=" << grid << ",dense=" << dense_limit << ",graph=" << (graph ? 1 : 0) << ")";
+	  << ",grid=" << grid << ",dense=" << dense_limit << ",graph=" << (graph ? 1 : 0);
+	if (sink_smem != 96 * 1024) {
+		o << ",sinksmem=" << sink_smem;
+	}
+	o << ")";
 	return o.str();
 }
 
@@ -112,6 +116,8 @@ Flavor Flavor::parse(const std::string& s0)
 			f.grid = num(0, 64);
 		} else if (k == "dense") {
 			f.dense_limit = num(1, 1 << 22);
+		} else if (k == "sinksmem") {
+			f.sink_smem = num(0, 96 * 1024);
 		} else if (k == "graph") {
 			f.graph = num(0, 1) != 0;
 		} else if (k == "load") {

@@ -197,6 +197,7 @@ struct Flavor {
 	std::string hash = "mix"; /* table positions: mix (finalizer of the packed key) | voila (runtime.hpp hash) */
 	int fill = 50;            /* largest load factor (percent) of group tables */
 	int64_t direct_limit = 64ll << 20; /* auto: direct when the upper-bound table fits this many bytes */
+	int sink_smem = 96 * 1024; /* most shared memory a dense aggregation keeps its slots in (else global) */
 
 	std::string str() const;
 	static Flavor parse(const std::string& s);
@@ -331,6 +332,7 @@ struct Batch {
 	std::shared_ptr<JitModule> mod;
 	cudaKernel_t kernel = nullptr;
 	int occupancy = 0;
+	int regs = 0;
 	size_t smem = 0;
 	int64_t nitems = 0;
 	std::vector<void*> allocations;

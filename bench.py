@@ -299,6 +299,21 @@ def main():
             dom_ms.append(t[dom][1])
             all_ms.append([x[1] for x in t])
         q.profile(False)
+        # the floor of a short scan: torch's int64 sum over the same number of bytes, L2
+        # flushed the same way (launch and ramp dominate below a few hundred MB)
+        floor_buf = torch.ones(max(w.probe_bytes // 8, 1), dtype=torch.int64, device="cuda")
+        floor_ms = []
+        for i in range(min(args.steps, 50) + 3):
+            flush.fill_((i + 3) & 0xff)
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            floor_buf.sum()
+            ev1.record(stream)
+            ev1.synchronize()
+            if i >= 3:
+                floor_ms.append(ev0.elapsed_time(ev1))
+        del floor_buf
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -377,6 +392,9 @@ def main():
             "roofline": {"bound": "hbm", "kernel": kernels[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes": w.probe_bytes, "kernel_ms": dom_avg,
+                         "scan_floor": {"gbs": w.probe_bytes / (statistics.mean(floor_ms) / 1e3) / 1e9,
+                                        "frac": achieved / (w.probe_bytes / (statistics.mean(floor_ms) / 1e3) / 1e9),
+                                        "method": "torch int64 sum over the same byte count, same L2 flush"},
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
                          else "fallback 6650 GB/s"},
             "gpu_launches": len(kernels) * args.steps,

@@ -221,6 +221,15 @@ struct PipeGen {
 		} else {
 			o << "extern \"C\" __global__ void __launch_bounds__(" << T << ") " << name << suffix
 			  << "(const VcParams p) {\n";
+			o << "  vd::pdl_launch_dependents();\n";
+		}
+	}
+
+	/* before the first access to anything an earlier kernel of the query writes (tables,
+	 * accumulators, results); the pipeline's own base columns may be read before it */
+	void emit_pdl_wait() {
+		if (!item) {
+			o << "  vd::pdl_wait();\n";
 		}
 	}
 
@@ -254,6 +263,7 @@ struct PipeGen {
 		}
 		const bool tma = fl.load == "tma" && any_eager && !item;
 		if (tma) {
+			emit_pdl_wait();
 			gen_tma_loop();
 		} else if (fl.prefetch && any_eager) {
 			/* register double buffering: the next tile's eager columns are in flight while
@@ -268,6 +278,8 @@ struct PipeGen {
 			o << "  if (t < " << tend() << ") {\n    const int64_t r0p = t * tile + (int64_t)threadIdx.x * " << V << ";\n";
 			emit_load_cols("ldg", "pf", "r0p");
 			o << "  }\n";
+			/* the first tile's columns are in flight while the previous kernel finishes */
+			emit_pdl_wait();
 			o << "  for (; t < " << tend() << "; t += " << tstep() << ") {\n";
 			emit_decl_cols(true, V);
 			for (size_t c = 0; c < p.cols.size(); c++) {
@@ -282,6 +294,7 @@ struct PipeGen {
 			emit_body("pre");
 			o << "  }\n  }\n";
 		} else {
+			emit_pdl_wait();
 			o << "  for (int64_t t = " << tstart() << "; t < " << tend() << "; t += " << tstep() << ") {\n";
 			emit_body("ldg");
 			o << "  }\n";
@@ -1005,6 +1018,7 @@ struct PipeGen {
 		const std::string words = Pptr(jd.words, "unsigned long long*");
 		const std::string table = Pptr(jd.table, S + "*");
 		k << "extern \"C\" __global__ void __launch_bounds__(256) " << name << "_clear(const VcParams p) {\n";
+		k << "  vd::pdl_launch_dependents();\n  vd::pdl_wait();\n";
 		k << "  unsigned long long* const words = " << words << ";\n";
 		k << "  " << S << "* const jt = " << table << ";\n";
 		k << "  const uint64_t nb = vd::join_buckets<" << S << ">(words[0]);\n";
@@ -1013,6 +1027,7 @@ struct PipeGen {
 		k << "  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nslots; i += (uint64_t)gridDim.x * blockDim.x) {\n";
 		k << "    jt[i].key = 0; jt[i].pay = 0;\n  }\n}\n\n";
 		k << "extern \"C\" __global__ void __launch_bounds__(256) " << name << "_insert(const VcParams p) {\n";
+		k << "  vd::pdl_launch_dependents();\n  vd::pdl_wait();\n";
 		k << "  unsigned long long* const words = " << words << ";\n";
 		k << "  " << S << "* const jt = " << table << ";\n";
 		k << "  const " << KT << "* const skeys = " << Pptr(jd.stage_keys, "const " + KT + "*") << ";\n";
@@ -1037,6 +1052,7 @@ struct PipeGen {
 			k << "  (void)nitems;\n";
 		} else {
 			k << "extern \"C\" __global__ void __launch_bounds__(256) " << name << "_extract(const VcParams p) {\n";
+			k << "  vd::pdl_launch_dependents();\n  vd::pdl_wait();\n";
 		}
 		k << "  int64_t* const out = " << Pptr(qs.out, "int64_t*") << ";\n";
 		k << "  const int64_t ocap = " << P((unsigned long long)qs.out_cap) << ";\n";

@@ -266,6 +266,20 @@ __device__ __forceinline__ void block_sync()
 	asm volatile("barrier.sync 0;" ::: "memory");
 }
 
+/* Programmatic dependent launch: pdl_launch_dependents() lets the stream's next kernel be
+ * scheduled while this one runs; pdl_wait() blocks until the previous kernel of the stream
+ * has completed and its memory is visible.  Both are no-ops for a kernel that was launched
+ * without programmatic stream serialization. */
+__device__ __forceinline__ void pdl_launch_dependents()
+{
+	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+__device__ __forceinline__ void pdl_wait()
+{
+	asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 /* block_sync() that also returns whether any thread passed `v` true (the non-aligned form
  * of __syncthreads_or). */
 __device__ __forceinline__ bool block_any(bool v)

@@ -425,8 +425,24 @@ static void launch_all(Query& q, cudaStream_t stream, bool capturing = false)
 		if (q.profile) {
 			VC_CHECK_CUDA(cudaEventRecordWithFlags(q.ev[2 * i], stream, capturing ? cudaEventRecordExternal : 0));
 		}
-		VC_CHECK_CUDA(cudaLaunchKernel((const void*)st.kernels[i], dim3((unsigned)grid), dim3((unsigned)l.threads), args,
-			l.smem, stream));
+		if (i > 0 && !q.profile) {
+			/* programmatic dependent launch: this kernel is scheduled while the previous one
+			 * finishes and waits (vd::pdl_wait) before touching what that one wrote */
+			cudaLaunchConfig_t cfg = {};
+			cfg.gridDim = dim3((unsigned)grid);
+			cfg.blockDim = dim3((unsigned)l.threads);
+			cfg.dynamicSmemBytes = l.smem;
+			cfg.stream = stream;
+			cudaLaunchAttribute attr[1];
+			attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+			attr[0].val.programmaticStreamSerializationAllowed = 1;
+			cfg.attrs = attr;
+			cfg.numAttrs = 1;
+			VC_CHECK_CUDA(cudaLaunchKernelExC(&cfg, (const void*)st.kernels[i], args));
+		} else {
+			VC_CHECK_CUDA(cudaLaunchKernel((const void*)st.kernels[i], dim3((unsigned)grid), dim3((unsigned)l.threads),
+				args, l.smem, stream));
+		}
 		if (q.profile) {
 			VC_CHECK_CUDA(cudaEventRecordWithFlags(q.ev[2 * i + 1], stream, capturing ? cudaEventRecordExternal : 0));
 		}

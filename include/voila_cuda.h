@@ -126,7 +126,11 @@ int vc_workload_batch(int count, uint64_t seed, int64_t min_rows, int64_t max_ro
  * compiles their kernels (NVRTC, cached by source) and allocates the query's device
  * state.  Replaces Compiler::_generate + call_cxx_compiler + voila_query_new
  * (compiler.cpp:19-57, :343-385; codegen.cpp:371-376).
- * flavor: "" or "cuda(threads=256,rows=4,aggr=auto,cache=1024,grid=0,graph=0)". */
+ * flavor: "" or "cuda(key=value,...)" with keys threads, rows, load=ldg|tma, stages,
+ * prefetch, compact, aggr=auto|dense|global|cache, cache, lowcard=combine|atomic|private|redux,
+ * build=auto|direct|staged|dense, hash=mix|voila, fill, dense, sinksmem, grid, graph.
+ * VC_ERR_INVALID for an unknown or out-of-range knob; VC_ERR_UNSUPPORTED when the flavor's
+ * shared memory exceeds the device's per-CTA limit or build=dense meets a large key space. */
 int vc_query_new(vc_engine* eng, const char* plan, const char* flavor, vc_query** out);
 
 /* Launches the query's pipelines on `stream` (voila_query_run, codegen.cpp:390; the

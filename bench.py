@@ -474,7 +474,7 @@ def run_config5(args):
     # phase per table): a staged build becomes the automatic choice
     batch_flavors = [f.replace("build=staged", "build=auto") for f in learned]
     queries_learned = [e.query(workload(s).plan, f) for e, s, f in zip(engines, specs, batch_flavors)]
-    batch = Batch(queries_learned, threads=256, tiles_per_item=64)
+    batch = Batch(queries_learned, threads=256, tiles_per_item=16)
     for _ in range(2):
         batch.run(stream)
         batch.wait()

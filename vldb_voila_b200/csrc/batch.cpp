@@ -68,11 +68,15 @@ static void batch_prepare(Batch& b, const std::vector<Flavor>& flavors, int64_t 
 	VC_CHECK_CUDA(cudaSetDevice(b.eng->device));
 	BatchCode bc = generate_batch(b.queries, flavors, b.flavor.threads, tiles_per_item);
 
-	/* clear items: every query's per-run state, in chunks of at most 8 MiB */
-	std::vector<BatchItem> clears;
+	/* clear items: every query's per-run state, in chunks of at most 8 MiB, placed just
+	 * before the query's first work item, with a done-counter per query that the query's
+	 * first-phase items wait for (a table cleared right before its pipeline runs can still
+	 * be in L2 when the pipeline reaches it) */
+	const size_t nq = b.queries.size();
+	std::vector<std::vector<BatchItem>> clears(nq);
 	const int64_t chunk = 8ll << 20;
-	for (Query* q : b.queries) {
-		for (auto& m : state_of(*q).memsets) {
+	for (size_t qi = 0; qi < nq; qi++) {
+		for (auto& m : state_of(*b.queries[qi]).memsets) {
 			const int64_t bytes = (int64_t)((m.second + 15) & ~(size_t)15); /* allocations are 256-byte granular */
 			const int64_t poff = (int64_t)bc.params.size();
 			bc.params.push_back((unsigned long long)(uintptr_t)m.first);
@@ -85,18 +89,41 @@ static void batch_prepare(Batch& b, const std::vector<Flavor>& flavors, int64_t 
 				it.end = std::min(off + chunk, bytes);
 				it.nitems = 1;
 				it.dep_target = 0;
-				it.done = 1;
+				it.done = bc.ncounters + (int)qi;
 				it.finish = -1;
-				clears.push_back(it);
+				clears[qi].push_back(it);
 			}
 		}
 	}
-	for (auto& it : bc.items) {
+	auto query_of = [&](const BatchItem& it) {
+		const auto& qb = bc.query_params_begin;
+		return (size_t)(std::upper_bound(qb.begin(), qb.end(), it.params) - qb.begin()) - 1;
+	};
+	std::vector<BatchItem> ordered;
+	ordered.reserve(bc.items.size() + 64);
+	std::vector<bool> placed(nq, false);
+	for (auto it : bc.items) {
+		const size_t qi = query_of(it);
+		if (qi >= nq) {
+			throw Error(VC_ERR_INVALID, "batch item outside every query's parameters");
+		}
+		if (!placed[qi]) {
+			ordered.insert(ordered.end(), clears[qi].begin(), clears[qi].end());
+			placed[qi] = true;
+		}
 		if (it.dep_target == -2) {
-			it.dep_target = (int64_t)clears.size();
+			it.dep = bc.ncounters + (int)qi;
+			it.dep_target = (int64_t)clears[qi].size();
+		}
+		ordered.push_back(it);
+	}
+	for (size_t qi = 0; qi < nq; qi++) {
+		if (!placed[qi]) {
+			ordered.insert(ordered.end(), clears[qi].begin(), clears[qi].end());
 		}
 	}
-	bc.items.insert(bc.items.begin(), clears.begin(), clears.end());
+	bc.items.swap(ordered);
+	bc.ncounters += (int)nq;
 	b.nitems = (int64_t)bc.items.size();
 	b.source = bc.source;
 	std::string log;

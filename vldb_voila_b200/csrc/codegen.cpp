@@ -208,7 +208,9 @@ struct PipeGen {
 	 * memory instead of the kernel parameter space */
 	bool item = false;
 	std::string tstart() const { return item ? "t_begin" : "(int64_t)blockIdx.x"; }
-	std::string tstep() const { return item ? "1" : "(int64_t)gridDim.x"; }
+	/* item k of a pipeline's nitems items takes tiles k, k + nitems, ...: items that run at
+	 * the same time read neighbouring tiles, as the CTAs of a standalone launch do */
+	std::string tstep() const { return item ? "nitems" : "(int64_t)gridDim.x"; }
 	std::string tend() const { return item ? "tlim" : "ntiles"; }
 	std::string blocks_total() const { return item ? "(unsigned long long)nitems" : "(unsigned long long)gridDim.x"; }
 
@@ -1206,6 +1208,7 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 	for (size_t qi = 0; qi < queries.size(); qi++) {
 		Query& q = *queries[qi];
 		QueryState& st = state_of(q);
+		bc.query_params_begin.push_back((int64_t)bc.params.size());
 		Flavor fl = flavors[qi];
 		fl.threads = threads;
 		fl.load = "ldg";
@@ -1265,8 +1268,8 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 				BatchItem it;
 				it.shape = sid;
 				it.params = poff;
-				it.begin = k * tiles_per_item;
-				it.end = std::min((k + 1) * tiles_per_item, ntiles);
+				it.begin = k; /* tiles k, k + nit, k + 2 nit, ... (the item functions stride by nitems) */
+				it.end = ntiles;
 				it.nitems = nit;
 				it.dep = phase == 0 ? 1 : build_counter;
 				it.dep_target = phase == 0 ? -2 : build_items;
@@ -1319,6 +1322,7 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 			bc.items.insert(bc.items.end(), by_stage[k].begin(), by_stage[k].end());
 		}
 	}
+	bc.query_params_begin.push_back((int64_t)bc.params.size());
 	bc.ncounters = ncounters;
 
 	std::ostringstream src;

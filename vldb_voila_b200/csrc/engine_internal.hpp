@@ -354,6 +354,7 @@ struct BatchCode {
 	size_t smem = 0;
 	std::vector<BatchItem> items;
 	std::vector<unsigned long long> params;
+	std::vector<int64_t> query_params_begin; /* query i's parameters: [begin[i], begin[i + 1]) */
 	int ncounters = 0;
 };
 

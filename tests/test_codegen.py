@@ -7,7 +7,8 @@ from vldb_voila_b200 import Engine, VoilaError, workload
 SPECS = ["sel_aggr:rows=1000", "join_aggr:build=100,probe=1000", "groupby:rows=1000,keys=100000,zipf=1.0",
          "groupby:rows=1000,keys=50", "star:rows=1000"]
 FLAVORS = ["", "cuda(load=tma,stages=2)", "cuda(lowcard=private,prefetch=0)", "cuda(aggr=cache,build=staged)",
-           "cuda(compact=0,rows=8,threads=128)", "cuda(hash=voila,compact=-1)", "cuda(build=direct,prefetch=0)"]
+           "cuda(compact=0,rows=8,threads=128)", "cuda(hash=voila,compact=-1)", "cuda(build=direct,prefetch=0)",
+           "cuda(lowcard=redux,aggr=cache,cache=64)", "cuda(lowcard=atomic,sinksmem=4096)"]
 
 
 def offline(spec):
@@ -79,6 +80,30 @@ def test_batch_module_compiles_and_dedups_shapes():
     # one persistent kernel; shapes shared: far less code than one copy per query
     assert many.info()["source_bytes"] < 4 * one.info()["source_bytes"] * 3
     assert many.info()["work_items"] >= len(specs)
+    src = many.source()
+    # a pipeline's item k strides its tiles by the pipeline's item count
+    assert "t += nitems" in src
+    # block barriers are the non-aligned form: warps may arrive diverged after probe loops
+    assert "__syncthreads" not in src and "vd::block_sync()" in src
+
+
+@pytest.mark.parametrize("spec", SPECS)
+def test_generated_kernels_use_non_aligned_barriers(spec):
+    w, e = offline(spec)
+    for flavor in ["", "cuda(load=tma,stages=2)", "cuda(compact=0)", "cuda(lowcard=private)"]:
+        src = e.query(w.plan, flavor).source()
+        assert "__syncthreads" not in src, flavor
+
+
+def test_dense_join_tables_follow_the_key_space():
+    # join_aggr's build keys span 1..1.5M: a bitmap of 2^21 bits beats a 2^22-slot hash table
+    w, e = offline("join_aggr:build=1500000,probe=6000000,sel=0.2,seed=2")
+    assert "vd::dense_test" in e.query(w.plan).source()
+    assert "join_probe_bucket" in e.query(w.plan, "cuda(build=direct)").source()
+    # star's dimension joins carry payloads: dense payload arrays
+    w, e = offline("star:rows=1000")
+    src = e.query(w.plan).source()
+    assert "atomicCAS(&jdt" in src and "join_probe_bucket" not in src
 
 
 @pytest.mark.parametrize("flavor", ["cuda(rows=3)", "cuda(threads=100)", "cuda(aggr=magic)", "gpu(x=1)", "cuda(nokey=1)"])

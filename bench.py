@@ -392,6 +392,7 @@ def main():
             "roofline": {"bound": "hbm", "kernel": kernels[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes": w.probe_bytes, "kernel_ms": dom_avg,
+                         "kernel_rows_per_s": w.fact_rows / (dom_avg / 1e3),
                          "scan_floor": {"gbs": w.probe_bytes / (statistics.mean(floor_ms) / 1e3) / 1e9,
                                         "frac": achieved / (w.probe_bytes / (statistics.mean(floor_ms) / 1e3) / 1e9),
                                         "method": "torch int64 sum over the same byte count, same L2 flush"},

@@ -223,7 +223,7 @@ int vc_batch_free(vc_batch* b);
  * the GPU by the library's own kernels.  It maps a pipeline's features to the predicted
  * relative time of every candidate flavor; the caller picks the argmin.  It stands beside
  * the exhaustive search over blends that the reference's explorer performs
- * (explorer.cpp:111-134, :352-426), which remains the fallback and judge. */
+ * (explorer.cpp:111-134, :352-426), which remains the fallback and the yardstick of its choices. */
 typedef struct vc_mlp vc_mlp;
 
 /* Glorot-uniform weights from `seed`, zero biases. */

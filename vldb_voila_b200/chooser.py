@@ -11,7 +11,7 @@ Here:
     own kernels (csrc/mlp.cu), maps per-pipeline features (row count, predicate selectivity,
     build size, key cardinality, Zipf skew, payload widths, operator counts) to the predicted
     relative time of every candidate flavor and picks the argmin.  Results never depend on the
-    choice, only speed; the autotuner is its fallback and its judge.
+    choice, only speed; the autotuner is its fallback and the yardstick of its choices.
 """
 import json
 import math

@@ -3,7 +3,7 @@
  * ReLU) trained and evaluated on the GPU by hand-written kernels.  The reference searches
  * the blend space by running variants (explorer.cpp:111-134, :352-426); here a network maps
  * per-pipeline features to the predicted relative time of each candidate flavor, trained on
- * timings measured by the exhaustive autotuner, which stays its fallback and judge.
+ * timings measured by the exhaustive autotuner, which stays its fallback and yardstick.
  *
  * Sizes are tiny (tens of features, a few dozen flavors, <= a few thousand samples), so the
  * layers are plain FFMA kernels: one thread per output element, fp32, deterministic (no

@@ -215,6 +215,10 @@ int vc_batch_latencies(vc_batch* b, double* us, int n);
 int vc_batch_info(vc_batch* b, char* buf, size_t cap, size_t* len);
 /* The generated CUDA source of the batch's persistent kernel. */
 int vc_batch_source(vc_batch* b, char* buf, size_t cap, size_t* len);
+/* The work queue in claim order, 8 int64 per item: shape (-1 = clear), done-counter waited
+ * for (-1 = none), its target, done-counter incremented, items of the stage, tile (or byte)
+ * range begin and end, parameter offset.  *n = item count; out may be NULL. */
+int vc_batch_items(vc_batch* b, int64_t* out, int64_t cap, int64_t* n);
 int vc_batch_free(vc_batch* b);
 
 /* ---------------------------------------------------------------- flavor chooser ------ */

@@ -87,6 +87,39 @@ def test_batch_module_compiles_and_dedups_shapes():
     assert "__syncthreads" not in src and "vd::block_sync()" in src
 
 
+def test_batch_work_queue_only_waits_on_earlier_items():
+    """CTAs of the persistent kernel claim items in queue order, so the queue is deadlock-free
+    when every item's dependency is met by items before it; each query's clears also precede
+    its first work item."""
+    from collections import Counter
+
+    from vldb_voila_b200.engine import Batch, batch_specs
+    specs = batch_specs(12, seed=3, min_rows=1000, max_rows=400000)
+    specs += ["star:rows=5000,seed=9", "join_aggr:build=1000,probe=5000,seed=4", "groupby:rows=0,keys=10,seed=1"]
+    engines, queries = [], []
+    for s in specs:
+        w, e = offline(s)
+        engines.append(e)
+        queries.append(e.query(w.plan))
+    b = Batch(queries, tiles_per_item=4)
+    items = b.items()
+    assert len(items) == b.info()["work_items"]
+    F = {k: i for i, k in enumerate(Batch.ITEM_FIELDS)}
+    produced = Counter()
+    for row in items:
+        if row[F["dep"]] >= 0:
+            assert produced[row[F["dep"]]] >= row[F["dep_target"]]
+        produced[row[F["done"]]] += 1
+    clears = items[items[:, F["shape"]] == -1]
+    work = items[items[:, F["shape"]] >= 0]
+    assert len(clears) >= len(specs) and len(work) >= len(specs)
+    # every first-phase work item waits for its own query's clears, which all precede it
+    waits_on_clears = [r for r in work if r[F["dep"]] in set(clears[:, F["done"]])]
+    assert waits_on_clears
+    for r in waits_on_clears:
+        assert produced[r[F["dep"]]] == r[F["dep_target"]]
+
+
 @pytest.mark.parametrize("spec", SPECS)
 def test_generated_kernels_use_non_aligned_barriers(spec):
     w, e = offline(spec)

@@ -53,25 +53,13 @@ static void* balloc(Batch& b, size_t bytes)
 	return p;
 }
 
-static void batch_prepare(Batch& b, const std::vector<Flavor>& flavors, int64_t tiles_per_item)
+/* Clear items: every query's per-run state, in chunks of at most 8 MiB, placed just before
+ * the query's first work item, with a done-counter per query that the query's first-phase
+ * items wait for (a table cleared right before its pipeline runs can still be in L2 when the
+ * pipeline reaches it).  Every dependency then points at items earlier in the queue, which is
+ * what lets the persistent kernel's CTAs claim items in order without deadlock. */
+static void add_clears_in_order(Batch& b, BatchCode& bc)
 {
-	if (b.eng->offline) {
-		/* compile-only engines: generate and compile the batch module, nothing more */
-		BatchCode bc = generate_batch(b.queries, flavors, b.flavor.threads, tiles_per_item);
-		b.source = bc.source;
-		b.nitems = (int64_t)bc.items.size();
-		b.smem = bc.smem;
-		std::string log;
-		jit_cubin(bc.source, &log);
-		return;
-	}
-	VC_CHECK_CUDA(cudaSetDevice(b.eng->device));
-	BatchCode bc = generate_batch(b.queries, flavors, b.flavor.threads, tiles_per_item);
-
-	/* clear items: every query's per-run state, in chunks of at most 8 MiB, placed just
-	 * before the query's first work item, with a done-counter per query that the query's
-	 * first-phase items wait for (a table cleared right before its pipeline runs can still
-	 * be in L2 when the pipeline reaches it) */
 	const size_t nq = b.queries.size();
 	std::vector<std::vector<BatchItem>> clears(nq);
 	const int64_t chunk = 8ll << 20;
@@ -124,6 +112,27 @@ static void batch_prepare(Batch& b, const std::vector<Flavor>& flavors, int64_t 
 	}
 	bc.items.swap(ordered);
 	bc.ncounters += (int)nq;
+}
+
+static void batch_prepare(Batch& b, const std::vector<Flavor>& flavors, int64_t tiles_per_item)
+{
+	if (b.eng->offline) {
+		/* compile-only engines: generate and compile the batch module and build its work
+		 * queue (on the host only, for inspection) */
+		BatchCode bc = generate_batch(b.queries, flavors, b.flavor.threads, tiles_per_item);
+		add_clears_in_order(b, bc);
+		b.host_items = bc.items;
+		b.source = bc.source;
+		b.nitems = (int64_t)bc.items.size();
+		b.smem = bc.smem;
+		std::string log;
+		jit_cubin(bc.source, &log);
+		return;
+	}
+	VC_CHECK_CUDA(cudaSetDevice(b.eng->device));
+	BatchCode bc = generate_batch(b.queries, flavors, b.flavor.threads, tiles_per_item);
+	add_clears_in_order(b, bc);
+	b.host_items = bc.items;
 	b.nitems = (int64_t)bc.items.size();
 	b.source = bc.source;
 	std::string log;
@@ -331,6 +340,35 @@ int vc_batch_source(vc_batch* h, char* buf, size_t cap, size_t* len)
 			const size_t k = std::min(cap - 1, s.size());
 			std::memcpy(buf, s.data(), k);
 			buf[k] = 0;
+		}
+	});
+}
+
+int vc_batch_items(vc_batch* h, int64_t* out, int64_t cap, int64_t* n)
+{
+	return abi_guard_mlp([&] {
+		if (!h) {
+			throw Error(VC_ERR_INVALID, "null batch");
+		}
+		const auto& items = h->b.host_items;
+		if (n) {
+			*n = (int64_t)items.size();
+		}
+		if (!out) {
+			return;
+		}
+		const int64_t k = std::min<int64_t>(cap, (int64_t)items.size());
+		for (int64_t i = 0; i < k; i++) {
+			const BatchItem& it = items[(size_t)i];
+			int64_t* r = out + 8 * i;
+			r[0] = it.shape;
+			r[1] = it.dep;
+			r[2] = it.dep_target;
+			r[3] = it.done;
+			r[4] = it.nitems;
+			r[5] = it.begin;
+			r[6] = it.end;
+			r[7] = it.params;
 		}
 	});
 }

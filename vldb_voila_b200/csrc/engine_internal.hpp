@@ -335,6 +335,7 @@ struct Batch {
 	int regs = 0;
 	size_t smem = 0;
 	int64_t nitems = 0;
+	std::vector<BatchItem> host_items; /* the work queue as uploaded (for inspection) */
 	std::vector<void*> allocations;
 	BatchItem* items = nullptr;
 	unsigned long long* counters = nullptr; /* [0] queue head, [1..] done counters */

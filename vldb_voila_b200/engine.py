@@ -91,6 +91,7 @@ def lib():
         "vc_batch_latencies": (c.c_int, [P, c.POINTER(c.c_double), c.c_int]),
         "vc_batch_info": (c.c_int, [P, P, c.c_size_t, c.POINTER(c.c_size_t)]),
         "vc_batch_source": (c.c_int, [P, P, c.c_size_t, c.POINTER(c.c_size_t)]),
+        "vc_batch_items": (c.c_int, [P, P, c.c_int64, c.POINTER(c.c_int64)]),
         "vc_batch_free": (c.c_int, [P]),
         "vc_query_timings": (c.c_int, [P, c.POINTER(c.c_float), c.c_int, c.POINTER(c.c_int), P, c.c_size_t]),
     }
@@ -428,6 +429,16 @@ class Batch:
 
     def source(self):
         return _text_call(lib().vc_batch_source, self._h)
+
+    ITEM_FIELDS = ("shape", "dep", "dep_target", "done", "nitems", "begin", "end", "params")
+
+    def items(self):
+        """The work queue in claim order: an (items, 8) int64 array, columns ITEM_FIELDS."""
+        n = ctypes.c_int64()
+        check(lib().vc_batch_items(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, 8), dtype=np.int64)
+        check(lib().vc_batch_items(self._h, out.ctypes.data, n.value, ctypes.byref(n)))
+        return out
 
 
 class Mlp:

@@ -128,7 +128,8 @@ int vc_workload_batch(int count, uint64_t seed, int64_t min_rows, int64_t max_ro
  * (compiler.cpp:19-57, :343-385; codegen.cpp:371-376).
  * flavor: "" or "cuda(key=value,...)" with keys threads, rows, load=ldg|tma, stages,
  * prefetch, compact, aggr=auto|dense|global|cache, cache, lowcard=combine|atomic|private|redux,
- * build=auto|direct|staged|dense, hash=mix|voila, fill, dense, sinksmem, grid, graph.
+ * build=auto|direct|staged|dense, hash=mix|voila, fill, dense, sinksmem, gcap (group table
+ * slots), ocap (result rows of an emitting plan), grid, graph.
  * VC_ERR_INVALID for an unknown or out-of-range knob; VC_ERR_UNSUPPORTED when the flavor's
  * shared memory exceeds the device's per-CTA limit or build=dense meets a large key space. */
 int vc_query_new(vc_engine* eng, const char* plan, const char* flavor, vc_query** out);
@@ -172,6 +173,12 @@ int vc_query_profile(vc_query* q, int enable);
  * timed hot repetitions, compiler.cpp:521-575). */
 int vc_query_time(vc_query* q, int reps, int flush_l2, void* stream, float* ms_out, int cap);
 
+/* Reads `bytes` of device memory once, as fast as a plain streaming read can (16-byte loads,
+ * several in flight per thread, whole waves of CTAs), and XORs the words into *device_out.
+ * The bandwidth floor a pipeline over the same bytes is measured against; no counterpart in
+ * the reference (its CPU baseline has no device roofline).  Asynchronous on `stream`. */
+int vc_stream_read(const void* device_buf, int64_t bytes, unsigned long long* device_out, void* stream);
+
 /* ---------------------------------------------------------------- no allocation ------- */
 
 /* The hash join + global aggregate pipeline (a join_aggr query: build rows with
@@ -181,7 +188,9 @@ int vc_query_time(vc_query* q, int reps, int flush_l2, void* stream, float* ms_o
  * code running where allocation is forbidden or unsafe (host callbacks, allocator-owned
  * device memory, allocation-free service paths).  All pointers are caller-owned device
  * memory; out receives 3 int64: sum(probe_val) over matches, the match count, and error
- * bits (0 = none).
+ * bits (0 = none).  The error bits are the only report of a table that ran out of probes:
+ * a VC_OK return means the launch succeeded, so callers must check out[2] == 0 (after the
+ * stream has finished) before using out[0] and out[1].
  * Limit: at most 2,097,152 build rows (the join table is a static 4 Mi-slot, 32 MiB device
  * array that every GPU loading the library keeps until the process exits); larger inputs fail
  * with VC_ERR_INVALID.  The first call on a device looks the arrays' addresses up
@@ -219,6 +228,16 @@ int vc_batch_source(vc_batch* b, char* buf, size_t cap, size_t* len);
  * for (-1 = none), its target, done-counter incremented, items of the stage, tile (or byte)
  * range begin and end, parameter offset.  *n = item count; out may be NULL. */
 int vc_batch_items(vc_batch* b, int64_t* out, int64_t cap, int64_t* n);
+/* Longest time (ns, 1 us .. 60 s; default 2 s) that a work item waits for its dependency
+ * before the batch gives up on it: the item is skipped, the batch's error word records the
+ * timeout and vc_batch_wait returns VC_ERR_TIMEOUT.  Replaces the reference's fork-isolated
+ * timeout classification (safe_env.cpp:66-187) for the device side. */
+int vc_batch_set_wait_limit(vc_batch* b, uint64_t ns);
+/* Test hook for the timeout path, made on the host: with hold != 0, work item `index` (claim
+ * order, as vc_batch_items lists it) waits for a dependency that never completes, so its
+ * bounded wait runs out on the next run; hold == 0 restores it.  No counterpart in the
+ * reference. */
+int vc_batch_hold_item(vc_batch* b, int64_t index, int hold);
 int vc_batch_free(vc_batch* b);
 
 /* ---------------------------------------------------------------- flavor chooser ------ */

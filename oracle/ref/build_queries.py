@@ -14,7 +14,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
+REF = os.environ.get("VOILA_REFERENCE", "/root/reference")
 
 WORKLOADS = {
     "sel_aggr": "sel_aggr:rows=6000000,seed=1",

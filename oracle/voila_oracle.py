@@ -132,19 +132,79 @@ def _pack_keys(cols):
     return inv.reshape(-1).astype(np.int64)
 
 
-def _op(node, db):
+def _aggr_names(node, counter=None, names=None):
+    """Output table name of every aggregation below the root, as the reference's translator
+    numbers them: one id per hash join, taken before its build side is translated
+    (relalg_translator.cpp:814), and two per aggregation, taken after its input (the build
+    pass and the re-aggregation, :392 and :776-808); the re-aggregation's table names the
+    visible columns <name>.key_<i> and <name>.aggr_<j> (:740-760)."""
+    if counter is None:
+        counter, names = [0], {}
     head = node[0]
+    if head in ("select", "project"):
+        _aggr_names(node[2], counter, names)
+    elif head == "join":
+        counter[0] += 1
+        _aggr_names(node[7], counter, names)
+        _aggr_names(node[4], counter, names)
+    elif head == "aggr":
+        _aggr_names(node[4], counter, names)
+        counter[0] += 2
+        names[id(node)] = f"aggr_ht{counter[0] - 1}"
+    return names
+
+
+def _aggregate(node, f):
+    """Keys and visible aggregates of an aggregation over frame f: (key columns, aggregate
+    columns), one entry per group with count > 0 (relalg_translator.cpp:469-472, :692-701)."""
+    glob = node[1] == "global"
+    keys = [_eval(k, f, {}) for k in node[2]]
+    aggs = []
+    for a in node[3]:
+        if a[1] == "count":
+            aggs.append(("count", None))
+        else:
+            aggs.append(("sum", _eval(a[2], f, {}).astype(np.int64)))
+    _check_int64(keys + [v for _, v in aggs if v is not None])
+    if f.n == 0:
+        return [np.zeros(0, dtype=np.int64) for _ in keys], [np.zeros(0, dtype=np.int64) for _ in aggs]
+    if glob:
+        return [], [np.array([f.n if kind == "count" else int(v.sum(dtype=np.int64))], dtype=np.int64)
+                    for kind, v in aggs]
+    stacked = np.stack(keys, axis=1)
+    uniq, inv = np.unique(stacked, axis=0, return_inverse=True)
+    inv = inv.reshape(-1)
+    order = np.argsort(inv, kind="stable")
+    bounds = np.concatenate([[0], np.nonzero(np.diff(inv[order]))[0] + 1])
+    counts = np.diff(np.concatenate([bounds, [f.n]]))
+    out = []
+    for kind, v in aggs:
+        out.append(counts.astype(np.int64) if kind == "count" else np.add.reduceat(v[order], bounds).astype(np.int64))
+    return [uniq[:, i].astype(np.int64) for i in range(uniq.shape[1])], out
+
+
+def _op(node, db, names=None):
+    if names is None:
+        names = _aggr_names(node)
+    head = node[0]
+    if head == "aggr":
+        f = _op(node[4], db, names)
+        keys, aggs = _aggregate(node, f)
+        name = names[id(node)]
+        cols = [(f"{name}.key_{i}", k) for i, k in enumerate(keys)]
+        cols += [(f"{name}.aggr_{j}", a) for j, a in enumerate(aggs)]
+        return Frame(cols, len(aggs[0]) if aggs else (len(keys[0]) if keys else 0))
     if head == "scan":
         table = node[1]
         cols = [(f"{table}.{c}", np.asarray(db[table][c]).astype(np.int64)) for c in node[2]]
         n = len(cols[0][1]) if cols else 0
         return Frame(cols, n)
     if head == "select":
-        f = _op(node[2], db)
+        f = _op(node[2], db, names)
         m = _eval(node[1], f, {}).astype(bool)
         return f.take(np.nonzero(m)[0])
     if head == "project":
-        f = _op(node[2], db)
+        f = _op(node[2], db, names)
         env = {}
         out = []
         for e in node[1]:
@@ -159,8 +219,8 @@ def _op(node, db):
         return Frame(out, f.n)
     if head == "join":
         join01 = node[1] == "join01"
-        probe = _op(node[4], db)
-        build = _op(node[7], db)
+        probe = _op(node[4], db, names)
+        build = _op(node[7], db, names)
         pk = [_eval(k, probe, {}) for k in node[2]]
         bk = [_eval(k, build, {}) for k in node[5]]
         bpay = [(p[1], _eval(p, build, {})) for p in node[6]]
@@ -195,48 +255,15 @@ def _op(node, db):
 def run_plan(plan, db):
     """Result rows (list of tuples of ints) of plan text over db = {table: {col: array}}."""
     node = parse_sexpr(plan) if isinstance(plan, str) else plan
+    names = _aggr_names(node)
     if node[0] != "aggr":
-        f = _op(node, db)
+        f = _op(node, db, names)
         return [tuple(int(v[i]) for _, v in f.cols) for i in range(f.n)]
-    glob = node[1] == "global"
-    f = _op(node[4], db)
-    keys = [_eval(k, f, {}) for k in node[2]]
-    aggs = []
-    has_count = False
-    for a in node[3]:
-        if a[1] == "count":
-            aggs.append(("count", None, True))
-            has_count = True
-        else:
-            aggs.append(("sum", _eval(a[2], f, {}).astype(np.int64), True))
-    if not has_count:
-        aggs.append(("count", None, False))
-    _check_int64(keys + [v for _, v, _ in aggs if v is not None])
-    if glob:
-        if f.n == 0:
-            return []
-        row = []
-        for kind, v, vis in aggs:
-            if vis:
-                row.append(int(f.n) if kind == "count" else int(v.sum(dtype=np.int64)))
-        return [tuple(row)]
-    if f.n == 0:
-        return []
-    stacked = np.stack(keys, axis=1)
-    uniq, inv = np.unique(stacked, axis=0, return_inverse=True)
-    inv = inv.reshape(-1)
-    order = np.argsort(inv, kind="stable")
-    bounds = np.concatenate([[0], np.nonzero(np.diff(inv[order]))[0] + 1])
-    counts = np.diff(np.concatenate([bounds, [f.n]]))
-    cols = [uniq[:, i] for i in range(uniq.shape[1])]
-    for kind, v, vis in aggs:
-        if not vis:
-            continue
-        if kind == "count":
-            cols.append(counts.astype(np.int64))
-        else:
-            cols.append(np.add.reduceat(v[order], bounds).astype(np.int64))
-    return [tuple(int(c[i]) for c in cols) for i in range(len(uniq))]
+    f = _op(node[4], db, names)
+    keys, aggs = _aggregate(node, f)
+    cols = keys + aggs
+    n = len(cols[0]) if cols else 0
+    return [tuple(int(c[i]) for c in cols) for i in range(n)]
 
 
 def result_lines(rows):

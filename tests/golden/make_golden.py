@@ -16,7 +16,7 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
+REF = os.environ.get("VOILA_REFERENCE", "/root/reference")
 
 SEL_EMIT = ("(select (fun < (col lineitem.l_quantity) (const 3))"
             " (scan lineitem (l_quantity l_discount l_returnflag)))")
@@ -41,6 +41,19 @@ JOIN_EMIT = ("(select (fun = (col date.d_year) (const 1995))"
              " (join join01 ((col lineorder.lo_orderdate)) () (scan lineorder (lo_orderdate lo_revenue))"
              " ((col date.d_datekey)) ((col date.d_year)) (scan date (d_datekey d_year))))")
 
+# aggregation below the plan root: the sub-aggregation's outputs are named
+# aggr_ht<N>.key_<i> / aggr_ht<N>.aggr_<j> by the reference's translator
+AGG_OF_AGG = ("(aggr hash ((col aggr_ht1.aggr_1)) ((fun sum (col aggr_ht1.aggr_0)) (fun count))"
+              " (aggr hash ((col lineitem.l_orderkey)) ((fun sum (col lineitem.l_quantity)) (fun count))"
+              " (scan lineitem (l_orderkey l_quantity))))")
+HAVING_GLOBAL = ("(aggr global () ((fun sum (col aggr_ht1.aggr_0)) (fun count))"
+                 " (select (fun > (col aggr_ht1.aggr_1) (const 10))"
+                 " (aggr hash ((col lineitem.l_orderkey)) ((fun sum (col lineitem.l_extendedprice)) (fun count))"
+                 " (scan lineitem (l_orderkey l_extendedprice)))))")
+HAVING_EMIT = ("(select (fun > (col aggr_ht1.aggr_0) (const 200))"
+               " (aggr hash ((col lineitem.l_orderkey)) ((fun sum (col lineitem.l_quantity)))"
+               " (scan lineitem (l_orderkey l_quantity))))")
+
 CASES = [
     ("sel_aggr_1k", "sel_aggr:rows=1000,seed=11", None),
     ("sel_aggr_100k", "sel_aggr:rows=100000,seed=12", None),
@@ -61,6 +74,9 @@ CASES = [
     ("join_n", "star:rows=20000,dates=100,custs=500,supps=10,parts=100,seed=54", JOIN_N),
     ("join_2key", "star:rows=20000,dates=100,custs=500,supps=10,parts=400,seed=55", JOIN_2KEY),
     ("join_emit", "star:rows=5000,dates=2556,custs=10,supps=10,parts=10,seed=56", JOIN_EMIT),
+    ("agg_of_agg", "groupby:rows=20000,keys=3000,zipf=0.8,seed=71", AGG_OF_AGG),
+    ("having_global", "groupby:rows=20000,keys=3000,zipf=0.8,seed=72", HAVING_GLOBAL),
+    ("having_emit", "groupby:rows=20000,keys=3000,zipf=0.8,seed=73", HAVING_EMIT),
 ]
 
 

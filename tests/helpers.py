@@ -36,3 +36,15 @@ def data_checksum(w, data):
                 x = v * np.uint64(31) + i * np.uint64(1000003) + np.uint64(ti * 131) + np.uint64(ci)
                 total = total + _mix64(x).sum(dtype=np.uint64)
     return int(total)
+
+
+# A join whose build side is itself a join (over the star workload's tables): customers are
+# kept when their region is the weekday of one of the first three dates.  In a batch, the
+# customer build probes the date table and must wait for the date build.
+NESTED_BUILD_PLAN = (
+    "(aggr global () ((fun sum (col lineorder.lo_revenue)) (fun count))"
+    " (join join01 ((col lineorder.lo_custkey)) () (scan lineorder (lo_custkey lo_revenue))"
+    "  ((col customer.c_custkey)) ()"
+    "  (join join01 ((col customer.c_region)) () (scan customer (c_custkey c_region))"
+    "   ((col date.d_weekday)) ()"
+    "   (select (fun < (col date.d_datekey) (const 4)) (scan date (d_datekey d_weekday))))))")

@@ -2,6 +2,7 @@
 (compile-only) engine: runs on a build host without a GPU."""
 import pytest
 
+from helpers import NESTED_BUILD_PLAN
 from vldb_voila_b200 import Engine, VoilaError, workload
 
 SPECS = ["sel_aggr:rows=1000", "join_aggr:build=100,probe=1000", "groupby:rows=1000,keys=100000,zipf=1.0",
@@ -45,9 +46,23 @@ def test_pipeline_structure_follows_the_plan():
 
 
 def test_shapes_share_generated_code_across_instances():
+    # the accumulator words' bit fields follow the row-count bound: instances whose fields
+    # have the same widths share one compiled shape, whatever their sizes, keys and skew
     w1, e1 = offline("groupby:rows=1000,keys=100000,zipf=1.0,seed=1")
-    w2, e2 = offline("groupby:rows=5000,keys=200000,zipf=0.5,seed=2")
+    w2, e2 = offline("groupby:rows=1020,keys=200000,zipf=0.5,seed=2")
     assert e1.query(w1.plan).source() == e2.query(w2.plan).source()
+    w3, e3 = offline("join_aggr:build=100,probe=1000,seed=1")
+    w4, e4 = offline("join_aggr:build=300,probe=5000,seed=2")
+    assert e3.query(w3.plan).source() == e4.query(w4.plan).source()
+
+
+def test_hash_group_aggregates_share_accumulator_words():
+    """sum(v1) (20-bit values), sum(v2) (6-bit) and count over 6M rows need 43, 29 and 23 bits:
+    two 64-bit words, so each group update is two atomics instead of three."""
+    w, e = offline("groupby:rows=6000000,keys=1500000,zipf=0.0,seed=3")
+    src = e.query(w.plan).source()
+    assert "uint64_t w[2]" in src and "gt_add<2>" in src
+    assert "gt_find_or_insert<uint32_t>" in src
 
 
 @pytest.mark.parametrize("plan,code", [
@@ -101,6 +116,8 @@ def test_batch_work_queue_only_waits_on_earlier_items():
         w, e = offline(s)
         engines.append(e)
         queries.append(e.query(w.plan))
+    # a build side that is itself a join: its build items must wait for the inner build
+    queries.append(engines[-3].query(NESTED_BUILD_PLAN))
     b = Batch(queries, tiles_per_item=4)
     items = b.items()
     assert len(items) == b.info()["work_items"]
@@ -118,6 +135,17 @@ def test_batch_work_queue_only_waits_on_earlier_items():
     assert waits_on_clears
     for r in waits_on_clears:
         assert produced[r[F["dep"]]] == r[F["dep_target"]]
+    # the nested query (last): date build, then the customer build that probes it, then the
+    # fact pipeline -- three distinct done-counters chained by their waits
+    nested = [r for r in work if r[F["params"]] >= sorted(set(work[:, F["params"]]))[-3]]
+    done_counters = []
+    for r in nested:
+        if r[F["done"]] not in done_counters:
+            done_counters.append(r[F["done"]])
+    assert len(done_counters) == 3, done_counters
+    by_done = {d: [r for r in nested if r[F["done"]] == d] for d in done_counters}
+    assert all(r[F["dep"]] == done_counters[0] for r in by_done[done_counters[1]])
+    assert all(r[F["dep"]] == done_counters[1] for r in by_done[done_counters[2]])
 
 
 @pytest.mark.parametrize("spec", SPECS)
@@ -154,3 +182,26 @@ def test_flavor_beyond_the_shared_memory_limit_is_rejected_at_creation():
         e.query(w.plan, "cuda(threads=512,rows=8,load=tma,stages=4)")
     assert ex.value.code == 6
     assert "shared memory" in str(ex.value)
+
+
+JOIN_N_PLAN = ("(aggr hash ((col customer.c_region)) ((fun sum (col lineorder.lo_revenue)) (fun count))"
+               " (join joinN ((col customer.c_custkey)) () (scan customer (c_custkey c_region))"
+               " ((col lineorder.lo_custkey)) ((col lineorder.lo_revenue)) (scan lineorder (lo_custkey lo_revenue))))")
+
+
+@pytest.mark.parametrize("flavor", FLAVORS)
+def test_join_n_plans_compile(flavor):
+    """JoinN probes: a hash table (never dense: duplicates need their own slots) and a match
+    loop around the rest of the pipeline."""
+    w, e = offline("star:rows=1000,custs=50")
+    q = e.query(JOIN_N_PLAN, flavor)
+    src = q.source()
+    assert "__any_sync" in src and "VD_MAX_PROBES * SPB" in src
+    assert "vd::dense_test" not in src
+
+
+def test_join_n_rejects_dense_builds():
+    w, e = offline("star:rows=1000,custs=50")
+    with pytest.raises(VoilaError) as ex:
+        e.query(JOIN_N_PLAN, "cuda(build=dense)")
+    assert ex.value.code == 6

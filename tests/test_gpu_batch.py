@@ -72,3 +72,27 @@ def test_batch_mixing_smem_and_probe_heavy_shapes():
         b.wait()
         for s, q, e in zip(specs, queries, expect):
             assert q.result_lines() == e, s
+
+
+def test_batch_with_a_join_whose_build_side_is_a_join():
+    """The customer table's build probes the date table: inside the persistent kernel it must
+    wait for the date build, or it silently misses rows."""
+    from helpers import NESTED_BUILD_PLAN
+    spec = "star:rows=200000,custs=30000,supps=200,parts=14000,seed=11"
+    w = workload(spec)
+    data = generate_workload_host(w)
+    e = Engine(0)
+    e.load_workload(w, data=data)
+    expect = result_lines(run_plan(NESTED_BUILD_PLAN, data))
+    assert expect and expect[0] != "0|0"
+    q = e.query(NESTED_BUILD_PLAN)
+    q.run()
+    assert q.result_lines() == expect
+    others, oq, oexp = _setup(batch_specs(6, seed=8, min_rows=10_000, max_rows=200_000))
+    b = Batch([q] + oq, tiles_per_item=2)
+    for _ in range(3):
+        b.run()
+        b.wait()
+        assert q.result_lines() == expect
+        for x, ex in zip(oq, oexp):
+            assert x.result_lines() == ex

@@ -17,7 +17,6 @@ FLAVORS = ["", "cuda(rows=8,threads=128,load=tma,stages=3)", "cuda(aggr=cache,ca
            "cuda(load=tma,build=staged,rows=2,lowcard=atomic)", "cuda(compact=0,lowcard=private,rows=8)",
            "cuda(hash=voila,lowcard=private,threads=128,fill=75)", "cuda(build=direct,prefetch=0)",
            "cuda(lowcard=redux,aggr=cache,cache=64)"]
-UNSUPPORTED = {"join_n"}  # JoinN probes are rejected by the CUDA flavor for now
 
 
 def run_gpu(w, plan, flavor="", on_device=False, data=None):
@@ -36,11 +35,6 @@ def run_gpu(w, plan, flavor="", on_device=False, data=None):
 def test_golden(name, entry, flavor):
     w = workload(entry["spec"])
     plan = entry["plan"] or w.plan
-    if name in UNSUPPORTED:
-        with pytest.raises(VoilaError) as ex:
-            run_gpu(w, plan, flavor)
-        assert ex.value.code == 6
-        return
     assert run_gpu(w, plan, flavor) == golden_lines(name, "vectorwise")
 
 

@@ -20,7 +20,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", 
 CXX_FLAGS = ["-O2", "-g", "-fPIC", "-std=c++17", "-Wall", "-Wno-unused-function", "-ffp-contract=off"]
 
 CPP_SOURCES = ["engine.cpp", "plan.cpp", "codegen.cpp", "jit.cpp", "batch.cpp"]
-CU_SOURCES = ["datagen.cu", "mlp.cu", "noalloc.cu"]
+CU_SOURCES = ["datagen.cu", "mlp.cu", "noalloc.cu", "floor.cu"]
 HEADERS = ["datagen.h", "engine_internal.hpp", "sexpr.hpp", "workloads.hpp", "device/voila_device.cuh"]
 
 

@@ -9,9 +9,10 @@
  * from a device work queue in dependency order (see generate_batch).  The launch (clears
  * included) is captured once into a CUDA graph and replayed.
  *
- * Waits on dependencies are bounded (2 s); a wait that gives up records VD_ERR_WAIT_TIMEOUT
- * in the batch's error word and the item is skipped, so a stuck batch ends with an error
- * instead of a hang.
+ * Waits on dependencies are bounded (2 s unless vc_batch_set_wait_limit says otherwise); a
+ * wait that gives up records VD_ERR_WAIT_TIMEOUT in the batch's error word and the item is
+ * skipped (it still counts as done, so nothing waits on it in turn), so a stuck batch ends
+ * with an error instead of a hang.
  */
 #include <algorithm>
 #include <cstring>
@@ -64,7 +65,10 @@ static void add_clears_in_order(Batch& b, BatchCode& bc)
 	std::vector<std::vector<BatchItem>> clears(nq);
 	const int64_t chunk = 8ll << 20;
 	for (size_t qi = 0; qi < nq; qi++) {
-		for (auto& m : state_of(*b.queries[qi]).memsets) {
+		QueryState& qst = state_of(*b.queries[qi]);
+		std::vector<std::pair<void*, size_t>> all = qst.memsets;
+		all.insert(all.end(), qst.clean_memsets.begin(), qst.clean_memsets.end());
+		for (auto& m : all) {
 			const int64_t bytes = (int64_t)((m.second + 15) & ~(size_t)15); /* allocations are 256-byte granular */
 			const int64_t poff = (int64_t)bc.params.size();
 			bc.params.push_back((unsigned long long)(uintptr_t)m.first);
@@ -175,7 +179,7 @@ static void batch_launch_all(Batch& b, cudaStream_t s)
 	VC_CHECK_CUDA(cudaMemsetAsync(b.counters, 0, book, s));
 	long long nwork = b.nitems;
 	int nq = (int)b.queries.size();
-	void* args[] = {&b.items, &nwork, &b.counters, &b.params, &b.finish, &nq, &b.err};
+	void* args[] = {&b.items, &nwork, &b.counters, &b.params, &b.finish, &nq, &b.err, &b.wait_ns};
 	VC_CHECK_CUDA(cudaLaunchKernel((const void*)b.kernel, dim3((unsigned)b.grid), dim3((unsigned)b.flavor.threads), args,
 		b.smem, s));
 }
@@ -275,6 +279,12 @@ int vc_batch_wait(vc_batch* h)
 		VC_CHECK_CUDA(cudaStreamSynchronize(b.stream));
 		unsigned err = 0;
 		VC_CHECK_CUDA(cudaMemcpy(&err, b.err, sizeof(err), cudaMemcpyDeviceToHost));
+		if (err) {
+			/* skipped items may leave the queries' self-cleaning tables set */
+			for (Query* q : b.queries) {
+				q->dirty = true;
+			}
+		}
 		if (err & 2u) {
 			throw Error(VC_ERR_TIMEOUT, "a batch dependency wait gave up");
 		}
@@ -370,6 +380,62 @@ int vc_batch_items(vc_batch* h, int64_t* out, int64_t cap, int64_t* n)
 			r[6] = it.end;
 			r[7] = it.params;
 		}
+	});
+}
+
+int vc_batch_set_wait_limit(vc_batch* h, uint64_t ns)
+{
+	return abi_guard_mlp([&] {
+		if (!h || ns < 1000 || ns > 60000000000ull) {
+			throw Error(VC_ERR_INVALID, "wait limit must be between 1 us and 60 s");
+		}
+		Batch& b = h->b;
+		if (b.wait_ns != ns) {
+			b.wait_ns = ns;
+			if (b.graph) {
+				/* the limit is a kernel argument of the captured launch */
+				VC_CHECK_CUDA(cudaGraphExecDestroy(b.graph));
+				b.graph = nullptr;
+			}
+		}
+	});
+}
+
+int vc_batch_hold_item(vc_batch* h, int64_t index, int hold)
+{
+	return abi_guard_mlp([&] {
+		if (!h || index < 0 || index >= h->b.nitems) {
+			throw Error(VC_ERR_INVALID, "no such work item");
+		}
+		Batch& b = h->b;
+		if (b.eng->offline) {
+			throw Error(VC_ERR_NO_DEVICE, "an offline engine only generates and compiles code");
+		}
+		VC_CHECK_CUDA(cudaSetDevice(b.eng->device));
+		if (b.stream) {
+			VC_CHECK_CUDA(cudaStreamSynchronize(b.stream));
+		}
+		auto it = std::find(b.held_index.begin(), b.held_index.end(), index);
+		BatchItem item = b.host_items[(size_t)index];
+		if (hold) {
+			if (it == b.held_index.end()) {
+				b.held_index.push_back(index);
+				b.held.push_back(item);
+			}
+			/* the clears' counter never reaches this: the item's bounded wait runs out */
+			item.dep = 1;
+			item.dep_target = (int64_t)1 << 62;
+		} else {
+			if (it == b.held_index.end()) {
+				return;
+			}
+			const size_t k = (size_t)(it - b.held_index.begin());
+			item = b.held[k];
+			b.held.erase(b.held.begin() + (long)k);
+			b.held_index.erase(it);
+		}
+		b.host_items[(size_t)index] = item;
+		VC_CHECK_CUDA(cudaMemcpy(b.items + index, &item, sizeof(BatchItem), cudaMemcpyHostToDevice));
 	});
 }
 

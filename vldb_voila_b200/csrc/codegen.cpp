@@ -135,6 +135,48 @@ struct PipeGen {
 	}
 
 	int A() const { return (int)p.sink.aggs.size(); }
+	/* stored key width of the split hash group table */
+	int gkey_bytes() const { return p.sink.key_bits <= 31 ? 4 : 8; }
+	std::string gkey_type() const { return p.sink.key_bits <= 31 ? "uint32_t" : "uint64_t"; }
+
+	/* bits of value - lo for one row of aggregate a (the per-row span of the warp pre-sum) */
+	int row_bits(int a) const {
+		const auto& ag = p.sink.aggs[a];
+		const __int128 span = ag.arg->b.hi - ag.arg->b.lo;
+		if (span < 0 || span >= ((__int128)1 << 64)) {
+			return 64;
+		}
+		int bits = 0;
+		for (unsigned __int128 x = (unsigned __int128)span; x; x >>= 1) {
+			bits++;
+		}
+		return std::max(bits, 1);
+	}
+
+	/* Warp pre-aggregation into packed accumulator words: lanes with the same group key
+	 * (__match_any_sync) sum each aggregate's biased value with redux.sync; the sums are
+	 * shifted into their word's bit field.  `lead` marks each group's lowest active lane. */
+	void emit_packed_words(const std::string& key, const std::string& v) {
+		const Sink& s = p.sink;
+		o << "      const unsigned gm = __match_any_sync(0xffffffffu, " << key << ");\n";
+		o << "      const bool lead = act[" << v << "] && (gm & vd::lanemask_lt()) == 0u;\n";
+		o << "      uint64_t w[" << s.nwords << "] = {";
+		for (int i = 0; i < s.nwords; i++) {
+			o << (i ? ", " : "") << "0ull";
+		}
+		o << "};\n";
+		for (int a = 0; a < A(); a++) {
+			const auto& ag = s.aggs[a];
+			const std::string sh = std::to_string(s.agg_shift[a]);
+			if (ag.count) {
+				o << "      w[" << s.agg_word[a] << "] += (uint64_t)__popc(gm) << " << sh << ";\n";
+				continue;
+			}
+			const std::string lo = P((unsigned long long)(int64_t)ag.arg->b.lo);
+			o << "      w[" << s.agg_word[a] << "] += vd::group_sum_u<" << row_bits(a) << ">(gm, (uint64_t)(" << expr(ag.arg, v)
+			  << ") - (uint64_t)" << lo << ") << " << sh << ";\n";
+		}
+	}
 
 	/* Warp pre-aggregation of one row per lane: the lanes holding the same group key (`key`,
 	 * a 32- or 64-bit expression that is `sentinel` on inactive lanes) form a group; each
@@ -424,8 +466,17 @@ struct PipeGen {
 		return r;
 	}
 
+	bool has_join_n() const {
+		for (auto& op : p.ops) {
+			if (op.kind == Op::Probe && !plan.joins[op.join].join01) {
+				return true;
+			}
+		}
+		return false;
+	}
+
 	void plan_phases() {
-		compact_at = fl.compact;
+		compact_at = has_join_n() ? -1 : fl.compact;
 		if (compact_at == -2) {
 			/* auto: after the first probe when more probes follow */
 			compact_at = -1;
@@ -501,6 +552,100 @@ struct PipeGen {
 		}
 	}
 
+	/* ops [from, end) and the sink; a JoinN probe turns the rest of the pipeline into the body
+	 * of its loop over matches */
+	void emit_rest(int from) {
+		for (int i = from; i < (int)p.ops.size(); i++) {
+			const Op& op = p.ops[i];
+			if (op.kind == Op::Probe && !plan.joins[op.join].join01) {
+				gen_probe_n(i, op);
+				return;
+			}
+			emit_ops(i, i + 1);
+		}
+		sink_row();
+	}
+
+	/* sinks whose rows use block-wide collectives (appends): loops around them must be
+	 * uniform over the block, not just the warp */
+	bool sink_block_collective() const {
+		return p.sink.kind == Sink::Emit ||
+			(p.sink.kind == Sink::JoinBuild && !plan.joins[p.sink.join].direct && !plan.joins[p.sink.join].dense);
+	}
+
+	/*
+	 * JoinN probe (relalg_translator.cpp:1032-1042 without the Join01 exit; bucket_next,
+	 * kernel_generator.py:543-555): every build row with the probe row's key is a match and
+	 * the rest of the pipeline runs once per match.  The table keeps duplicate keys in
+	 * separate slots of the probe sequence, which ends at the first empty slot.  Each round
+	 * of the loop gives every row at most one more match (act = has one); the loop runs
+	 * while any row of the warp (or block, for appending sinks) still has slots to scan, so
+	 * the warp-wide pre-aggregation of the sink sees converged warps.
+	 */
+	void gen_probe_n(int opi, const Op& op) {
+		JoinDesc& jd = plan.joins[op.join];
+		const std::string KT = jd.key64 ? "uint64_t" : "uint32_t";
+		const std::string S = join_slot_type(jd);
+		const std::string j = std::to_string(opi);
+		for (int k = 0; k < op.npay; k++) {
+			o << "    int64_t pay" << j << "_" << k << "[" << V << "];\n";
+		}
+		o << "    {\n";
+		o << "      const " << S << "* __restrict__ jt" << j << " = " << Pptr(jd.table, "const " + S + "*") << ";\n";
+		if (jd.direct) {
+			o << "      const uint64_t bmask" << j << " = " << Pu(jd.direct_bmask) << ";\n";
+		} else {
+			/* staged build: the table was sized by the materialised count */
+			o << "      const uint64_t bmask" << j << " = ((const unsigned long long*)" << Pptr(jd.words, "const void*")
+			  << ")[1];\n";
+		}
+		o << "      constexpr int SPB" << j << " = vd::slots_per_bucket<" << S << ">();\n";
+		o << "      uint64_t nb" << j << "[" << V << "]; int ns" << j << "[" << V << "]; int ng" << j << "[" << V << "]; "
+		  << KT << " nk" << j << "[" << V << "]; bool np" << j << "[" << V << "];\n";
+		o << "#pragma unroll\n      for (int v = 0; v < " << V << "; v++) {\n";
+		std::string inrange = "act[v]";
+		std::string packed = "0ull";
+		for (size_t k = 0; k < op.keys.size(); k++) {
+			const std::string kv = expr(op.keys[k], "v");
+			const std::string lo = P((unsigned long long)(int64_t)jd.key_b[k].lo);
+			const std::string span = Pu((unsigned long long)(int64_t)(jd.key_b[k].hi - jd.key_b[k].lo));
+			inrange += " && (uint64_t)(" + kv + " - " + lo + ") <= " + span;
+			packed += " | ((uint64_t)(" + kv + " - " + lo + ") << " + P((unsigned long long)jd.key_shift[k]) + ")";
+		}
+		o << "        const bool ok = " << inrange << ";\n";
+		o << "        const uint64_t pk = " << packed << ";\n";
+		o << "        nk" << j << "[v] = (" << KT << ")(pk + 1ull);\n";
+		o << "        nb" << j << "[v] = (" << table_hash(op.keys, "pk", jd.key_bits, "v") << ") & bmask" << j << ";\n";
+		o << "        ns" << j << "[v] = 0; ng" << j << "[v] = 0; np" << j << "[v] = ok;\n";
+		o << "      }\n";
+		o << "      for (;;) {\n";
+		o << "        bool anyp = false;\n";
+		o << "#pragma unroll\n        for (int v = 0; v < " << V << "; v++) { anyp = anyp || np" << j << "[v]; }\n";
+		if (sink_block_collective()) {
+			o << "        if (!vd::block_any(anyp)) { break; }\n";
+		} else {
+			o << "        if (!__any_sync(0xffffffffu, anyp)) { break; }\n";
+		}
+		o << "#pragma unroll\n        for (int v = 0; v < " << V << "; v++) {\n";
+		o << "          uint64_t raw = 0;\n";
+		o << "          act[v] = false;\n";
+		o << "          while (np" << j << "[v]) {\n";
+		o << "            if (++ng" << j << "[v] > VD_MAX_PROBES * SPB" << j << ") { atomicOr(err, VD_ERR_TABLE_FULL); np" << j
+		  << "[v] = false; break; }\n";
+		o << "            const " << S << "* sp = jt" << j << " + nb" << j << "[v] * SPB" << j << " + ns" << j << "[v];\n";
+		o << "            const " << KT << " sk = vd::table_ld(&sp->key);\n";
+		o << "            if (++ns" << j << "[v] == SPB" << j << ") { ns" << j << "[v] = 0; nb" << j << "[v] = (nb" << j
+		  << "[v] + 1) & bmask" << j << "; }\n";
+		o << "            if (sk == 0) { np" << j << "[v] = false; break; }\n";
+		o << "            if (sk == nk" << j << "[v]) { act[v] = true; raw = (uint64_t)vd::table_ld(&sp->pay); break; }\n";
+		o << "          }\n";
+		emit_payload_unpack(op, jd, j, "raw");
+		o << "        }\n";
+		emit_rest(opi + 1);
+		o << "      }\n";
+		o << "    }\n";
+	}
+
 	/* one tile's work for the tile index `t`: loads (mode "ldg", "smem" or "pre" = the
 	 * eager columns are already in x<c>), ops, sink */
 	void emit_body(const std::string& mode) {
@@ -513,8 +658,7 @@ struct PipeGen {
 			emit_load_cols(mode, "x", "r0");
 		}
 		if (compact_at < 0) {
-			emit_ops(0, (int)p.ops.size());
-			sink_row();
+			emit_rest(0);
 			o << "    }\n";
 			return;
 		}
@@ -542,8 +686,7 @@ struct PipeGen {
 			o << "      int64_t pay" << carried[k].first << "_" << carried[k].second << "[1] = {live ? ccar" << k
 			  << "[ci] : 0};\n";
 		}
-		emit_ops(compact_at + 1, (int)p.ops.size());
-		sink_row();
+		emit_rest(compact_at + 1);
 		V = saveV;
 		o << "    }\n";
 		o << "    vd::block_sync();\n";
@@ -606,9 +749,6 @@ struct PipeGen {
 
 	void gen_probe(int opi, const Op& op) {
 		JoinDesc& jd = plan.joins[op.join];
-		if (!jd.join01) {
-			throw Error(6, "joinN probes are not supported by the CUDA flavor yet");
-		}
 		const std::string KT = jd.key64 ? "uint64_t" : "uint32_t";
 		const std::string PT = jd.pay64 ? "uint64_t" : "uint32_t";
 		const std::string S = join_slot_type(jd);
@@ -727,18 +867,25 @@ struct PipeGen {
 			}
 			break;
 		}
-		case Sink::AggHash:
-			o << "  unsigned long long* const gtab = " << Pptr(st.sink_dev, "unsigned long long*") << ";\n";
-			o << "  const uint64_t gmask = " << Pu((unsigned long long)(st.sink_cap - 1)) << ";\n";
+		case Sink::AggHash: {
+			const std::string K = gkey_type();
+			const int W = s.nwords;
+			o << "  " << K << "* const gkeys = " << Pptr(st.sink_dev, K + "*") << ";\n";
+			o << "  unsigned long long* const gacc = " << Pptr(st.sink_acc, "unsigned long long*") << ";\n";
+			o << "  const uint64_t gbmask = " << Pu((unsigned long long)(st.sink_cap / (32 / gkey_bytes()) - 1)) << ";\n";
 			if (fl.aggr == "cache") {
 				const int S = (int)pow2_at_least(std::max(32, fl.cache_slots));
-				smem_sink = (size_t)S * (1 + A()) * 8;
-				o << "  unsigned long long* const scache = (unsigned long long*)vd_smem;\n";
-				o << "  for (int i = threadIdx.x; i < " << S * (1 + A()) << "; i += blockDim.x) { scache[i] = 0ull; }\n";
+				const size_t kbytes = ((size_t)S * gkey_bytes() + 15) & ~(size_t)15;
+				smem_sink = kbytes + (size_t)S * W * 8;
+				o << "  " << K << "* const ckeys = (" << K << "*)vd_smem;\n";
+				o << "  unsigned long long* const cacc = (unsigned long long*)(vd_smem + " << kbytes << ");\n";
+				o << "  for (int i = threadIdx.x; i < " << S << "; i += blockDim.x) { ckeys[i] = 0; }\n";
+				o << "  for (int i = threadIdx.x; i < " << S * W << "; i += blockDim.x) { cacc[i] = 0ull; }\n";
 				o << "  vd::block_sync();\n";
 				cache_slots = S;
 			}
 			break;
+		}
 		case Sink::JoinBuild: {
 			JoinDesc& jd = plan.joins[s.join];
 			const std::string S = join_slot_type(jd);
@@ -831,22 +978,22 @@ struct PipeGen {
 			for (auto& k : s.keys) {
 				kb.push_back(k->b);
 			}
+			const std::string K = gkey_type();
+			const int W = s.nwords;
 			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
 			o << "      const uint64_t pk = act[v] ? (" << packed_key(s.keys, kb, s.key_shift, "v") << ") : 0ull;\n";
-			o << "      " << agg_vals("v") << "\n";
-			if (s.key_bits < 64) {
-				emit_group_reduce("act[v] ? (unsigned long long)pk : ~0ull");
-				o << "      if (lead) {\n";
-			} else {
-				o << "      if (vd::warp_combine<" << A() << ">(pk, act[v], vals)) {\n";
-			}
+			emit_packed_words("act[v] ? (unsigned long long)pk : ~0ull", "v");
+			o << "      if (lead) {\n";
 			o << "        const uint64_t h = " << table_hash(s.keys, "pk", s.key_bits, "v") << ";\n";
+			o << "        const " << K << " key = (" << K << ")(pk + 1ull);\n";
 			if (fl.aggr == "cache") {
-				o << "        if (!vd::cache_add<" << A() << ">(scache, " << cache_slots << ", h, pk + 1ull, vals)) {\n";
-				o << "          vd::group_add<" << A() << ">(gtab, gmask, h, pk + 1ull, vals, err);\n";
+				o << "        if (!vd::gt_cache_add<" << K << ", " << W << ">(ckeys, cacc, " << cache_slots << ", h, key, w)) {\n";
+				o << "          const int64_t slot = vd::gt_find_or_insert<" << K << ">(gkeys, gbmask, h, key, err);\n";
+				o << "          if (slot >= 0) { vd::gt_add<" << W << ">(gacc, slot, w); }\n";
 				o << "        }\n";
 			} else {
-				o << "        vd::group_add<" << A() << ">(gtab, gmask, h, pk + 1ull, vals, err);\n";
+				o << "        const int64_t slot = vd::gt_find_or_insert<" << K << ">(gkeys, gbmask, h, key, err);\n";
+				o << "        if (slot >= 0) { vd::gt_add<" << W << ">(gacc, slot, w); }\n";
 			}
 			o << "      }\n    }\n";
 			break;
@@ -980,14 +1127,15 @@ struct PipeGen {
 			break;
 		case Sink::AggHash:
 			if (fl.aggr == "cache") {
+				const std::string K = gkey_type();
+				const int W = s.nwords;
 				o << "  vd::block_sync();\n";
 				o << "  for (int i = threadIdx.x; i < " << cache_slots << "; i += blockDim.x) {\n";
-				o << "    const unsigned long long sk = scache[i * " << (1 + A()) << "];\n";
-				o << "    if (sk != 0ull) {\n";
-				o << "      int64_t vals[" << A() << "];\n";
-				o << "#pragma unroll\n      for (int a = 0; a < " << A() << "; a++) { vals[a] = (int64_t)scache[i * "
-				  << (1 + A()) << " + 1 + a]; }\n";
-				o << "      const uint64_t pk = sk - 1ull;\n";
+				o << "    const " << K << " sk = ckeys[i];\n";
+				o << "    if (sk != 0) {\n";
+				o << "      uint64_t w[" << W << "];\n";
+				o << "#pragma unroll\n      for (int a = 0; a < " << W << "; a++) { w[a] = cacc[i * " << W << " + a]; }\n";
+				o << "      const uint64_t pk = (uint64_t)sk - 1ull;\n";
 				std::string h;
 				for (size_t k = 0; k < s.keys.size(); k++) {
 					const int bits = (k + 1 < s.keys.size() ? s.key_shift[k + 1] : s.key_bits) - s.key_shift[k];
@@ -999,7 +1147,8 @@ struct PipeGen {
 				if (fl.hash != "voila") {
 					h = s.key_bits <= 32 ? "vd::mix_hash32((uint32_t)pk)" : "vd::mix_hash64(pk)";
 				}
-				o << "      vd::group_add<" << A() << ">(gtab, gmask, " << h << ", sk, vals, err);\n";
+				o << "      const int64_t slot = vd::gt_find_or_insert<" << K << ">(gkeys, gbmask, " << h << ", sk, err);\n";
+				o << "      if (slot >= 0) { vd::gt_add<" << W << ">(gacc, slot, w); }\n";
 				o << "    }\n  }\n";
 			}
 			break;
@@ -1043,7 +1192,9 @@ struct PipeGen {
 		return k.str();
 	}
 
-	/* hash-group extraction: rows with count > 0, keys unpacked, visible aggregates */
+	/* Hash-group extraction: rows with count > 0, keys unpacked, each visible aggregate's field
+	 * taken out of its word and un-biased (sum = field + lo * count).  Every slot it reads is
+	 * zeroed again, so the table is clear for the next run without a memset. */
 	std::string gen_extract() {
 		Sink& s = p.sink;
 		std::ostringstream k;
@@ -1056,14 +1207,16 @@ struct PipeGen {
 			k << "extern \"C\" __global__ void __launch_bounds__(256) " << name << "_extract(const VcParams p) {\n";
 			k << "  vd::pdl_launch_dependents();\n  vd::pdl_wait();\n";
 		}
+		const std::string K = gkey_type();
+		const int W = s.nwords;
 		k << "  int64_t* const out = " << Pptr(qs.out, "int64_t*") << ";\n";
 		k << "  const int64_t ocap = " << P((unsigned long long)qs.out_cap) << ";\n";
 		k << "  unsigned long long* const ocount = " << Pptr(qs.out_count, "unsigned long long*") << ";\n";
-		k << "  const unsigned long long* const g = " << Pptr(st.sink_dev, "const unsigned long long*") << ";\n";
-		const int W = 1 + A();
+		k << "  " << K << "* const gkeys = " << Pptr(st.sink_dev, K + "*") << ";\n";
+		k << "  unsigned long long* const gacc = " << Pptr(st.sink_acc, "unsigned long long*") << ";\n";
 		k << "  const int64_t nslots = " << P((unsigned long long)st.sink_cap) << ";\n";
-		/* each warp covers kExtractK groups of 32 slots per step: all their key and count
-		 * words are loaded (from L2, coherent) before any is used */
+		/* each warp covers kExtractK groups of 32 slots per step: all their keys are loaded
+		 * (from L2, coherent) before any is used */
 		if (item) {
 			/* one item = slot groups [t_begin, t_end) of blockDim.x * kExtractK slots */
 			k << "  const int64_t stride = (int64_t)blockDim.x * " << kExtractK << ";\n";
@@ -1075,15 +1228,26 @@ struct PipeGen {
 			k << "  for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * " << kExtractK
 			  << "; base < nslots; base += stride) {\n";
 		}
-		k << "    unsigned long long kw[" << kExtractK << "]; long long cw[" << kExtractK << "];\n";
+		k << "    " << K << " kw[" << kExtractK << "];\n";
 		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
 		k << "      const int64_t i = base + q * 32 + (threadIdx.x & 31);\n";
-		k << "      kw[q] = i < nslots ? __ldcg(&g[i * " << W << "]) : 0ull;\n";
-		k << "      cw[q] = i < nslots ? (long long)__ldcg(&g[i * " << W << " + 1 + " << s.count_idx << "]) : 0;\n";
+		k << "      kw[q] = i < nslots ? __ldcg(&gkeys[i]) : (" << K << ")0;\n";
 		k << "    }\n";
 		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
 		k << "    const int64_t i = base + q * 32 + (threadIdx.x & 31);\n";
-		k << "    const bool take = kw[q] != 0ull && cw[q] > 0;\n";
+		k << "    uint64_t w[" << W << "];\n";
+		k << "#pragma unroll\n    for (int a = 0; a < " << W << "; a++) { w[a] = kw[q] != 0 ? __ldcg(&gacc[i * " << W
+		  << " + a]) : 0ull; }\n";
+		auto field = [&](int a) {
+			const int bits = s.agg_bits[a];
+			const unsigned long long mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
+			return "((w[" + std::to_string(s.agg_word[a]) + "] >> " + std::to_string(s.agg_shift[a]) + ") & " +
+				std::to_string(mask) + "ull)";
+		};
+		k << "    const int64_t cnt = (int64_t)" << field(s.count_idx) << ";\n";
+		k << "    const bool take = kw[q] != 0 && cnt > 0;\n";
+		k << "    if (kw[q] != 0) {\n      gkeys[i] = 0;\n";
+		k << "#pragma unroll\n      for (int a = 0; a < " << W << "; a++) { gacc[i * " << W << " + a] = 0ull; }\n    }\n";
 		k << "    const int64_t pos = vd::warp_append(ocount, take);\n";
 		k << "    if (take && pos < ocap) {\n";
 		int col = 0;
@@ -1091,14 +1255,20 @@ struct PipeGen {
 			const std::string lo = P((unsigned long long)(int64_t)s.keys[kk]->b.lo);
 			const int bits = (kk + 1 < s.keys.size() ? s.key_shift[kk + 1] : s.key_bits) - s.key_shift[kk];
 			const unsigned long long mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
-			k << "      out[" << col << " * ocap + pos] = " << lo << " + (int64_t)(((kw[q] - 1ull) >> "
+			k << "      out[" << col << " * ocap + pos] = " << lo << " + (int64_t)((((uint64_t)kw[q] - 1ull) >> "
 			  << P((unsigned long long)s.key_shift[kk]) << ") & " << Pu(mask) << ");\n";
 		}
 		for (int a = 0; a < A(); a++) {
 			if (!s.aggs[a].visible) {
 				continue;
 			}
-			k << "      out[" << col << " * ocap + pos] = (int64_t)g[i * " << W << " + " << 1 + a << "];\n";
+			if (s.aggs[a].count) {
+				k << "      out[" << col << " * ocap + pos] = cnt;\n";
+			} else {
+				const std::string lo = P((unsigned long long)(int64_t)s.aggs[a].arg->b.lo);
+				k << "      out[" << col << " * ocap + pos] = (int64_t)(" << field(a) << " + (uint64_t)" << lo
+				  << " * (uint64_t)cnt);\n";
+			}
 			col++;
 		}
 		k << "    }\n    }\n  }\n}\n\n";
@@ -1173,12 +1343,18 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 /*
  * Batch code: every pipeline of every query becomes a device item function (deduplicated by
  * generated text, so instances of one shape share code) and a list of work items over its
- * tiles.  Items are ordered by phase -- phase 0: join builds and pipelines without inputs
- * from other pipelines, phase 1: probes that read a built table, phase 2: group extraction --
- * and carry the done-counter they must wait for, so the persistent kernel's queue runs them
- * in dependency order.  Phase-0 items wait for the state clears the runtime prepends
- * (dep_target -2 is patched with their count).  Counter 0 is the queue head, counter 1
- * counts finished clears.
+ * tiles.  Items are ordered by dependency level and carry the done-counter they must wait
+ * for, so the persistent kernel's queue runs them in dependency order:
+ *   level L of a query's join builds: a build pipeline that probes no join is level 0; one
+ *     whose rows probe other joins (a build side that is itself a join chain) is one level
+ *     above the builds of those joins.  Level-0 builds wait for the query's state clears
+ *     (dep_target -2, patched by the runtime with their count), level-L builds for every
+ *     item of level L-1;
+ *   the query's other pipelines (probes, aggregations, emits) wait for the top build level;
+ *   group extraction waits for its group-by pipeline.
+ * The queue concatenates the phases in level order across queries, so an item only ever
+ * waits for items earlier in the queue.  Counter 0 is the queue head, counter 1 counts
+ * finished clears.
  */
 BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>& flavors, int threads,
 	int64_t tiles_per_item)
@@ -1187,7 +1363,13 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 	std::map<std::string, int> shape_of;
 	std::vector<std::string> shape_fn;
 	std::ostringstream funcs;
-	std::vector<BatchItem> phases[3];
+	std::vector<std::vector<BatchItem>> phases;
+	auto phase_list = [&](size_t ph) -> std::vector<BatchItem>& {
+		if (ph >= phases.size()) {
+			phases.resize(ph + 1);
+		}
+		return phases[ph];
+	};
 	int ncounters = 2;
 	auto add_shape = [&](const std::string& text, const std::string& suffix) -> int {
 		auto it = shape_of.find(text);
@@ -1223,12 +1405,46 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 		qs.out = q.out;
 		qs.out_cap = q.out_cap;
 		qs.out_count = q.out_count;
-		int build_counter = -1;
-		int64_t build_items = 0;
+		const int64_t tile = (int64_t)fl.threads * fl.rows;
+		auto items_of = [&](const Pipeline& p) {
+			const int64_t ntiles = std::max<int64_t>((p.rows + tile - 1) / tile, 1);
+			return (ntiles + tiles_per_item - 1) / tiles_per_item;
+		};
+		/* dependency levels of the join builds, and the work items per level */
+		std::vector<int> level(q.plan.pipes.size(), 0);
+		std::map<int, int> build_pipe_of_join;
+		int top_level = -1;
 		for (auto& p : q.plan.pipes) {
 			if (p.sink.kind == Sink::JoinBuild && !q.plan.joins[p.sink.join].direct) {
 				throw Error(6, "batched queries need direct join builds (build=staged is not batchable)");
 			}
+			int lv = 0;
+			for (auto& op : p.ops) {
+				if (op.kind == Op::Probe) {
+					auto b = build_pipe_of_join.find(op.join);
+					if (b == build_pipe_of_join.end()) {
+						throw Error(6, "batch: a pipeline probes a join whose build pipeline comes later");
+					}
+					lv = std::max(lv, level[b->second] + 1);
+				}
+			}
+			level[p.id] = lv;
+			if (p.sink.kind == Sink::JoinBuild) {
+				build_pipe_of_join[p.sink.join] = p.id;
+				top_level = std::max(top_level, lv);
+			}
+		}
+		std::vector<int> level_counter(top_level + 1, -1);
+		std::vector<int64_t> level_items(top_level + 1, 0);
+		for (auto& p : q.plan.pipes) {
+			if (p.sink.kind == Sink::JoinBuild) {
+				if (level_counter[level[p.id]] < 0) {
+					level_counter[level[p.id]] = ncounters++;
+				}
+				level_items[level[p.id]] += items_of(p);
+			}
+		}
+		for (auto& p : q.plan.pipes) {
 			std::vector<unsigned long long> prm;
 			/* the query keeps its own parameter layout for standalone runs */
 			const int saved_err = p.err_slot;
@@ -1250,20 +1466,25 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 			bc.params.insert(bc.params.end(), prm.begin(), prm.end());
 
 			const int sid = add_shape(main_src, "_main");
-			const int64_t tile = (int64_t)fl.threads * fl.rows;
 			const int64_t ntiles = std::max<int64_t>((p.rows + tile - 1) / tile, 1);
-			const int64_t nit = (ntiles + tiles_per_item - 1) / tiles_per_item;
+			const int64_t nit = items_of(p);
 			const bool is_build = p.sink.kind == Sink::JoinBuild;
-			int counter;
+			/* phase (position in the queue), the counter waited for and its target */
+			size_t phase;
+			int dep, counter;
+			int64_t dep_target;
 			if (is_build) {
-				if (build_counter < 0) {
-					build_counter = ncounters++;
-				}
-				counter = build_counter;
+				const int lv = level[p.id];
+				phase = (size_t)lv;
+				counter = level_counter[lv];
+				dep = lv == 0 ? 1 : level_counter[lv - 1];
+				dep_target = lv == 0 ? -2 : level_items[lv - 1];
 			} else {
+				phase = (size_t)(top_level + 1);
 				counter = ncounters++;
+				dep = top_level < 0 ? 1 : level_counter[top_level];
+				dep_target = top_level < 0 ? -2 : level_items[top_level];
 			}
-			const int phase = is_build ? 0 : (build_counter >= 0 ? 1 : 0);
 			for (int64_t k = 0; k < nit; k++) {
 				BatchItem it;
 				it.shape = sid;
@@ -1271,14 +1492,11 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 				it.begin = k; /* tiles k, k + nit, k + 2 nit, ... (the item functions stride by nitems) */
 				it.end = ntiles;
 				it.nitems = nit;
-				it.dep = phase == 0 ? 1 : build_counter;
-				it.dep_target = phase == 0 ? -2 : build_items;
+				it.dep = dep;
+				it.dep_target = dep_target;
 				it.done = counter;
 				it.finish = (!is_build && p.sink.kind != Sink::AggHash) ? (int)qi : -1;
-				phases[phase].push_back(it);
-			}
-			if (is_build) {
-				build_items += nit;
+				phase_list(phase).push_back(it);
 			}
 			if (p.sink.kind == Sink::AggHash) {
 				const int sid2 = add_shape(extract_src, "_extract");
@@ -1298,7 +1516,7 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 					it.dep_target = nit;
 					it.done = counter2;
 					it.finish = (int)qi;
-					phases[std::min(phase + 1, 2)].push_back(it);
+					phase_list(phase + 1).push_back(it);
 				}
 			}
 		}
@@ -1336,7 +1554,7 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 	src << "extern \"C\" __global__ void __launch_bounds__(" << threads << ", " << min_blocks
 		<< ") vc_batch(const VcBatchItem* __restrict__ items, "
 		"long long nwork, unsigned long long* counters, const unsigned long long* __restrict__ pool, "
-		"unsigned long long* finish_ns, int nq, unsigned* err) {\n";
+		"unsigned long long* finish_ns, int nq, unsigned* err, unsigned long long wait_ns) {\n";
 	src << "  __shared__ long long s_w;\n  __shared__ int s_ok;\n";
 	src << "  if (threadIdx.x == 0) { atomicCAS(&finish_ns[nq], 0ull, (unsigned long long)vd::globaltimer_ns()); }\n";
 	src << "  for (;;) {\n";
@@ -1351,7 +1569,7 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 	src << "        uint64_t t0 = 0;\n";
 	src << "        for (unsigned spin = 0; *(volatile unsigned long long*)&counters[it.dep] < (unsigned long long)it.dep_target; spin++) {\n";
 	src << "          if (spin == 0) { t0 = vd::globaltimer_ns(); }\n";
-	src << "          else if ((spin & 255u) == 0 && vd::globaltimer_ns() - t0 > 2000000000ull) { ok = 0; break; }\n";
+	src << "          else if ((spin & 255u) == 0 && vd::globaltimer_ns() - t0 > wait_ns) { ok = 0; break; }\n";
 	src << "          __nanosleep(100);\n";
 	src << "        }\n";
 	src << "        __threadfence();\n";

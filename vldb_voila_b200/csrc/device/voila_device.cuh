@@ -674,6 +674,106 @@ __device__ __forceinline__ int64_t group_find_or_insert(unsigned long long* __re
 	return -1;
 }
 
+/*
+ * Split group table: the stored keys (packed group key + 1, 0 = empty) in an array of their
+ * own, grouped into 32-byte buckets (8 keys of 32 bits or 4 of 64 bits), and the groups'
+ * accumulator words in a second array, W 64-bit words per slot.  A probe reads one key sector
+ * per bucket; only the group's own slot is touched in the accumulator array.  Several
+ * aggregates share one word where their (lower-bound biased, non-negative) sums cannot carry
+ * into each other, so one atomic updates them all.
+ *
+ * Returns the slot of `key` (inserting it into the first free slot of its probe sequence) or
+ * -1 when VD_MAX_PROBES buckets hold other keys.  Keys are read from L2 (other CTAs insert
+ * concurrently); a slot, once claimed, never changes, and the slots of a bucket fill in
+ * order, so a key absent from the occupied prefix of a bucket can only be claimed at or past
+ * its first free slot.
+ */
+template <typename K>
+__device__ __forceinline__ int64_t gt_find_or_insert(K* __restrict__ keys, uint64_t bmask, uint64_t h, K key,
+	unsigned* err)
+{
+	constexpr int KPB = 32 / (int)sizeof(K);
+	uint64_t b = h & bmask;
+	for (int probe = 0; probe < VD_MAX_PROBES; probe++) {
+		K* bk = keys + b * KPB;
+		K k[KPB];
+		const uint4 lo = __ldcg(reinterpret_cast<const uint4*>(bk));
+		const uint4 hi = __ldcg(reinterpret_cast<const uint4*>(bk) + 1);
+		reinterpret_cast<uint4*>(k)[0] = lo;
+		reinterpret_cast<uint4*>(k)[1] = hi;
+#pragma unroll
+		for (int i = 0; i < KPB; i++) {
+			if (k[i] == key) {
+				return (int64_t)(b * KPB + i);
+			}
+		}
+#pragma unroll
+		for (int i = 0; i < KPB; i++) {
+			if (k[i] == 0) {
+				K prev;
+				if constexpr (sizeof(K) == 4) {
+					prev = (K)atomicCAS((unsigned int*)&bk[i], 0u, (unsigned int)key);
+				} else {
+					prev = (K)atomicCAS((unsigned long long*)&bk[i], 0ull, (unsigned long long)key);
+				}
+				if (prev == 0 || prev == key) {
+					return (int64_t)(b * KPB + i);
+				}
+			}
+		}
+		b = (b + 1) & bmask;
+	}
+	atomicOr(err, VD_ERR_TABLE_FULL);
+	return -1;
+}
+
+/* adds W packed accumulator words into a slot of the split group table */
+template <int W>
+__device__ __forceinline__ void gt_add(unsigned long long* __restrict__ acc, int64_t slot, const uint64_t (&w)[W])
+{
+	unsigned long long* row = acc + (uint64_t)slot * W;
+#pragma unroll
+	for (int i = 0; i < W; i++) {
+		if (w[i]) {
+			atomicAdd(row + i, (unsigned long long)w[i]);
+		}
+	}
+}
+
+/* Per-CTA shared-memory cache of S (power of two) slots in the split layout (keys, then
+ * S * W words).  Returns false when the key finds no slot within 8 probes; the caller then
+ * updates the global table.  Flushed into the global table at the end of the CTA's work. */
+template <typename K, int W>
+__device__ __forceinline__ bool gt_cache_add(K* ckeys, unsigned long long* cacc, int S, uint64_t h, K key,
+	const uint64_t (&w)[W])
+{
+	uint64_t i = h & (uint64_t)(S - 1);
+	for (int probe = 0; probe < 8; probe++) {
+		K cur = *(volatile K*)&ckeys[i];
+		if (cur == 0) {
+			if constexpr (sizeof(K) == 4) {
+				cur = (K)atomicCAS((unsigned int*)&ckeys[i], 0u, (unsigned int)key);
+			} else {
+				cur = (K)atomicCAS((unsigned long long*)&ckeys[i], 0ull, (unsigned long long)key);
+			}
+			if (cur == 0) {
+				cur = key;
+			}
+		}
+		if (cur == key) {
+#pragma unroll
+			for (int a = 0; a < W; a++) {
+				if (w[a]) {
+					atomicAdd(cacc + i * W + a, (unsigned long long)w[a]);
+				}
+			}
+			return true;
+		}
+		i = (i + 1) & (uint64_t)(S - 1);
+	}
+	return false;
+}
+
 /* adds the A values of one group (key already packed and +1) into the global group table */
 template <int A>
 __device__ __forceinline__ void group_add(unsigned long long* __restrict__ table, uint64_t mask, uint64_t h,

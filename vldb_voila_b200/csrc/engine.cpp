@@ -54,6 +54,12 @@ std::string Flavor::str() const
 	if (sink_smem != 96 * 1024) {
 		o << ",sinksmem=" << sink_smem;
 	}
+	if (group_slots) {
+		o << ",gcap=" << group_slots;
+	}
+	if (out_rows) {
+		o << ",ocap=" << out_rows;
+	}
 	o << ")";
 	return o.str();
 }
@@ -116,6 +122,10 @@ Flavor Flavor::parse(const std::string& s0)
 			f.grid = num(0, 64);
 		} else if (k == "dense") {
 			f.dense_limit = num(1, 1 << 22);
+		} else if (k == "ocap") {
+			f.out_rows = num(0, 1 << 30);
+		} else if (k == "gcap") {
+			f.group_slots = num(0, 1 << 30);
 		} else if (k == "sinksmem") {
 			f.sink_smem = num(0, 96 * 1024);
 		} else if (k == "graph") {
@@ -263,7 +273,11 @@ void query_prepare(Query& q)
 		if (bm == "dense" && dense_bytes == 0) {
 			throw Error(VC_ERR_UNSUPPORTED, "build=dense needs a join key space of at most 2^30 values");
 		}
-		jd.dense = dense_bytes > 0 &&
+		/* a dense table holds one entry per key: JoinN (duplicate build keys) needs the hash table */
+		if (bm == "dense" && !jd.join01) {
+			throw Error(VC_ERR_UNSUPPORTED, "build=dense cannot hold the duplicate keys of a joinN build");
+		}
+		jd.dense = jd.join01 && dense_bytes > 0 &&
 			(bm == "dense" || (bm == "auto" && dense_bytes <= std::max<size_t>(jd.table_bytes, 1 << 20)));
 		if (jd.dense) {
 			jd.table_bytes = dense_bytes;
@@ -299,9 +313,16 @@ void query_prepare(Query& q)
 			ps.sink_bytes = (size_t)p.sink.domain * A * 8;
 			break;
 		case Sink::AggHash:
-			ps.sink_cap = std::max<int64_t>(
-				pow2_at_least((std::max<int64_t>(p.sink.groups_bound, 1) * 100 + q.flavor.fill - 1) / q.flavor.fill), 1024);
-			ps.sink_bytes = (size_t)ps.sink_cap * (1 + A) * 8;
+			/* a user-set capacity (gcap) is taken as given: too small a table fails the run
+			 * with VC_ERR_CAPACITY (bounded probe sequences), it never returns wrong rows */
+			ps.sink_cap = q.flavor.group_slots > 0 ? pow2_at_least(q.flavor.group_slots)
+				: std::max<int64_t>(pow2_at_least((std::max<int64_t>(p.sink.groups_bound, 1) * 100 + q.flavor.fill - 1) /
+					q.flavor.fill), 1024);
+			/* split layout: the keys (4 or 8 bytes per slot) in 32-byte buckets, then the
+			 * packed accumulator words */
+			ps.sink_bytes = (size_t)ps.sink_cap * (p.sink.key_bits <= 31 ? 4 : 8);
+			ps.sink_bytes = (ps.sink_bytes + 255) & ~(size_t)255;
+			ps.sink_bytes += (size_t)ps.sink_cap * p.sink.nwords * 8;
 			break;
 		case Sink::Emit:
 			break;
@@ -310,15 +331,36 @@ void query_prepare(Query& q)
 			ps.sink_dev = ps.sink_bytes <= (64 << 10) ? arena_take(ps.sink_bytes) : nullptr;
 			if (!ps.sink_dev) {
 				ps.sink_dev = dev_alloc(q, ps.sink_bytes);
-				st.memsets.push_back({ps.sink_dev, ps.sink_bytes});
+				if (p.sink.kind == Sink::AggHash && !e.offline) {
+					/* the group extraction zeroes every slot it reads, so the table is left
+					 * clear for the next run: it is cleared once here, not on every run
+					 * (batches, which may skip items, still clear it per run) */
+					ps.self_cleaning = true;
+					VC_CHECK_CUDA(cudaMemset(ps.sink_dev, 0, ps.sink_bytes));
+					st.clean_memsets.push_back({ps.sink_dev, ps.sink_bytes});
+				} else {
+					st.memsets.push_back({ps.sink_dev, ps.sink_bytes});
+				}
 			}
+		}
+		if (p.sink.kind == Sink::AggHash) {
+			const size_t kb = (((size_t)ps.sink_cap * (p.sink.key_bits <= 31 ? 4 : 8)) + 255) & ~(size_t)255;
+			ps.sink_acc = (char*)ps.sink_dev + kb;
 		}
 	}
 	st.memsets.insert(st.memsets.begin(), {arena, arena_used});
 	switch (rp.sink.kind) {
 	case Sink::AggGlobal: q.out_cap = 1; break;
 	case Sink::AggDense: q.out_cap = (int64_t)rp.sink.domain; break;
-	default: q.out_cap = std::max<int64_t>(rp.sink.groups_bound, 1); break;
+	default:
+		q.out_cap = std::max<int64_t>(rp.sink.groups_bound, 1);
+		if (rp.sink.kind == Sink::Emit) {
+			/* joinN can multiply rows up to probe rows x build rows: the buffer is bounded, and a
+			 * result beyond it fails the run with VC_ERR_CAPACITY (raise it with ocap=) */
+			const int64_t cap = q.flavor.out_rows > 0 ? q.flavor.out_rows : 4 * rp.rows + (1 << 20);
+			q.out_cap = std::max<int64_t>(std::min(q.out_cap, cap), 1);
+		}
+		break;
 	}
 	q.out = (int64_t*)dev_alloc(q, (size_t)q.out_cap * plan.result_cols * 8);
 
@@ -458,6 +500,12 @@ void query_launch(Query& q, cudaStream_t stream)
 	refresh_column_params(q);
 	q.stream = stream;
 	q.result_rows = -1;
+	if (q.dirty) {
+		for (auto& m : state_of(q).clean_memsets) {
+			VC_CHECK_CUDA(cudaMemsetAsync(m.first, 0, m.second, stream));
+		}
+		q.dirty = false;
+	}
 	if (q.flavor.graph) {
 		if (q.graph && q.graph_profiled != q.profile) {
 			/* profiling events are nodes of the graph: re-capture when profiling toggles */
@@ -513,6 +561,9 @@ void query_fetch(Query& q)
 	unsigned long long cnt = 0;
 	VC_CHECK_CUDA(cudaMemcpy(&err, q.err, sizeof(err), cudaMemcpyDeviceToHost));
 	VC_CHECK_CUDA(cudaMemcpy(&cnt, q.out_count, sizeof(cnt), cudaMemcpyDeviceToHost));
+	if (err) {
+		q.dirty = true; /* a failed run may leave its tables set */
+	}
 	if (err & 1u) {
 		throw Error(3, "a device hash table ran out of slots");
 	}
@@ -612,6 +663,7 @@ void query_mark_external_run(Query& q, cudaStream_t s)
 	q.ran = true;
 	q.result_rows = -1;
 	q.profile = false;
+	q.dirty = false; /* the batch clears every table of the query before using it */
 }
 } // namespace vc
 

@@ -157,6 +157,11 @@ struct Sink {
 	int key_bits = 0;
 	__int128 domain = 0;         /* product of key ranges */
 	int64_t groups_bound = 0;    /* upper bound of distinct groups */
+	/* packed accumulator words of a hash group table: aggregate a's sum of (value - lower
+	 * bound) -- the count for a count -- is the bit field [agg_shift[a], agg_shift[a] +
+	 * agg_bits[a]) of word agg_word[a]; the bounds keep every field from carrying over */
+	std::vector<int> agg_word, agg_shift, agg_bits;
+	int nwords = 0;
 };
 
 struct PipeColumn {
@@ -198,6 +203,9 @@ struct Flavor {
 	int fill = 50;            /* largest load factor (percent) of group tables */
 	int64_t direct_limit = 64ll << 20; /* auto: direct when the upper-bound table fits this many bytes */
 	int sink_smem = 96 * 1024; /* most shared memory a dense aggregation keeps its slots in (else global) */
+	int64_t group_slots = 0;  /* hash group table slots (0 = sized from the groups bound and fill) */
+	int64_t out_rows = 0;     /* result row capacity of an emitting pipeline (0 = from its bound, at
+	                           * most 4 rows per input row + 2^20 when joinN probes multiply rows) */
 
 	std::string str() const;
 	static Flavor parse(const std::string& s);
@@ -237,6 +245,8 @@ struct PipeDeviceState {
 	void* sink_dev = nullptr;            /* aggregation state (global sums, dense slots, group table) */
 	int64_t sink_cap = 0;
 	size_t sink_bytes = 0;
+	void* sink_acc = nullptr;            /* hash group table: accumulator words (sink_dev holds the keys) */
+	bool self_cleaning = false;          /* the pipeline's last kernel leaves sink_dev zeroed */
 	void* stage_hash = nullptr;          /* staged join build: materialised hashes */
 	unsigned long long* done = nullptr;  /* last-block counter */
 };
@@ -295,6 +305,7 @@ struct Query {
 	bool graph_profiled = false;         /* the graph records the profiling events */
 	cudaStream_t graph_stream = nullptr;
 	bool ran = false;
+	bool dirty = false;                  /* self-cleaning state may be left set: clear before the next run */
 	int64_t result_rows = -1;
 	std::vector<int64_t> result_host;    /* column-major copy of the last result */
 	~Query();
@@ -306,6 +317,9 @@ struct QueryState {
 	std::vector<cudaKernel_t> kernels;
 	std::vector<int> occupancy;
 	std::vector<std::pair<void*, size_t>> memsets;
+	/* state a run leaves clear by itself (self-cleaning group tables): cleared once, and again
+	 * only before a run that follows a failed one; batches clear it on every run */
+	std::vector<std::pair<void*, size_t>> clean_memsets;
 };
 
 QueryState& state_of(Query& q);
@@ -347,6 +361,9 @@ struct Batch {
 	cudaGraphExec_t graph = nullptr;
 	cudaStream_t stream = nullptr;
 	int grid = 0;
+	unsigned long long wait_ns = 2000000000ull; /* longest wait of an item on its dependency */
+	std::vector<BatchItem> held;               /* original items replaced by vc_batch_hold_item */
+	std::vector<int64_t> held_index;
 	~Batch();
 };
 

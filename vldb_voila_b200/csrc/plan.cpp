@@ -543,6 +543,7 @@ struct Lowerer {
 					throw Error(kErrUnsupported, "group key domain needs more than 62 bits");
 				}
 				sink.kind = Sink::AggHash;
+				pack_aggregates(sink, rows);
 			}
 		}
 		p.sink = sink;
@@ -552,6 +553,40 @@ struct Lowerer {
 			vis += a.visible ? 1 : 0;
 		}
 		out.result_cols = vis;
+	}
+
+	/* First-fit-decreasing packing of the aggregates' bit fields into 64-bit words: the
+	 * field of a sum holds sum(value - lo) <= (hi - lo) * rows, a count's holds <= rows. */
+	static void pack_aggregates(Sink& sink, int64_t rows) {
+		const size_t A = sink.aggs.size();
+		sink.agg_word.assign(A, 0);
+		sink.agg_shift.assign(A, 0);
+		sink.agg_bits.assign(A, 0);
+		for (size_t a = 0; a < A; a++) {
+			const __int128 r = std::max<int64_t>(rows, 1);
+			const __int128 bound = sink.aggs[a].count ? r : (sink.aggs[a].arg->b.hi - sink.aggs[a].arg->b.lo) * r;
+			sink.agg_bits[a] = std::max(1, bits_for(bound + 1));
+		}
+		std::vector<size_t> order(A);
+		for (size_t a = 0; a < A; a++) {
+			order[a] = a;
+		}
+		std::stable_sort(order.begin(), order.end(),
+			[&](size_t x, size_t y) { return sink.agg_bits[x] > sink.agg_bits[y]; });
+		std::vector<int> used;
+		for (size_t a : order) {
+			size_t w = 0;
+			while (w < used.size() && used[w] + sink.agg_bits[a] > 64) {
+				w++;
+			}
+			if (w == used.size()) {
+				used.push_back(0);
+			}
+			sink.agg_word[a] = (int)w;
+			sink.agg_shift[a] = used[w];
+			used[w] += sink.agg_bits[a];
+		}
+		sink.nwords = (int)used.size();
 	}
 
 	void root(const RelOpP& op) {

@@ -93,7 +93,10 @@ def lib():
         "vc_batch_source": (c.c_int, [P, P, c.c_size_t, c.POINTER(c.c_size_t)]),
         "vc_batch_items": (c.c_int, [P, P, c.c_int64, c.POINTER(c.c_int64)]),
         "vc_batch_free": (c.c_int, [P]),
+        "vc_batch_set_wait_limit": (c.c_int, [P, c.c_uint64]),
+        "vc_batch_hold_item": (c.c_int, [P, c.c_int64, c.c_int]),
         "vc_query_timings": (c.c_int, [P, c.POINTER(c.c_float), c.c_int, c.POINTER(c.c_int), P, c.c_size_t]),
+        "vc_stream_read": (c.c_int, [P, c.c_int64, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)
@@ -196,6 +199,11 @@ def workload(spec):
 
 def batch_specs(count, seed, min_rows=10_000, max_rows=60_000_000):
     return _text_call(lib().vc_workload_batch, count, seed, min_rows, max_rows).split()
+
+
+def stream_read(device_ptr, nbytes, device_out, stream=None):
+    """One plain streaming read of nbytes at device_ptr (the bandwidth floor of a scan)."""
+    check(lib().vc_stream_read(ctypes.c_void_p(device_ptr), nbytes, ctypes.c_void_p(device_out), _stream_ptr(stream)))
 
 
 def zipf_cdf(s, n):
@@ -417,6 +425,14 @@ class Batch:
 
     def wait(self):
         check(lib().vc_batch_wait(self._h))
+
+    def set_wait_limit(self, ns):
+        """Longest wait (ns) of a work item on its dependency before the batch gives up."""
+        check(lib().vc_batch_set_wait_limit(self._h, int(ns)))
+
+    def hold_item(self, index, hold=True):
+        """Test hook: work item `index` waits for a dependency that never completes."""
+        check(lib().vc_batch_hold_item(self._h, int(index), 1 if hold else 0))
 
     def latencies_us(self):
         out = (ctypes.c_double * len(self.queries))()

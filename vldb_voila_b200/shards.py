@@ -11,10 +11,21 @@ hash-partitioned so every rank merges a disjoint key range; global partials are 
 import numpy as np
 
 
+EMIT = -1
+
+
 def plan_group_keys(plan):
-    """Number of group keys of the plan's root aggregation (0 for a global aggregate)."""
+    """Number of group keys of the plan's root aggregation: 0 for a global aggregate, EMIT for
+    a plan whose root emits rows (no aggregation; the ranks' rows are disjoint and their union
+    is the result).  Raises ValueError for text that is not a plan."""
     tokens = plan.replace("(", " ( ").replace(")", " ) ").split()
-    if len(tokens) < 4 or tokens[1] != "aggr" or tokens[2] != "hash":
+    if len(tokens) < 2 or tokens[0] != "(":
+        raise ValueError("not a plan: " + plan[:40])
+    if tokens[1] != "aggr":
+        return EMIT
+    if len(tokens) < 4 or tokens[2] not in ("hash", "global"):
+        raise ValueError("malformed aggregation at the plan root")
+    if tokens[2] == "global":
         return 0
     depth, n, i = 0, 0, 3
     while i < len(tokens):  # count the top-level items of the key list
@@ -29,6 +40,18 @@ def plan_group_keys(plan):
                 break
         i += 1
     return n
+
+
+def load_shard(engine, w, data, rank, world):
+    """Declares the workload's tables on `engine` with this rank's row range of the fact table
+    (the other tables replicated) and uploads them from host arrays ({table: {col: array}})."""
+    b, e = shard_rows(w.fact_rows, rank, world)
+    for t, rows in w.tables.items():
+        engine.create_table(t, (e - b) if t == w.fact_table else rows)
+    for c in w.columns:
+        engine.add_column(c.table, c.name, c.type, c.lo, c.hi)
+        a = data[c.table][c.name]
+        engine.upload(c.table, c.name, a[b:e] if c.table == w.fact_table else a)
 
 
 def shard_rows(n, rank, world):
@@ -77,22 +100,34 @@ def _all_gather_rows(rows, ncols, group, device):
     return [o[:int(s.item())].cpu().numpy() for o, s in zip(outs, sizes)]
 
 
-def merge_partials(rows, nkeys, ncols, group=None, device="cpu"):
-    """Merges this rank's partial result rows (keys then aggregates, int64) with the other
-    ranks'.  Returns this rank's share of the merged rows: a disjoint key partition for
-    grouped results; for a global aggregate (nkeys == 0) rank 0 gets the single row (if any
-    rank had one) and the others get none."""
-    import torch.distributed as dist
-    rows = np.asarray(rows, dtype=np.int64).reshape(-1, ncols)
-    rank, world = dist.get_rank(group), dist.get_world_size(group)
-    parts = _all_gather_rows(rows, ncols, group, device)
-    allrows = np.concatenate(parts, axis=0) if parts else rows[:0]
+def merge_rows(allrows, nkeys, rank, world):
+    """This rank's share of the merged result, given every rank's partial rows (keys then
+    aggregates): a disjoint key partition, summed per key, for grouped results; the single
+    summed row on rank 0 for a global aggregate (none on the others, and none at all when no
+    rank had a row: an aggregate over zero matches emits nothing)."""
+    allrows = np.asarray(allrows, dtype=np.int64)
+    if nkeys == EMIT:
+        raise ValueError("emit plans are not merged: each rank's rows are its share")
     if nkeys == 0:
         if rank != 0 or len(allrows) == 0:
             return allrows[:0]
         return allrows.sum(axis=0, keepdims=True).astype(np.int64)
     mine = allrows[_key_partition(allrows[:, :nkeys], world) == rank]
     return _merge_local(mine, nkeys)
+
+
+def merge_partials(rows, nkeys, ncols, group=None, device="cpu"):
+    """Merges this rank's partial result rows (keys then aggregates, int64) with the other
+    ranks' (an all-gather, then merge_rows).  For an emit plan (nkeys == EMIT) there is nothing
+    to merge: the rank's own rows are its share of the union."""
+    import torch.distributed as dist
+    rows = np.asarray(rows, dtype=np.int64).reshape(-1, ncols)
+    if nkeys == EMIT:
+        return rows
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    parts = _all_gather_rows(rows, ncols, group, device)
+    allrows = np.concatenate(parts, axis=0) if parts else rows[:0]
+    return merge_rows(allrows, nkeys, rank, world)
 
 
 def gather_result(rows, ncols, group=None, device="cpu"):

@@ -116,6 +116,11 @@ int vc_gen_zipf_cdf(double s, int64_t n, double* out);
  * their domains and the plan text.  Writes at most `cap` bytes; *len gets the full length. */
 int vc_workload_describe(const char* spec, char* buf, size_t cap, size_t* len);
 
+/* The base-table columns a plan scans, one "table column" line each, in the order the plan
+ * names them: what a host uploads before vc_query_new (the reference binds the same
+ * attributes when it sets up a generated query, runtime_struct.cpp:825-842). */
+int vc_plan_columns(const char* plan, char* buf, size_t cap, size_t* len);
+
 /* Spec strings of the seeded mixed batch (one per line). */
 int vc_workload_batch(int count, uint64_t seed, int64_t min_rows, int64_t max_rows, char* buf, size_t cap,
 	size_t* len);
@@ -129,7 +134,8 @@ int vc_workload_batch(int count, uint64_t seed, int64_t min_rows, int64_t max_ro
  * flavor: "" or "cuda(key=value,...)" with keys threads, rows, load=ldg|tma, stages,
  * prefetch, compact, aggr=auto|dense|global|cache, cache, lowcard=combine|atomic|private|redux,
  * build=auto|direct|staged|dense, hash=mix|voila, fill, dense, sinksmem, gcap (group table
- * slots), ocap (result rows of an emitting plan), grid, graph.
+ * slots), ocap (result rows of an emitting plan), probe (1..32 lanes that probe one join key
+ * together), grid, graph.
  * VC_ERR_INVALID for an unknown or out-of-range knob; VC_ERR_UNSUPPORTED when the flavor's
  * shared memory exceeds the device's per-CTA limit or build=dense meets a large key space. */
 int vc_query_new(vc_engine* eng, const char* plan, const char* flavor, vc_query** out);
@@ -159,6 +165,12 @@ int vc_query_result_text(vc_query* q, char* buf, size_t cap, size_t* len);
 
 /* JSON description: pipelines, kernels, flavor, algorithmic bytes, generated source size. */
 int vc_query_info(vc_query* q, char* buf, size_t cap, size_t* len);
+
+/* Lowers plan text with a flavor (no code generation, no compilation) and describes its
+ * pipelines as JSON: table, rows, columns, filters, probes (joinN among them), rows of the
+ * probed builds, sink kind, aggregates, key domain, groups bound, scanned bytes.  The
+ * features the flavor chooser works from. */
+int vc_plan_describe(vc_engine* eng, const char* plan, const char* flavor, char* buf, size_t cap, size_t* len);
 
 /* Generated CUDA source of the query (for inspection and tests). */
 int vc_query_source(vc_query* q, char* buf, size_t cap, size_t* len);

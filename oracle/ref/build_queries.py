@@ -4,10 +4,16 @@ For each workload in WORKLOADS and each reference flavor (hyper, vectorwise), ru
 reference's own code generator through ref_gen (oracle/ref/ref_gen.cpp) and stores
 oracle/_ref/<isa>/q_<name>_<flavor>.so.  Generated code depends only on the plan and the
 columns' declared min/max, so the libraries run on any table size of the same spec shape.
+
+It also builds the CUDA flavor's generated libraries (ref_gen --flavor cuda: the plan through
+the reference's relalg tree into the glue of cuda_glue.inc over libvoila_cuda.so) for the
+same workloads and for every golden case, q_<name>_cuda.so and q_golden_<case>_cuda.so, which
+ref_run drives through the reference's voila_query_* ABI in the GPU tests.
 Needs the reference tree (build host only); the results travel with the repository.
 
     python oracle/ref/build_queries.py [--isa avx512|avx2]
 """
+import json
 import os
 import subprocess
 import sys
@@ -22,6 +28,15 @@ WORKLOADS = {
     "groupby": "groupby:rows=6000000,keys=1500000,zipf=1.25,seed=3",
     "star": "star:rows=60000000,seed=4",
 }
+
+
+def _cuda_libs():
+    """(library name, workload spec, plan or None) of the CUDA-flavor glue libraries."""
+    out = [(f"q_{name}_cuda", spec, None) for name, spec in WORKLOADS.items()]
+    with open(os.path.join(REPO, "tests", "golden", "manifest.json")) as f:
+        for case, entry in sorted(json.load(f).items()):
+            out.append((f"q_golden_{case}_cuda", entry["spec"], entry["plan"]))
+    return out
 
 
 def build(isa="avx512", flavors=("hyper", "vectorwise")):
@@ -41,6 +56,24 @@ def build(isa="avx512", flavors=("hyper", "vectorwise")):
             if r.returncode != 0:
                 raise RuntimeError(f"ref_gen failed for {name}/{fl}: {r.stderr[-2000:]}")
             out.append(lib)
+    glue_deps = [os.path.join(rdir, "ref_gen"), os.path.join(HERE, "cuda_glue.inc"),
+                 os.path.join(REPO, "include", "voila_cuda.h")]
+    stamp = max(os.path.getmtime(d) for d in glue_deps)
+    link = ("-L" + os.path.join(REPO, "vldb_voila_b200") + " -lvoila_cuda"
+            " -Wl,-rpath,'$ORIGIN/../../../vldb_voila_b200'")
+    for name, spec, plan in _cuda_libs():
+        lib = os.path.join(rdir, name + ".so")
+        if os.path.exists(lib) and os.path.getmtime(lib) > stamp:
+            out.append(lib)
+            continue
+        cmd = [os.path.join(rdir, "ref_gen"), "--workload", spec, "--flavor", "cuda", "--out", lib,
+               "--cxx", cxx + f" -I{HERE} -I{REPO}/include", "--link", link]
+        if plan:
+            cmd += ["--plan", plan]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_gen failed for {name}: {r.stderr[-2000:]}")
+        out.append(lib)
     return out
 
 

@@ -9,8 +9,13 @@
  * independent of the table sizes: code generation only reads each column's declared
  * min/max (codegen.cpp:11-19).
  *
- * usage: ref_gen --workload SPEC --flavor hyper|vectorwise --out LIB.so --cxx "g++ ..."
- *                [--plan PLAN-TEXT] [--keep-src FILE]
+ * usage: ref_gen --workload SPEC --flavor hyper|vectorwise|cuda --out LIB.so --cxx "g++ ..."
+ *                [--plan PLAN-TEXT] [--keep-src FILE] [--link "LDFLAGS"] [--cuda-flavor "cuda(...)"]
+ *
+ * --flavor cuda plays the part of a Flavor::Cuda case in Compiler::_generate: the plan goes
+ * through the reference's relalg tree, is printed back as plan text (cuda_flavor.hpp) and
+ * becomes the generated library's constant; the library is the fixed glue (cuda_glue.inc)
+ * over libvoila_cuda.so, linked with --link.
  */
 #include <cstdio>
 #include <cstdlib>
@@ -21,12 +26,13 @@
 
 #include "common/runtime/Database.hpp"
 #include "compiler.hpp"
+#include "cuda_flavor.hpp"
 #include "ref_plans.hpp"
 #include "runtime_framework.hpp"
 
 int main(int argc, char** argv)
 {
-	std::string spec, flavor = "hyper", out, cxx, plan, keep_src;
+	std::string spec, flavor = "hyper", out, cxx, plan, keep_src, link, cuda_flavor;
 	for (int i = 1; i + 1 < argc; i += 2) {
 		std::string k = argv[i];
 		if (k == "--workload") spec = argv[i + 1];
@@ -35,6 +41,8 @@ int main(int argc, char** argv)
 		else if (k == "--cxx") cxx = argv[i + 1];
 		else if (k == "--plan") plan = argv[i + 1];
 		else if (k == "--keep-src") keep_src = argv[i + 1];
+		else if (k == "--link") link = argv[i + 1];
+		else if (k == "--cuda-flavor") cuda_flavor = argv[i + 1];
 		else {
 			std::cerr << "ref_gen: unknown option " << k << std::endl;
 			return 2;
@@ -48,6 +56,28 @@ int main(int argc, char** argv)
 		auto w = vc_workload::make(spec);
 		if (!plan.empty()) {
 			w.plan = plan;
+		}
+		if (flavor == "cuda") {
+			auto root = ref_harness::to_ref_op(vc_sexpr::parse(w.plan));
+			const std::string src_name = out + ".glue.cpp";
+			{
+				std::ofstream f(src_name);
+				f << voila_cuda_flavor::glue_source(voila_cuda_flavor::plan_text(*root), cuda_flavor);
+			}
+			std::ostringstream cmd;
+			cmd << cxx << " -shared -fPIC " << src_name << " -o " << out << " " << link;
+			const int rc = std::system(cmd.str().c_str());
+			if (!keep_src.empty()) {
+				std::ifstream in(src_name);
+				std::ofstream o(keep_src);
+				o << in.rdbuf();
+			}
+			std::remove(src_name.c_str());
+			if (rc != 0) {
+				std::cerr << "ref_gen: compiler failed: " << cmd.str() << std::endl;
+				return 1;
+			}
+			return 0;
 		}
 		runtime::Database db;
 		ref_harness::load_workload(db, w, 64, 1);

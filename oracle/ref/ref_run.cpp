@@ -3,7 +3,7 @@
  * on a synthetic workload, the way Compiler::_run does (compiler.cpp:465-598): dlopen, dlsym
  * of the voila_query_* ABI, qnew, then per hot repetition qreset + a timed qrun.
  *
- * usage: ref_run --workload SPEC --lib LIB.so --flavor hyper|vectorwise
+ * usage: ref_run --workload SPEC --lib LIB.so --flavor hyper|vectorwise|cuda
  *                [--threads N] [--reps R] [--result FILE] [--no-result 1] [--checksum 1]
  *                [--max-rows N] [--vector-size N] [--morsel-size N]
  *
@@ -67,7 +67,8 @@ int main(int argc, char** argv)
 		qconf.vector_size = vector_size;
 		qconf.morsel_size = morsel_size;
 		qconf.print_result = !no_result;
-		qconf.flavor = flavor == "hyper" ? QueryConfig::Flavor::Hyper : QueryConfig::Flavor::Vectorwise;
+		/* a CUDA-flavor library ignores the flavor field (the reference has no Flavor::Cuda) */
+		qconf.flavor = flavor == "vectorwise" ? QueryConfig::Flavor::Vectorwise : QueryConfig::Flavor::Hyper;
 
 		void* h = dlopen(lib.c_str(), RTLD_NOW);
 		if (!h) {

@@ -63,3 +63,28 @@ def test_batch_specs_are_seeded():
     a = E.batch_specs(16, 5)
     assert a == E.batch_specs(16, 5) and a != E.batch_specs(16, 6)
     assert {s.split(":")[0] for s in a} <= {"sel_aggr", "join_aggr", "groupby"}
+
+
+def test_reference_side_glue_library_exports_the_generated_query_abi():
+    """The CUDA flavor's generated library (oracle/ref/cuda_glue.inc, built for each golden
+    case by oracle/ref/build_queries.py) exports the reference's voila_query_* ABI and, driven
+    by the reference's runner on a host without a GPU, fails with the engine's message instead
+    of crashing."""
+    import os
+    import subprocess
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    rdir = os.path.join(repo, "oracle", "_ref", "avx512")
+    lib = os.path.join(rdir, "q_golden_join_n_cuda.so")
+    with open("/proc/cpuinfo") as f:
+        avx512 = "avx512f" in f.read()
+    if not os.path.exists(lib) or not avx512:
+        pytest.skip("the reference build in oracle/_ref is not available here")
+    syms = subprocess.run(["nm", "-D", "--defined-only", lib], capture_output=True, text=True).stdout
+    for s in ("voila_query_new", "voila_query_run", "voila_query_reset", "voila_query_free"):
+        assert f" T {s}" in syms
+    import torch
+    if torch.cuda.is_available():
+        return
+    r = subprocess.run([os.path.join(rdir, "ref_run"), "--workload", "star:rows=1000,custs=50", "--lib", lib,
+                        "--flavor", "cuda", "--reps", "1"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1 and "cuda flavor:" in r.stderr

@@ -9,7 +9,8 @@ SPECS = ["sel_aggr:rows=1000", "join_aggr:build=100,probe=1000", "groupby:rows=1
          "groupby:rows=1000,keys=50", "star:rows=1000"]
 FLAVORS = ["", "cuda(load=tma,stages=2)", "cuda(lowcard=private,prefetch=0)", "cuda(aggr=cache,build=staged)",
            "cuda(compact=0,rows=8,threads=128)", "cuda(hash=voila,compact=-1)", "cuda(build=direct,prefetch=0)",
-           "cuda(lowcard=redux,aggr=cache,cache=64)", "cuda(lowcard=atomic,sinksmem=4096)"]
+           "cuda(lowcard=redux,aggr=cache,cache=64)", "cuda(lowcard=atomic,sinksmem=4096)",
+           "cuda(build=direct,probe=8)"]
 
 
 def offline(spec):
@@ -28,6 +29,8 @@ def test_workload_plans_compile_for_sm100a(spec, flavor):
     src = q.source()
     assert any(k["dominant"] for k in info["kernels"])
     assert "vc_p0_main" in src
+    if "probe=" in flavor and w.template in ("join_aggr", "star"):
+        assert "__ballot_sync(cmask" in src  # warp-cooperative probing
     if w.template == "join_aggr":
         # small key spaces get a dense (direct-address) table unless a hash build is forced
         hashed = "build=staged" in flavor or "build=direct" in flavor
@@ -204,4 +207,36 @@ def test_join_n_rejects_dense_builds():
     w, e = offline("star:rows=1000,custs=50")
     with pytest.raises(VoilaError) as ex:
         e.query(JOIN_N_PLAN, "cuda(build=dense)")
+    assert ex.value.code == 6
+
+
+def test_sub_aggregation_lowers_to_an_intermediate_table():
+    """An aggregation below the root writes an intermediate table that the next pipeline scans
+    (row count read on the device); its columns carry the reference translator's names."""
+    from helpers import manifest
+    m = manifest()["agg_of_agg"]
+    w, e = offline(m["spec"])
+    q = e.query(m["plan"])
+    info = q.info()
+    assert [p["sink"] for p in info["pipelines"]] == ["aggr_dense", "aggr_hash"]
+    src = q.source()
+    assert "__ldcg(((const unsigned long long*)" in src  # the consumer's row count
+    # a join takes the translator's next id before its build side: below it, the first
+    # aggregation's table is aggr_ht2, and aggr_ht1 names nothing
+    plan = ("(aggr global () ((fun count)) (join join01 ((col X.key_0)) ()"
+            " (aggr hash ((col lineitem.l_orderkey)) ((fun count)) (scan lineitem (l_orderkey)))"
+            " ((col lineitem.l_orderkey)) () (scan lineitem (l_orderkey))))")
+    e.query(plan.replace("X", "aggr_ht2"))
+    with pytest.raises(VoilaError) as ex:
+        e.query(plan.replace("X", "aggr_ht1"))
+    assert ex.value.code == 1
+
+
+def test_sub_aggregations_are_not_batched_yet():
+    from helpers import manifest
+    from vldb_voila_b200.engine import Batch
+    m = manifest()["having_global"]
+    w, e = offline(m["spec"])
+    with pytest.raises(VoilaError) as ex:
+        Batch([e.query(m["plan"])])
     assert ex.value.code == 6

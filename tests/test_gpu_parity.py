@@ -16,7 +16,8 @@ FLAVORS = ["", "cuda(rows=8,threads=128,load=tma,stages=3)", "cuda(aggr=cache,ca
            "cuda(aggr=global,rows=1,threads=64,graph=0,prefetch=0,compact=-1)",
            "cuda(load=tma,build=staged,rows=2,lowcard=atomic)", "cuda(compact=0,lowcard=private,rows=8)",
            "cuda(hash=voila,lowcard=private,threads=128,fill=75)", "cuda(build=direct,prefetch=0)",
-           "cuda(lowcard=redux,aggr=cache,cache=64)"]
+           "cuda(lowcard=redux,aggr=cache,cache=64)", "cuda(build=direct,probe=4,rows=2)",
+           "cuda(build=staged,probe=32,compact=-1)"]
 
 
 def run_gpu(w, plan, flavor="", on_device=False, data=None):

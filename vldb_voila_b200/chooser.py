@@ -1,56 +1,128 @@
-"""Flavor selection for pipelines: the exhaustive autotuner and the learned chooser.
+"""Flavor selection for pipelines: the exhaustive autotuner, the explorer and the learned chooser.
 
 The reference explores its blend space by compiling and timing variants (explorer.cpp:111-134
-per-pipeline backtracking, :352-426 random sampling; runs logged to SQLite, compiler.cpp:91-256).
-Here:
+per-pipeline backtracking, :352-426 random sampling; domains explorer_helper.cpp:6-21; runs
+logged to the SQLite `runs` table, compiler.cpp:91-256).  Here:
 
-  * `autotune` is the exhaustive search: every candidate CUDA flavor of a pipeline is compiled
-    (NVRTC, cached by source) and timed on the GPU (device events, L2 flushed before every run);
-    results are appended to a JSONL log so a search can be resumed and reused as training data.
-  * `Chooser` is the learned part: a small MLP, trained and evaluated on the GPU by the library's
-    own kernels (csrc/mlp.cu), maps per-pipeline features (row count, predicate selectivity,
-    build size, key cardinality, Zipf skew, payload widths, operator counts) to the predicted
-    relative time of every candidate flavor and picks the argmin.  Results never depend on the
+  * the search space is a grid of CUDA-flavor knobs per pipeline kind (`GRIDS`): the kind of a
+    query's fact pipeline -- a scan with a small-domain aggregation, one join probe, a chain of
+    probes, a hash group-by -- decides which knobs can change its generated code, and the grid
+    is their full product;
+  * `autotune` is the exhaustive search over a kind's grid: every candidate is compiled
+    (NVRTC, cached by source) and timed on the GPU (device events, L2 flushed before every
+    run); candidates the device cannot run (shared memory) are skipped;
+  * `explore` is the reference explorer's counterpart: the full grid or a seeded random sample
+    of it, every run logged to a JSONL file and/or the reference's SQLite `runs` schema
+    (backend 'cuda', the flavor string as the blend);
+  * `Chooser` is the learned part: a small MLP, trained and evaluated on the GPU by the
+    library's own kernels (csrc/mlp.cu), maps a pipeline's features -- taken from the lowered
+    plan (vc_plan_describe: rows, probes, rows of the probed builds, key domain, groups bound,
+    aggregates, bytes per row, sink kind) plus the data statistics a caller knows (predicate
+    selectivity, Zipf skew) -- to the predicted relative time of every grid candidate, and
+    picks the argmin among the candidates of the query's kind.  Results never depend on the
     choice, only speed; the autotuner is its fallback and the yardstick of its choices.
 """
+import itertools
 import json
 import math
 import os
+import sqlite3
+import time
 
 import numpy as np
 
-from .engine import Engine, Mlp, workload
-
-# Candidate flavors (the computation_type=cuda(...) blends searched per pipeline).  Knobs
-# that do not apply to a pipeline leave its generated code unchanged.
-CANDIDATES = [
-    "cuda()",
-    "cuda(prefetch=0)",
-    "cuda(rows=2,prefetch=0)",
-    "cuda(rows=8,prefetch=0)",
-    "cuda(load=tma,stages=2)",
-    "cuda(lowcard=private)",
-    "cuda(lowcard=private,prefetch=0)",
-    "cuda(threads=128,lowcard=private,load=tma,stages=2)",
-    "cuda(aggr=cache,cache=128)",
-    "cuda(aggr=cache,cache=256,fill=75)",
-    "cuda(fill=75)",
-    "cuda(aggr=cache,cache=128,fill=75,prefetch=0)",
-    "cuda(build=staged,prefetch=0)",
-    "cuda(compact=-1,prefetch=0)",
-    "cuda(threads=128)",
-    "cuda(aggr=cache,cache=256,fill=75,prefetch=0)",
-    "cuda(aggr=cache,cache=2048,fill=75,prefetch=0,threads=512)",
-    "cuda(build=direct)",
-]
+from .engine import Engine, Mlp, VoilaError, workload
 
 DEFAULT = "cuda()"
 
-FEATURE_NAMES = ["log2_rows", "selectivity", "log2_build_rows", "log2_key_domain", "zipf", "bytes_per_row",
-                 "probes", "aggregates", "t_sel_aggr", "t_join_aggr", "t_groupby", "t_star"]
+
+def _load_modes():
+    # (load, prefetch, stages): vector loads with or without the next tile in flight, or the
+    # bulk-copy ring at two depths
+    return [("ldg", 1, None), ("ldg", 0, None), ("tma", None, 2), ("tma", None, 4)]
 
 
-def _params(spec):
+def _scan_grid():
+    out = []
+    for threads, rows, (load, pf, stages), lowcard in itertools.product(
+            (128, 256), (4, 8), _load_modes(), ("combine", "private", "redux")):
+        items = [f"threads={threads}", f"rows={rows}", f"load={load}", f"lowcard={lowcard}"]
+        items += [f"prefetch={pf}"] if pf is not None else [f"stages={stages}"]
+        out.append("cuda(" + ",".join(items) + ")")
+    return out
+
+
+def _hash_grid():
+    out = []
+    for threads, rows, pf, aggr, fill in itertools.product(
+            (256, 512), (2, 4), (0, 1), ("global", "cache,cache=256", "cache,cache=2048"), (50, 75)):
+        out.append(f"cuda(threads={threads},rows={rows},prefetch={pf},aggr={aggr},fill={fill})")
+    return out
+
+
+def _join_grid():
+    out = []
+    for threads, rows, pf, build in itertools.product((128, 256), (2, 4, 8), (0, 1), ("auto", "direct", "direct4")):
+        b = "build=direct,probe=4" if build == "direct4" else f"build={build}"
+        out.append(f"cuda(threads={threads},rows={rows},prefetch={pf},{b})")
+    return out
+
+
+def _star_grid():
+    out = []
+    for threads, rows, compact, pf, lowcard in itertools.product(
+            (128, 256), (4, 8), ("auto", -1), (0, 1), ("combine", "private")):
+        out.append(f"cuda(threads={threads},rows={rows},compact={compact},prefetch={pf},lowcard={lowcard})")
+    return out
+
+
+# the default flavor heads every grid: it is the chooser's "method without it"
+GRIDS = {k: [DEFAULT] + g() for k, g in
+         (("scan", _scan_grid), ("hash", _hash_grid), ("join", _join_grid), ("star", _star_grid))}
+KINDS = tuple(GRIDS)
+# every candidate of every kind (the chooser's outputs), the default first
+CANDIDATES = [DEFAULT] + sorted({c for g in GRIDS.values() for c in g} - {DEFAULT})
+
+FEATURE_NAMES = ["log2_rows", "log2_probed_build_rows", "log2_groups_bound", "log2_key_domain", "filters",
+                 "probes", "probes_n", "aggregates", "bytes_per_row", "selectivity", "zipf",
+                 "sink_global", "sink_dense", "sink_hash", "sink_emit"] + [f"kind_{k}" for k in KINDS]
+
+
+def fact_pipeline(desc):
+    """The pipeline that produces the query's result (the fact pipeline)."""
+    pipes = desc["pipelines"]
+    return next((p for p in pipes if p["result"]), max(pipes, key=lambda p: p["rows"]))
+
+
+def kind_of(desc):
+    """Pipeline kind of a lowered plan (see GRIDS)."""
+    p = fact_pipeline(desc)
+    if p["probes"] >= 2:
+        return "star"
+    if p["probes"] == 1:
+        return "join"
+    if p["sink"] == "aggr_hash":
+        return "hash"
+    return "scan"
+
+
+def plan_features(desc, selectivity=1.0, zipf=0.0):
+    """Feature vector (FEATURE_NAMES) of a lowered plan (Engine.describe / vc_plan_describe).
+    selectivity (fraction of fact rows that reach the sink) and zipf (key skew) are data
+    statistics the plan does not hold: the caller's estimates, else 1.0 and 0.0."""
+    p = fact_pipeline(desc)
+    rows = max(p["rows"], 1)
+    kind = kind_of(desc)
+    lg = lambda x: math.log2(max(float(x), 1.0))
+    return np.array([lg(rows), lg(p["probed_build_rows"] + 1), lg(p["groups_bound"]), lg(p["key_domain"]),
+                     p["filters"], p["probes"], p["probes_n"], p["aggregates"] / 8.0,
+                     p["scan_bytes"] / rows / 32.0, float(selectivity), float(zipf),
+                     float(p["sink"] == "aggr_global"), float(p["sink"] == "aggr_dense"),
+                     float(p["sink"] == "aggr_hash"), float(p["sink"] == "emit")] +
+                    [float(kind == k) for k in KINDS], dtype=np.float32)
+
+
+def _spec_params(spec):
     tmpl, _, rest = spec.partition(":")
     out = {}
     for item in rest.split(","):
@@ -60,52 +132,132 @@ def _params(spec):
     return tmpl, out
 
 
-def features(spec):
-    """Feature vector of a workload spec (see FEATURE_NAMES)."""
-    w = workload(spec)
-    tmpl, p = _params(spec)
-    rows = max(w.fact_rows, 1)
-    fact_cols = w.table_columns(w.fact_table)
-    bpr = sum(np.dtype(c.dtype).itemsize for c in fact_cols)
-    build_rows, domain, probes, aggs, sel, zipf = 0, 1, 0, 1, 1.0, 0.0
+def spec_statistics(spec):
+    """(selectivity, zipf) of a synthetic workload spec: the statistics its generator fixes."""
+    tmpl, p = _spec_params(spec)
     if tmpl == "sel_aggr":
-        sel = p.get("sel", 2436 / 2526.0)
-        domain, aggs = 180, 5
-    elif tmpl == "join_aggr":
-        build_rows = w.tables["orders"]
-        sel = p.get("sel", 0.2)
-        domain, probes, aggs = build_rows, 1, 2
-    elif tmpl == "groupby":
-        domain = p.get("keys", 1500000)
-        zipf = p.get("zipf", 0.0)
-        aggs = 3
-    elif tmpl == "star":
-        build_rows = sum(n for t, n in w.tables.items() if t != w.fact_table)
-        sel, domain, probes, aggs = 1 / 875.0, 35, 4, 2
-    onehot = [float(tmpl == t) for t in ("sel_aggr", "join_aggr", "groupby", "star")]
-    return np.array([math.log2(rows), sel, math.log2(build_rows + 1), math.log2(max(domain, 1)), zipf, bpr / 32.0,
-                     probes, aggs / 8.0] + onehot, dtype=np.float32)
+        return p.get("sel", 2436 / 2526.0), 0.0
+    if tmpl == "join_aggr":
+        return p.get("sel", 0.2), 0.0
+    if tmpl == "groupby":
+        return 1.0, p.get("zipf", 0.0)
+    if tmpl == "star":
+        return 1 / 875.0, 0.0
+    return 1.0, 0.0
 
 
-def autotune(spec, candidates=CANDIDATES, reps=5, log_path=None, engine=None, device=0):
-    """Exhaustive search: {flavor: median device ms} for every candidate on the workload."""
+_describe_cache = {}
+
+
+def describe_spec(spec):
+    """Lowered-plan description of a workload spec (an offline engine: no device, no compile)."""
+    if spec not in _describe_cache:
+        w = workload(spec)
+        e = Engine(offline=True)
+        e.load_workload(w)
+        _describe_cache[spec] = e.describe(w.plan)
+        e.close()
+    return _describe_cache[spec]
+
+
+def features(spec):
+    """Feature vector of a workload spec: its lowered plan plus the generator's statistics."""
+    sel, zipf = spec_statistics(spec)
+    return plan_features(describe_spec(spec), sel, zipf)
+
+
+def candidates_for(desc):
+    return GRIDS[kind_of(desc)]
+
+
+# ---------------------------------------------------------------------------- run logging
+
+
+class RunLog:
+    """Run records in the reference's SQLite `runs` table (compiler.cpp:100-106; columns it has
+    no counterpart for stay NULL) and/or a JSONL file."""
+
+    def __init__(self, sqlite_path=None, jsonl_path=None):
+        self.db = None
+        self.jsonl = jsonl_path
+        if sqlite_path:
+            self.db = sqlite3.connect(sqlite_path)
+            self.db.execute(
+                "CREATE TABLE IF NOT EXISTS runs(id INTEGER PRIMARY KEY AUTOINCREMENT, t TIMESTAMP, mode TEXT, "
+                "query TEXT, result TEXT, rep INTEGER, time_ms REAL NULL, tuples REAL NULL, cycles REAL NULL, "
+                "instructions REAL NULL, L1misses REAL NULL, LLCmisses REAL NULL, branchmisses REAL NULL, "
+                "taskclock REAL NULL, threads INTEGER, cgen_ms REAL NULL, ccomp_ms REAL NULL, default_blend TEXT, "
+                "key_check_blend TEXT, aggregates_blend TEXT, backend TEXT, scale_factor INTEGER, "
+                "pipeline_flavor TEXT, full_blend TEXT)")
+
+    def record(self, mode, query, flavor, result, rep, time_ms, tuples, ccomp_ms=None):
+        if self.db is not None:
+            self.db.execute(
+                "INSERT INTO runs(t, mode, query, result, rep, time_ms, tuples, threads, ccomp_ms, default_blend, "
+                "backend, scale_factor, full_blend) VALUES (datetime('now','localtime'), ?, ?, ?, ?, ?, ?, 1, ?, ?, "
+                "'cuda', 0, ?)", (mode, query, result, rep, time_ms, tuples, ccomp_ms, flavor, flavor))
+            self.db.commit()
+
+    def record_search(self, spec, times, feats):
+        if self.jsonl:
+            with open(self.jsonl, "a") as f:
+                f.write(json.dumps({"spec": spec, "features": feats.tolist(), "times_ms": times}) + "\n")
+
+    def close(self):
+        if self.db is not None:
+            self.db.close()
+            self.db = None
+
+
+# ---------------------------------------------------------------------------- search
+
+
+def autotune(spec, candidates=None, reps=5, log_path=None, engine=None, device=0, sqlite_path=None, mode="full"):
+    """Exhaustive search: {flavor: median device ms} over the workload kind's grid (or the
+    given candidates); candidates the device rejects are left out."""
     own = engine is None
     eng = engine or Engine(device)
     w = workload(spec)
     if own:
         eng.load_workload(w, on_device=True)
+    if candidates is None:
+        candidates = candidates_for(describe_spec(spec))
+    log = RunLog(sqlite_path, log_path)
     times = {}
     for fl in candidates:
-        q = eng.query(w.plan, fl)
+        t0 = time.perf_counter()
+        try:
+            q = eng.query(w.plan, fl)
+        except VoilaError as e:
+            log.record(mode, spec, fl, f"EXCEPT '{e}'", 0, None, w.fact_rows)
+            continue
+        ccomp = (time.perf_counter() - t0) * 1e3
         q.time(1)  # warm-up: module load, first-touch of tables
-        times[fl] = float(np.median(q.time(reps)))
+        ts = q.time(reps)
+        times[fl] = float(np.median(ts))
+        for r, t in enumerate(ts):
+            log.record(mode, spec, fl, "OK", r, float(t), w.fact_rows, ccomp)
         q.close()
-    if log_path:
-        with open(log_path, "a") as f:
-            f.write(json.dumps({"spec": spec, "features": features(spec).tolist(), "times_ms": times}) + "\n")
+    log.record_search(spec, times, features(spec))
+    log.close()
     if own:
         eng.close()
     return times
+
+
+def explore(spec, mode="full", sample=16, seed=1, reps=3, sqlite_path=None, log_path=None, engine=None):
+    """The reference explorer's modes over the CUDA flavor grid: 'full' times every candidate
+    of the workload's kind, 'sample' a seeded random subset of `sample` of them (the default
+    flavor always included).  Returns {flavor: ms}."""
+    cands = candidates_for(describe_spec(spec))
+    if mode == "sample":
+        rng = np.random.default_rng(seed)
+        pick = rng.choice(len(cands), size=min(sample, len(cands)), replace=False)
+        cands = [DEFAULT] + [cands[i] for i in sorted(pick) if cands[i] != DEFAULT]
+    elif mode != "full":
+        raise ValueError("mode must be full or sample")
+    return autotune(spec, candidates=cands, reps=reps, log_path=log_path, engine=engine,
+                    sqlite_path=sqlite_path, mode=mode)
 
 
 def load_log(path):
@@ -119,11 +271,15 @@ def load_log(path):
     return rows
 
 
+# ---------------------------------------------------------------------------- learned chooser
+
+
 class Chooser:
-    """MLP over workload features predicting log2(time / median time) of each candidate."""
+    """MLP over plan features predicting log2(time / median time) of each candidate."""
 
     def __init__(self, candidates=CANDIDATES, hidden=64, seed=7, device=0):
         self.candidates = list(candidates)
+        self.index = {c: i for i, c in enumerate(self.candidates)}
         self.hidden = hidden
         self.seed = seed
         self.device = device
@@ -136,11 +292,11 @@ class Chooser:
         M = np.zeros_like(T)
         for i, r in enumerate(records):
             t = r["times_ms"]
-            vals = [t[c] for c in self.candidates if c in t]
-            med = float(np.median(vals))
-            for j, c in enumerate(self.candidates):
-                if c in t and t[c] > 0:
-                    T[i, j] = math.log2(t[c] / med)
+            med = float(np.median(list(t.values())))
+            for c, ms in t.items():
+                j = self.index.get(c)
+                if j is not None and ms > 0:
+                    T[i, j] = math.log2(ms / med)
                     M[i, j] = 1.0
         return T, M
 
@@ -157,20 +313,34 @@ class Chooser:
         X = (np.atleast_2d(np.asarray(feats, dtype=np.float32)) - self.mu) / self.sd
         return self.mlp.predict(X)
 
-    def choose(self, spec_or_features):
-        f = features(spec_or_features) if isinstance(spec_or_features, str) else spec_or_features
-        return self.candidates[int(np.argmin(self.predict(f)[0]))]
+    def choose(self, spec_or_features, allowed=None):
+        """The candidate with the lowest predicted time among `allowed` (default: the grid of
+        the workload's kind when given a spec, else every candidate)."""
+        if isinstance(spec_or_features, str):
+            f = features(spec_or_features)
+            allowed = allowed or candidates_for(describe_spec(spec_or_features))
+        else:
+            f = spec_or_features
+        pred = self.predict(f)[0]
+        idx = [self.index[c] for c in allowed if c in self.index] if allowed else range(len(self.candidates))
+        return self.candidates[min(idx, key=lambda j: pred[j])]
+
+    def choose_for_plan(self, engine, plan, selectivity=1.0, zipf=0.0):
+        """Flavor for plan text on an engine holding its tables: featurized from the lowered plan."""
+        desc = engine.describe(plan)
+        return self.choose(plan_features(desc, selectivity, zipf), allowed=candidates_for(desc))
 
 
 def evaluate(chooser, records):
-    """Per record: time of the chosen, exhaustive-best and default flavors."""
+    """Per record: time of the chosen, exhaustive-best and default flavors (the chooser picks
+    among the candidates the record timed)."""
     out = []
     for r in records:
         t = r["times_ms"]
-        pick = chooser.choose(np.asarray(r["features"], dtype=np.float32))
+        pick = chooser.choose(np.asarray(r["features"], dtype=np.float32), allowed=list(t))
         best = min(t.values())
         out.append({"spec": r["spec"], "chosen": pick, "chosen_ms": t[pick], "best_ms": best,
-                    "best": min(t, key=t.get), "default_ms": t[DEFAULT]})
+                    "best": min(t, key=t.get), "default_ms": t.get(DEFAULT, max(t.values()))})
     return out
 
 

@@ -279,7 +279,16 @@ struct PipeGen {
 
 	std::string gen_main() {
 		fn_header("_main");
-		o << "  const int64_t n = " << P((unsigned long long)p.rows) << ";\n";
+		if (p.source_inter >= 0) {
+			/* the rows come from an earlier pipeline of the query: wait for it before reading
+			 * the row count (or any column) */
+			const InterTable& it = plan.inters[p.source_inter];
+			emit_pdl_wait();
+			o << "  const int64_t n = min((int64_t)__ldcg(" << Pptr(it.count, "const unsigned long long*") << "), "
+			  << P((unsigned long long)it.cap) << ");\n";
+		} else {
+			o << "  const int64_t n = " << P((unsigned long long)p.rows) << ";\n";
+		}
 		p.err_slot = (int)params.size();
 		o << "  unsigned* const err = (unsigned*)p.v[" << params.size() << "];\n";
 		params.push_back(0); /* error word, filled by the runtime */
@@ -342,6 +351,9 @@ struct PipeGen {
 			o << "  for (int64_t t = " << tstart() << "; t < " << tend() << "; t += " << tstep() << ") {\n";
 			emit_body("ldg");
 			o << "  }\n";
+		}
+		if (compact_at >= 0) {
+			o << "  if (cpend > 0) { cflush(); }\n";
 		}
 		sink_epilogue();
 		o << "}\n\n";
@@ -663,18 +675,41 @@ struct PipeGen {
 			return;
 		}
 		emit_ops(0, compact_at + 1);
-		/* selection vector: survivors' tile offsets (and carried payloads) in shared memory */
-		o << "    const int nsel = vd::block_compact<" << V << ">(act, (int)(threadIdx.x * " << V
-		  << "), csel, cscan, csel_pos);\n";
+		/* selection vector: the survivors' rows (and carried payloads) are appended to the
+		 * block's pending buffer; the rest of the pipeline runs once at least a full pass of
+		 * threads is pending, so every lane of the dependent gather/probe chain has a row */
+		o << "    const int nsel = vd::block_compact_rows<" << V << ">(act, r0, csel + cpend, cscan, csel_pos);\n";
 		for (size_t k = 0; k < carried.size(); k++) {
 			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) { if (act[v]) { ccar" << k
-			  << "[csel_pos[v]] = pay" << carried[k].first << "_" << carried[k].second << "[v]; } }\n";
+			  << "[cpend + csel_pos[v]] = pay" << carried[k].first << "_" << carried[k].second << "[v]; } }\n";
 		}
+		o << "    cpend += nsel;\n";
 		o << "    vd::block_sync();\n";
-		o << "    for (int base = 0; base < nsel; base += " << T << ") {\n";
+		o << "    if (cpend >= " << T << ") { cflush(); }\n";
+		o << "    }\n";
+	}
+
+	/* Shared-memory selection vector for compaction (declared once per kernel): room for a
+	 * pass of threads still pending plus one more tile's survivors, and the flush that runs
+	 * the pipeline's remaining ops and sink over the pending rows, one row per thread. */
+	void emit_compaction_smem() {
+		if (compact_at < 0) {
+			return;
+		}
+		const int cap = T + T * V;
+		/* row indices as 32 bits when every row of the table fits */
+		o << "  __shared__ " << (p.rows <= (int64_t)UINT32_MAX ? "uint32_t" : "int64_t") << " csel[" << cap << "];\n";
+		o << "  __shared__ int cscan[33];\n";
+		o << "  int csel_pos[" << V << "];\n";
+		o << "  int cpend = 0;\n";
+		for (size_t k = 0; k < carried.size(); k++) {
+			o << "  __shared__ int64_t ccar" << k << "[" << cap << "];\n";
+		}
+		o << "  auto cflush = [&]() {\n";
+		o << "    for (int base = 0; base < cpend; base += " << T << ") {\n";
 		o << "      const int ci = base + (int)threadIdx.x;\n";
-		o << "      const bool live = ci < nsel;\n";
-		o << "      const int64_t row = t * tile + (live ? csel[ci] : 0);\n";
+		o << "      const bool live = ci < cpend;\n";
+		o << "      const int64_t row = live ? (int64_t)csel[ci] : 0;\n";
 		const int saveV = V;
 		V = 1;
 		o << "      bool act[1] = {live};\n";
@@ -690,20 +725,8 @@ struct PipeGen {
 		V = saveV;
 		o << "    }\n";
 		o << "    vd::block_sync();\n";
-		o << "    }\n";
-	}
-
-	/* shared-memory selection vector for compaction (declared once per kernel) */
-	void emit_compaction_smem() {
-		if (compact_at < 0) {
-			return;
-		}
-		o << "  __shared__ int csel[" << T * V << "];\n";
-		o << "  __shared__ int cscan[33];\n";
-		o << "  int csel_pos[" << V << "];\n";
-		for (size_t k = 0; k < carried.size(); k++) {
-			o << "  __shared__ int64_t ccar" << k << "[" << T * V << "];\n";
-		}
+		o << "    cpend = 0;\n";
+		o << "  };\n";
 	}
 
 	/* payload outputs of a probe from the packed payload `raw` */
@@ -767,6 +790,10 @@ struct PipeGen {
 		} else {
 			o << "      const uint64_t bmask = ((const unsigned long long*)" << Pptr(jd.words, "const void*") << ")[1];\n";
 		}
+		if (fl.probe_lanes > 1) {
+			gen_probe_coop(op, jd, j);
+			return;
+		}
 		o << "      int st[" << V << "]; uint64_t bk[" << V << "]; " << KT << " key[" << V << "]; " << PT
 		  << " raw[" << V << "];\n";
 		o << "#pragma unroll\n      for (int v = 0; v < " << V << "; v++) {\n";
@@ -796,6 +823,70 @@ struct PipeGen {
 		o << "        }\n";
 		o << "        act[v] = st[v] == 1;\n";
 		emit_payload_unpack(op, jd, j, "raw[v]");
+		o << "      }\n";
+		o << "    }\n";
+	}
+
+	/*
+	 * Warp-cooperative probe (flavor probe=G): the G lanes of a lane group take the group's
+	 * keys one after another; for each key every lane reads a different bucket of its probe
+	 * sequence (b, b+1, ..., b+G-1), and a ballot over the group finds the earliest bucket that
+	 * holds the key (a match) or an empty slot (no match) -- linear probing never places a key
+	 * past an empty slot of its sequence.  Long probe sequences then cost one round trip per
+	 * G buckets instead of one per bucket; all lanes of a group stay converged.  Emitted inside
+	 * gen_probe's block after the table pointer and bucket mask (jt, bmask).
+	 */
+	void gen_probe_coop(const Op& op, const JoinDesc& jd, const std::string& j) {
+		const std::string KT = jd.key64 ? "uint64_t" : "uint32_t";
+		const std::string PT = jd.pay64 ? "uint64_t" : "uint32_t";
+		const int G = fl.probe_lanes;
+		o << "      const unsigned cl = vd::lane_id() & " << (G - 1) << "u, cbase = vd::lane_id() & ~" << (G - 1) << "u;\n";
+		o << "      const unsigned cmask = " << (G == 32 ? std::string("0xffffffffu") : "(" + std::to_string((1u << G) - 1u) + "u << cbase)")
+		  << ";\n";
+		o << "      bool cok[" << V << "]; uint64_t bk[" << V << "]; " << KT << " key[" << V << "];\n";
+		o << "#pragma unroll\n      for (int v = 0; v < " << V << "; v++) {\n";
+		std::string inrange = "act[v]";
+		std::string packed = "0ull";
+		for (size_t k = 0; k < op.keys.size(); k++) {
+			const std::string kv = expr(op.keys[k], "v");
+			const std::string lo = P((unsigned long long)(int64_t)jd.key_b[k].lo);
+			const std::string span = Pu((unsigned long long)(int64_t)(jd.key_b[k].hi - jd.key_b[k].lo));
+			inrange += " && (uint64_t)(" + kv + " - " + lo + ") <= " + span;
+			packed += " | ((uint64_t)(" + kv + " - " + lo + ") << " + P((unsigned long long)jd.key_shift[k]) + ")";
+		}
+		o << "        cok[v] = " << inrange << ";\n";
+		o << "        const uint64_t pk = " << packed << ";\n";
+		o << "        key[v] = (" << KT << ")(pk + 1ull);\n";
+		o << "        bk[v] = " << table_hash(op.keys, "pk", jd.key_bits, "v") << " & bmask;\n";
+		o << "      }\n";
+		o << "#pragma unroll\n      for (int v = 0; v < " << V << "; v++) {\n";
+		o << "        int mine = 0; " << PT << " myraw = 0;\n";
+		o << "        for (unsigned src = 0; src < " << G << "u; src++) {\n";
+		o << "          const bool ok = __shfl_sync(cmask, (unsigned)cok[v], cbase + src) != 0u;\n";
+		o << "          const " << KT << " k = __shfl_sync(cmask, key[v], cbase + src);\n";
+		o << "          uint64_t b = __shfl_sync(cmask, (unsigned long long)bk[v], cbase + src);\n";
+		o << "          int res = 0; " << PT << " r = 0;\n";
+		o << "          if (ok) {\n";
+		o << "            int step = 0;\n";
+		o << "            for (; step < VD_MAX_PROBES; step += " << G << ") {\n";
+		o << "              " << PT << " rr = 0;\n";
+		o << "              const int s = vd::join_probe_bucket(jt, (b + cl) & bmask, k, rr);\n";
+		o << "              const unsigned hit = __ballot_sync(cmask, s == 1) & cmask;\n";
+		o << "              const unsigned fin = (__ballot_sync(cmask, s == 0) & cmask) | hit;\n";
+		o << "              if (fin) {\n";
+		o << "                const int first = __ffs(fin) - 1;\n";
+		o << "                r = __shfl_sync(cmask, rr, first);\n";
+		o << "                res = (hit >> first) & 1u;\n";
+		o << "                break;\n";
+		o << "              }\n";
+		o << "              b += " << G << ";\n";
+		o << "            }\n";
+		o << "            if (step >= VD_MAX_PROBES && cl == 0) { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
+		o << "          }\n";
+		o << "          if (cl == src) { mine = res; myraw = r; }\n";
+		o << "        }\n";
+		o << "        act[v] = mine == 1;\n";
+		emit_payload_unpack(op, jd, j, "myraw");
 		o << "      }\n";
 		o << "    }\n";
 	}
@@ -1287,7 +1378,15 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 	params.assign(plan.pipes.size(), {});
 	for (auto& p : plan.pipes) {
 		auto& prm = params[p.id];
-		PipeGen g(p, plan, fl, st[p.id], qs, prm);
+		/* a pipeline feeding a later one writes its rows to its intermediate table */
+		QueryDeviceState target = qs;
+		if (p.out_inter >= 0) {
+			const InterTable& it = plan.inters[p.out_inter];
+			target.out = it.out;
+			target.out_cap = it.cap;
+			target.out_count = it.count;
+		}
+		PipeGen g(p, plan, fl, st[p.id], target, prm);
 		std::string main = g.gen_main();
 		std::string extra;
 		if (p.sink.kind == Sink::JoinBuild && !plan.joins[p.sink.join].direct) {
@@ -1410,6 +1509,9 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 			const int64_t ntiles = std::max<int64_t>((p.rows + tile - 1) / tile, 1);
 			return (ntiles + tiles_per_item - 1) / tiles_per_item;
 		};
+		if (!q.plan.inters.empty()) {
+			throw Error(6, "batched queries cannot hold aggregations below the plan root yet");
+		}
 		/* dependency levels of the join builds, and the work items per level */
 		std::vector<int> level(q.plan.pipes.size(), 0);
 		std::map<int, int> build_pipe_of_join;
@@ -1457,8 +1559,7 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 			bc.smem = std::max(bc.smem, g.smem_total);
 			prm[p.err_slot] = (unsigned long long)(uintptr_t)q.err;
 			for (size_t c = 0; c < p.cols.size(); c++) {
-				Column* col = q.eng->tables.at(p.cols[c].table).find(p.cols[c].name);
-				prm[p.col_slots[c]] = (unsigned long long)(uintptr_t)col->dev;
+				prm[p.col_slots[c]] = (unsigned long long)(uintptr_t)column_dev(q, p.cols[c]);
 			}
 			p.err_slot = saved_err;
 			p.col_slots = saved_cols;

@@ -438,6 +438,57 @@ __device__ __forceinline__ int block_compact(const bool (&act)[V], int off, int*
 	return scan[32];
 }
 
+/* block_compact for survivors collected across tiles: active rows get consecutive positions
+ * pos[v] (-1 otherwise) and sel[pos] = their absolute row index r0 + v.  Returns the count.
+ * All threads call it; `scan` holds 33 ints of shared memory. */
+template <int V, typename R>
+__device__ __forceinline__ int block_compact_rows(const bool (&act)[V], int64_t r0, R* sel, int* scan,
+	int (&pos)[V])
+{
+	int cnt = 0;
+#pragma unroll
+	for (int v = 0; v < V; v++) {
+		cnt += act[v] ? 1 : 0;
+	}
+	const unsigned lane = lane_id(), warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+	int x = cnt;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const int y = __shfl_up_sync(0xffffffffu, x, o);
+		if ((int)lane >= o) {
+			x += y;
+		}
+	}
+	if (lane == 31) {
+		scan[warp] = x;
+	}
+	block_sync();
+	if (threadIdx.x == 0) {
+		int run = 0;
+		for (unsigned w = 0; w < nw; w++) {
+			const int c = scan[w];
+			scan[w] = run;
+			run += c;
+		}
+		scan[32] = run;
+	}
+	block_sync();
+	int base = scan[warp] + x - cnt;
+#pragma unroll
+	for (int v = 0; v < V; v++) {
+		if (act[v]) {
+			pos[v] = base;
+			sel[base] = (R)(r0 + v);
+			base++;
+		} else {
+			pos[v] = -1;
+		}
+	}
+	const int total = scan[32];
+	block_sync();
+	return total;
+}
+
 /* Block dictionary of group slots for per-thread private accumulators: returns the dense
  * code (< gmax) of `slot`, assigning the next code on first sight, or -1 when the block has
  * run out of codes (or another thread's assignment did not become visible within a bounded

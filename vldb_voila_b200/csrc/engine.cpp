@@ -60,6 +60,9 @@ std::string Flavor::str() const
 	if (out_rows) {
 		o << ",ocap=" << out_rows;
 	}
+	if (probe_lanes != 1) {
+		o << ",probe=" << probe_lanes;
+	}
 	o << ")";
 	return o.str();
 }
@@ -122,6 +125,11 @@ Flavor Flavor::parse(const std::string& s0)
 			f.grid = num(0, 64);
 		} else if (k == "dense") {
 			f.dense_limit = num(1, 1 << 22);
+		} else if (k == "probe") {
+			f.probe_lanes = num(1, 32);
+			if (f.probe_lanes & (f.probe_lanes - 1)) {
+				throw Error(1, "probe lanes must be a power of two");
+			}
 		} else if (k == "ocap") {
 			f.out_rows = num(0, 1 << 30);
 		} else if (k == "gcap") {
@@ -225,6 +233,23 @@ QueryState& state_of(Query& q)
 	return g_state[&q];
 }
 
+/* device data of a pipeline column: a base table's column or an intermediate table's */
+void* column_dev(Query& q, const PipeColumn& pc)
+{
+	for (auto& it : q.plan.inters) {
+		if (it.name == pc.table) {
+			for (auto& c : it.cols) {
+				if (c.name == pc.name) {
+					return c.dev;
+				}
+			}
+			return nullptr;
+		}
+	}
+	Column* col = q.eng->tables.at(pc.table).find(pc.name);
+	return col ? col->dev : nullptr;
+}
+
 void query_prepare(Query& q)
 {
 	Engine& e = *q.eng;
@@ -291,6 +316,14 @@ void query_prepare(Query& q)
 		} else {
 			jd.stage_keys = dev_alloc(q, (size_t)rows * (jd.key64 ? 8 : 4));
 			jd.stage_pay = dev_alloc(q, (size_t)rows * (jd.pay64 ? 8 : 4));
+		}
+	}
+	/* intermediate tables: int64 columns of `cap` rows each, and a row count in the arena */
+	for (auto& it : plan.inters) {
+		it.out = (int64_t*)dev_alloc(q, (size_t)it.cap * it.cols.size() * 8);
+		it.count = (unsigned long long*)arena_take(8);
+		for (size_t c = 0; c < it.cols.size(); c++) {
+			it.cols[c].dev = it.out + (size_t)c * it.cap;
 		}
 	}
 	Pipeline& rp = plan.pipes[plan.result_pipe];
@@ -416,9 +449,7 @@ void query_prepare(Query& q)
 		auto& prm = q.params[p.id];
 		prm[p.err_slot] = (unsigned long long)(uintptr_t)q.err;
 		for (size_t c = 0; c < p.cols.size(); c++) {
-			Table& t = e.tables.at(p.cols[c].table);
-			Column* col = t.find(p.cols[c].name);
-			prm[p.col_slots[c]] = (unsigned long long)(uintptr_t)col->dev;
+			prm[p.col_slots[c]] = (unsigned long long)(uintptr_t)column_dev(q, p.cols[c]);
 		}
 	}
 }
@@ -428,12 +459,11 @@ static void refresh_column_params(Query& q)
 	for (auto& p : q.plan.pipes) {
 		auto& prm = q.params[p.id];
 		for (size_t c = 0; c < p.cols.size(); c++) {
-			Table& t = q.eng->tables.at(p.cols[c].table);
-			Column* col = t.find(p.cols[c].name);
-			if (!col || !col->dev) {
+			void* dev = column_dev(q, p.cols[c]);
+			if (!dev) {
 				throw Error(1, "column " + p.cols[c].table + "." + p.cols[c].name + " has no data");
 			}
-			prm[p.col_slots[c]] = (unsigned long long)(uintptr_t)col->dev;
+			prm[p.col_slots[c]] = (unsigned long long)(uintptr_t)dev;
 		}
 	}
 }
@@ -970,6 +1000,38 @@ int vc_workload_describe(const char* spec, char* buf, size_t cap, size_t* len)
 	});
 }
 
+int vc_plan_columns(const char* plan, char* buf, size_t cap, size_t* len)
+{
+	return guarded([&] {
+		if (!plan) {
+			throw Error(VC_ERR_INVALID, "null plan");
+		}
+		RelOpP root = parse_plan(plan);
+		std::vector<std::pair<std::string, std::string>> seen;
+		std::function<void(const RelOpP&)> walk = [&](const RelOpP& op) {
+			if (!op) {
+				return;
+			}
+			if (op->kind == RelOp::Scan) {
+				for (auto& c : op->columns) {
+					std::pair<std::string, std::string> k(op->table, c);
+					if (std::find(seen.begin(), seen.end(), k) == seen.end()) {
+						seen.push_back(k);
+					}
+				}
+			}
+			walk(op->left);
+			walk(op->right);
+		};
+		walk(root);
+		std::string d;
+		for (auto& k : seen) {
+			d += k.first + " " + k.second + "\n";
+		}
+		copy_out(d, buf, cap, len);
+	});
+}
+
 int vc_workload_batch(int count, uint64_t seed, int64_t min_rows, int64_t max_rows, char* buf, size_t cap,
 	size_t* len)
 {
@@ -1086,6 +1148,55 @@ int vc_query_result_text(vc_query* q, char* buf, size_t cap, size_t* len)
 	});
 }
 
+/* JSON list of a lowered plan's pipelines: what the flavor chooser featurizes */
+static std::string describe_pipelines(const LoweredPlan& plan)
+{
+	static const char* sinks[] = {"join_build", "aggr_global", "aggr_dense", "aggr_hash", "emit"};
+	std::ostringstream o;
+	o << "[";
+	for (size_t i = 0; i < plan.pipes.size(); i++) {
+		auto& p = plan.pipes[i];
+		int64_t bytes = 0;
+		for (auto& c : p.cols) {
+			bytes += p.rows * vc_gen_type_size(c.type);
+		}
+		int probes = 0, probes_n = 0, filters = 0;
+		int64_t build_rows = 0;
+		for (auto& op : p.ops) {
+			if (op.kind == Op::Filter) {
+				filters++;
+			} else {
+				probes++;
+				probes_n += plan.joins[op.join].join01 ? 0 : 1;
+				build_rows += plan.joins[op.join].build_rows;
+			}
+		}
+		const double domain = p.sink.domain > 0 ? (double)p.sink.domain : 0.0;
+		o << (i ? ", " : "") << "{\"table\": \"" << p.table << "\", \"rows\": " << p.rows << ", \"columns\": "
+		  << p.cols.size() << ", \"ops\": " << p.ops.size() << ", \"filters\": " << filters << ", \"probes\": " << probes
+		  << ", \"probes_n\": " << probes_n << ", \"probed_build_rows\": " << build_rows << ", \"sink\": \""
+		  << sinks[p.sink.kind] << "\", \"aggregates\": " << p.sink.aggs.size() << ", \"key_domain\": " << domain
+		  << ", \"groups_bound\": " << p.sink.groups_bound << ", \"scan_bytes\": " << bytes
+		  << ", \"intermediate_source\": " << (p.source_inter >= 0 ? "true" : "false")
+		  << ", \"result\": " << (p.id == plan.result_pipe ? "true" : "false") << "}";
+	}
+	o << "]";
+	return o.str();
+}
+
+int vc_plan_describe(vc_engine* eng, const char* plan, const char* flavor, char* buf, size_t cap, size_t* len)
+{
+	return guarded([&] {
+		if (!eng || !plan) {
+			throw Error(VC_ERR_INVALID, "null argument");
+		}
+		const Flavor fl = Flavor::parse(flavor ? flavor : "");
+		std::lock_guard<std::mutex> g(eng->e.mu);
+		LoweredPlan lp = lower_plan(parse_plan(plan), eng->e.tables, fl);
+		copy_out("{\"pipelines\": " + describe_pipelines(lp) + "}", buf, cap, len);
+	});
+}
+
 int vc_query_info(vc_query* q, char* buf, size_t cap, size_t* len)
 {
 	return guarded([&] {
@@ -1094,21 +1205,9 @@ int vc_query_info(vc_query* q, char* buf, size_t cap, size_t* len)
 		}
 		Query& qq = q->q;
 		std::ostringstream o;
-		static const char* sinks[] = {"join_build", "aggr_global", "aggr_dense", "aggr_hash", "emit"};
 		o << "{\"flavor\": \"" << qq.flavor.str() << "\", \"result_cols\": " << qq.plan.result_cols
-		  << ", \"source_bytes\": " << qq.code.source.size() << ", \"pipelines\": [";
-		for (size_t i = 0; i < qq.plan.pipes.size(); i++) {
-			auto& p = qq.plan.pipes[i];
-			int64_t bytes = 0;
-			for (auto& c : p.cols) {
-				bytes += p.rows * vc_gen_type_size(c.type);
-			}
-			o << (i ? ", " : "") << "{\"table\": \"" << p.table << "\", \"rows\": " << p.rows << ", \"columns\": "
-			  << p.cols.size() << ", \"ops\": " << p.ops.size() << ", \"sink\": \"" << sinks[p.sink.kind]
-			  << "\", \"scan_bytes\": " << bytes << ", \"result\": " << (p.id == qq.plan.result_pipe ? "true" : "false")
-			  << "}";
-		}
-		o << "], \"kernels\": [";
+		  << ", \"source_bytes\": " << qq.code.source.size() << ", \"pipelines\": " << describe_pipelines(qq.plan);
+		o << ", \"kernels\": [";
 		for (size_t i = 0; i < qq.code.launches.size(); i++) {
 			auto& l = qq.code.launches[i];
 			o << (i ? ", " : "") << "{\"name\": \"" << l.kernel << "\", \"pipeline\": " << l.pipe << ", \"smem\": "

@@ -164,6 +164,19 @@ struct Sink {
 	int nwords = 0;
 };
 
+/* An aggregation's result kept on the device as the input of a later pipeline of the same
+ * query: the reference's bucket_flush + re-aggregation + read chain (relalg_translator.cpp
+ * :659-809) becomes one table of int64 columns key_<i>, aggr_<j> with a device-side row
+ * count, written by the producing pipeline's sink and scanned by the consumer. */
+struct InterTable {
+	std::string name;                 /* aggr_ht<N>, as the reference's translator names it */
+	int producer = -1;                /* pipeline whose sink writes the rows */
+	int64_t cap = 0;                  /* row capacity: the producer's groups bound */
+	std::vector<Column> cols;         /* int64 columns with their value bounds */
+	int64_t* out = nullptr;           /* cols x cap, column-major */
+	unsigned long long* count = nullptr;
+};
+
 struct PipeColumn {
 	std::string table, name;
 	int type;
@@ -177,6 +190,8 @@ struct Pipeline {
 	std::vector<PipeColumn> cols;
 	std::vector<Op> ops;
 	Sink sink;
+	int source_inter = -1;       /* scans an intermediate table (row count read on the device) */
+	int out_inter = -1;          /* the sink writes an intermediate table, not the query result */
 	int err_slot = -1;           /* parameter slot of the device error word */
 	std::vector<int> col_slots;  /* parameter slots of the column pointers */
 };
@@ -204,6 +219,7 @@ struct Flavor {
 	int64_t direct_limit = 64ll << 20; /* auto: direct when the upper-bound table fits this many bytes */
 	int sink_smem = 96 * 1024; /* most shared memory a dense aggregation keeps its slots in (else global) */
 	int64_t group_slots = 0;  /* hash group table slots (0 = sized from the groups bound and fill) */
+	int probe_lanes = 1;      /* lanes that probe one join key together (1 = each lane its own key) */
 	int64_t out_rows = 0;     /* result row capacity of an emitting pipeline (0 = from its bound, at
 	                           * most 4 rows per input row + 2^20 when joinN probes multiply rows) */
 
@@ -214,6 +230,7 @@ struct Flavor {
 struct LoweredPlan {
 	std::vector<Pipeline> pipes;
 	std::vector<JoinDesc> joins;
+	std::vector<InterTable> inters;
 	int result_pipe = -1;
 	int result_cols = 0;
 };
@@ -323,6 +340,7 @@ struct QueryState {
 };
 
 QueryState& state_of(Query& q);
+void* column_dev(Query& q, const PipeColumn& pc);
 
 /* ------------------------------------------------------------------ batches ------------ */
 

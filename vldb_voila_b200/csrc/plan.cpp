@@ -189,9 +189,16 @@ struct Lowerer {
 	const Flavor& fl;
 	LoweredPlan out;
 
+	std::map<std::string, Table> inter_tables; /* intermediate tables by name */
+	int name_counter = 0; /* the reference translator's id counter (relalg_translator.hpp:26-30) */
+
 	Lowerer(std::map<std::string, Table>& t, const Flavor& f) : tables(t), fl(f) {}
 
 	Table& table(const std::string& n) {
+		auto ii = inter_tables.find(n);
+		if (ii != inter_tables.end()) {
+			return ii->second;
+		}
 		auto it = tables.find(n);
 		if (it == tables.end()) {
 			throw Error(kErrInvalid, "unknown table '" + n + "'");
@@ -358,6 +365,9 @@ struct Lowerer {
 			return pi;
 		}
 		case RelOp::HashJoin: {
+			/* the reference names the join table before translating either side
+			 * (relalg_translator.cpp:814): keep its numbering of later aggregations */
+			name_counter++;
 			/* build side first: its pipeline must run before the probe */
 			Scope bs;
 			int bi = lower(op->right, bs);
@@ -442,7 +452,7 @@ struct Lowerer {
 			return pi;
 		}
 		case RelOp::HashAggr:
-			throw Error(kErrUnsupported, "aggregation is only supported at the root of the plan");
+			return lower_inner_aggregate(op, sc);
 		}
 		throw Error(kErrInvalid, "bad operator");
 	}
@@ -457,9 +467,9 @@ struct Lowerer {
 		return r > kI64Max ? INT64_MAX : (int64_t)r;
 	}
 
-	void aggregate(const RelOpP& op) {
-		Scope sc;
-		int pi = lower(op->left, sc);
+	/* The sink of an aggregation over pipeline pi's rows (visible columns in sc): global,
+	 * dense slots or a hash table (relalg_translator.cpp:380-656).  *vis = result columns. */
+	Sink make_agg_sink(const RelOpP& op, Scope& sc, int pi, int* vis) {
 		Pipeline& p = out.pipes[pi];
 		Sink sink;
 		const int64_t rows = rows_bound(p);
@@ -486,10 +496,7 @@ struct Lowerer {
 				if (ag.arg->boolean) {
 					throw Error(kErrUnsupported, "sum over a predicate is not supported");
 				}
-				Bounds sb;
-				sb.lo = ag.arg->b.lo < 0 ? ag.arg->b.lo * rows : 0;
-				sb.hi = ag.arg->b.hi > 0 ? ag.arg->b.hi * rows : 0;
-				check_range(sb, "sum(...) over " + std::to_string(rows) + " rows");
+				check_range(sum_bounds(ag.arg->b, rows), "sum(...) over " + std::to_string(rows) + " rows");
 			}
 			sink.aggs.push_back(ag);
 		}
@@ -546,13 +553,99 @@ struct Lowerer {
 				pack_aggregates(sink, rows);
 			}
 		}
-		p.sink = sink;
-		out.result_pipe = pi;
-		int vis = (int)sink.keys.size();
+		int v = (int)sink.keys.size();
 		for (auto& a : sink.aggs) {
-			vis += a.visible ? 1 : 0;
+			v += a.visible ? 1 : 0;
 		}
+		*vis = v;
+		return sink;
+	}
+
+	static Bounds sum_bounds(const Bounds& b, int64_t rows) {
+		Bounds sb;
+		sb.lo = b.lo < 0 ? b.lo * rows : 0;
+		sb.hi = b.hi > 0 ? b.hi * rows : 0;
+		return sb;
+	}
+
+	void aggregate(const RelOpP& op) {
+		Scope sc;
+		int pi = lower(op->left, sc);
+		name_counter += 2;
+		int vis = 0;
+		out.pipes[pi].sink = make_agg_sink(op, sc, pi, &vis);
+		out.result_pipe = pi;
 		out.result_cols = vis;
+	}
+
+	/* An aggregation below the root: its rows (keys, then the visible aggregates) go to an
+	 * intermediate table named like the reference's re-aggregation table, aggr_ht<N> with
+	 * columns key_<i> and aggr_<j> (relalg_translator.cpp:392, :740-760, :776-808), and a new
+	 * pipeline scans it. */
+	int lower_inner_aggregate(const RelOpP& op, Scope& sc) {
+		Scope csc;
+		const int pi = lower(op->left, csc);
+		name_counter += 2;
+		const std::string name = "aggr_ht" + std::to_string(name_counter - 1);
+		int vis = 0;
+		Sink sink = make_agg_sink(op, csc, pi, &vis);
+		const int64_t rows = rows_bound(out.pipes[pi]);
+		InterTable it;
+		it.name = name;
+		it.producer = pi;
+		switch (sink.kind) {
+		case Sink::AggGlobal: it.cap = 1; break;
+		case Sink::AggDense: it.cap = (int64_t)sink.domain; break;
+		default: it.cap = std::max<int64_t>(sink.groups_bound, 1); break;
+		}
+		it.cap = (it.cap + 1) & ~(int64_t)1; /* even: every column starts 16-byte aligned */
+		Table t;
+		t.name = name;
+		t.rows = it.cap;
+		for (size_t i = 0; i < sink.keys.size(); i++) {
+			Column c;
+			c.name = "key_" + std::to_string(i);
+			c.type = VC_TYPE_I64;
+			c.lo = (int64_t)sink.keys[i]->b.lo;
+			c.hi = (int64_t)sink.keys[i]->b.hi;
+			t.cols.push_back(c);
+		}
+		int j = 0;
+		for (auto& a : sink.aggs) {
+			if (!a.visible) {
+				continue;
+			}
+			Column c;
+			c.name = "aggr_" + std::to_string(j++);
+			c.type = VC_TYPE_I64;
+			if (a.count) {
+				c.lo = 0;
+				c.hi = std::max<int64_t>(rows, 1);
+			} else {
+				const Bounds sb = sum_bounds(a.arg->b, rows);
+				c.lo = (int64_t)sb.lo;
+				c.hi = (int64_t)sb.hi;
+			}
+			t.cols.push_back(c);
+		}
+		it.cols = t.cols;
+		out.pipes[pi].sink = sink;
+		out.pipes[pi].out_inter = (int)out.inters.size();
+		out.inters.push_back(it);
+		inter_tables[name] = t;
+
+		Pipeline np;
+		np.id = (int)out.pipes.size();
+		np.table = name;
+		np.rows = it.cap;
+		np.source_inter = (int)out.inters.size() - 1;
+		np.sink.kind = Sink::Emit;
+		sc.cols.clear();
+		for (auto& c : t.cols) {
+			sc.cols.push_back(ScopeEntry{name + "." + c.name, nullptr, name, c.name});
+		}
+		out.pipes.push_back(np);
+		return np.id;
 	}
 
 	/* First-fit-decreasing packing of the aggregates' bit fields into 64-bit words: the

@@ -97,6 +97,8 @@ def lib():
         "vc_batch_hold_item": (c.c_int, [P, c.c_int64, c.c_int]),
         "vc_query_timings": (c.c_int, [P, c.POINTER(c.c_float), c.c_int, c.POINTER(c.c_int), P, c.c_size_t]),
         "vc_stream_read": (c.c_int, [P, c.c_int64, P, P]),
+        "vc_plan_columns": (c.c_int, [c.c_char_p, P, c.c_size_t, c.POINTER(c.c_size_t)]),
+        "vc_plan_describe": (c.c_int, [P, c.c_char_p, c.c_char_p, P, c.c_size_t, c.POINTER(c.c_size_t)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)
@@ -195,6 +197,11 @@ def workload(spec):
         elif tag == "plan":
             w.plan = rest
     return w
+
+
+def plan_columns(plan):
+    """[(table, column)] the plan scans."""
+    return [tuple(l.split()) for l in _text_call(lib().vc_plan_columns, _b(plan)).splitlines() if l]
 
 
 def batch_specs(count, seed, min_rows=10_000, max_rows=60_000_000):
@@ -322,6 +329,11 @@ class Engine:
 
     def query(self, plan, flavor=""):
         return Query(self, plan, flavor)
+
+    def describe(self, plan, flavor=""):
+        """The plan's lowered pipelines (no compilation): vc_plan_describe as a dict."""
+        import json
+        return json.loads(_text_call(lib().vc_plan_describe, self._h, _b(plan), _b(flavor or "")))
 
 
 class Query:

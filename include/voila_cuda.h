@@ -81,6 +81,10 @@ int vc_table_drop(vc_engine* eng, const char* table);
  * its device storage. */
 int vc_column_add(vc_engine* eng, const char* table, const char* column, int type, int64_t lo, int64_t hi);
 
+/* A column's type, declared domain [lo, hi] and its table's row count (any pointer may be NULL). */
+int vc_column_info(vc_engine* eng, const char* table, const char* column, int32_t* type, int64_t* lo, int64_t* hi,
+	int64_t* rows);
+
 /* Copies `rows` values from host memory into the column (Attribute::operator=,
  * Database.hpp:59-62).  Asynchronous on `stream`; pinned host memory gives full speed. */
 int vc_column_upload(vc_engine* eng, const char* table, const char* column, const void* host, int64_t rows,
@@ -102,6 +106,17 @@ int vc_column_device_ptr(vc_engine* eng, const char* table, const char* column, 
  * VC_GEN_ZIPF column.  Stands in for the TPC-H/SSB import (Import.cpp:165-250). */
 int vc_column_generate(vc_engine* eng, const char* table, const char* column, int32_t kind, int64_t a,
 	int64_t b, int64_t c, double s, uint64_t seed, const double* zipf_cdf, void* stream);
+
+/* Imports <dir>/<table>.tbl (pipe-separated text, one row per line: the TPC-H/SSB dbgen
+ * format) as a new table: `schema` lists every field of a line in order as name:type (int,
+ * bigint, date = YYYY-MM-DD as its Julian day number, decN = decimal as value * 10^N, char =
+ * first byte) or "-" to skip it.  Parsed on `threads` host threads (0 = all) and cached as
+ * raw column arrays <dir>/cached/<table>_<name>, which later imports read instead of the
+ * text -- the reference's import path and cache layout (Import.cpp:165-250).  Each column's
+ * declared domain is its observed [min, max] (the reference's MinMaxInfo).  *rows_out gets
+ * the row count.  The upload is synchronous. */
+int vc_table_import(vc_engine* eng, const char* table, const char* dir, const char* schema, int threads,
+	int64_t* rows_out);
 
 /* Host-side generator for the same columns: writes rows [begin, begin+count) into `out`
  * (element type `type`). */

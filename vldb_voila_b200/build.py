@@ -19,7 +19,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", 
               "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
 CXX_FLAGS = ["-O2", "-g", "-fPIC", "-std=c++17", "-Wall", "-Wno-unused-function", "-ffp-contract=off"]
 
-CPP_SOURCES = ["engine.cpp", "plan.cpp", "codegen.cpp", "jit.cpp", "batch.cpp"]
+CPP_SOURCES = ["engine.cpp", "plan.cpp", "codegen.cpp", "jit.cpp", "batch.cpp", "import.cpp"]
 CU_SOURCES = ["datagen.cu", "mlp.cu", "noalloc.cu", "floor.cu"]
 HEADERS = ["datagen.h", "engine_internal.hpp", "sexpr.hpp", "workloads.hpp", "device/voila_device.cuh"]
 

@@ -732,6 +732,62 @@ static Column& column_of(vc_engine* eng, const char* t, const char* c)
 	return *col;
 }
 
+namespace vc {
+Engine& engine_of(vc_engine* e)
+{
+	return e->e;
+}
+
+/* Declares an imported table with its columns (domains as observed) and uploads the host
+ * data synchronously (the import's host buffers are released when it returns).  On a
+ * compile-only engine the columns get stand-in addresses and no data. */
+void import_declare(Engine& e, const std::string& table, int64_t rows, const std::vector<std::string>& names,
+	const std::vector<int>& types, const std::vector<int64_t>& lo, const std::vector<int64_t>& hi,
+	const std::vector<const void*>& data)
+{
+	std::lock_guard<std::mutex> g(e.mu);
+	if (e.tables.count(table)) {
+		throw Error(VC_ERR_INVALID, "table '" + table + "' exists");
+	}
+	Table t;
+	t.name = table;
+	t.rows = rows;
+	try {
+		for (size_t i = 0; i < names.size(); i++) {
+			Column c;
+			c.name = names[i];
+			c.type = types[i];
+			c.lo = rows ? lo[i] : 0;
+			c.hi = rows ? hi[i] : 0;
+			const size_t bytes = (size_t)std::max<int64_t>(rows, 1) * vc_gen_type_size(c.type);
+			if (e.offline) {
+				c.dev = (void*)e.fake_next;
+				e.fake_next += ((bytes + 255) / 256 + 1) * 256;
+			} else {
+				VC_CHECK_CUDA(cudaSetDevice(e.device));
+				VC_CHECK_CUDA(cudaMalloc(&c.dev, ((bytes + 255) / 256) * 256));
+				c.owned = true;
+				t.cols.push_back(c);
+				if (rows) {
+					VC_CHECK_CUDA(cudaMemcpy(c.dev, data[i], (size_t)rows * vc_gen_type_size(c.type),
+						cudaMemcpyHostToDevice));
+				}
+				continue;
+			}
+			t.cols.push_back(c);
+		}
+	} catch (...) {
+		for (auto& c : t.cols) {
+			if (c.owned && c.dev) {
+				cudaFree(c.dev);
+			}
+		}
+		throw;
+	}
+	e.tables[table] = t;
+}
+} // namespace vc
+
 extern "C" {
 
 const char* vc_last_error(void)
@@ -851,6 +907,19 @@ int vc_column_add(vc_engine* eng, const char* table, const char* column, int typ
 			c.owned = true;
 		}
 		t.cols.push_back(c);
+	});
+}
+
+int vc_column_info(vc_engine* eng, const char* table, const char* column, int32_t* type, int64_t* lo, int64_t* hi,
+	int64_t* rows)
+{
+	return guarded([&] {
+		Table& t = table_of(eng, table);
+		Column& c = column_of(eng, table, column);
+		if (type) *type = c.type;
+		if (lo) *lo = c.lo;
+		if (hi) *hi = c.hi;
+		if (rows) *rows = t.rows;
 	});
 }
 

@@ -98,6 +98,9 @@ def lib():
         "vc_query_timings": (c.c_int, [P, c.POINTER(c.c_float), c.c_int, c.POINTER(c.c_int), P, c.c_size_t]),
         "vc_stream_read": (c.c_int, [P, c.c_int64, P, P]),
         "vc_plan_columns": (c.c_int, [c.c_char_p, P, c.c_size_t, c.POINTER(c.c_size_t)]),
+        "vc_table_import": (c.c_int, [P, c.c_char_p, c.c_char_p, c.c_char_p, c.c_int, c.POINTER(c.c_int64)]),
+        "vc_column_info": (c.c_int, [P, c.c_char_p, c.c_char_p, c.POINTER(c.c_int32), c.POINTER(c.c_int64),
+                                     c.POINTER(c.c_int64), c.POINTER(c.c_int64)]),
         "vc_plan_describe": (c.c_int, [P, c.c_char_p, c.c_char_p, P, c.c_size_t, c.POINTER(c.c_size_t)]),
     }
     for name, (res, args) in sigs.items():
@@ -299,6 +302,26 @@ class Engine:
 
     def attach(self, table, name, device_ptr):
         check(lib().vc_column_attach(self._h, _b(table), _b(name), ctypes.c_void_p(device_ptr)))
+
+    def column_info(self, table, name):
+        """(type, lo, hi, rows) of a column: its type code, declared domain and table rows."""
+        t, lo, hi, n = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        check(lib().vc_column_info(self._h, _b(table), _b(name), ctypes.byref(t), ctypes.byref(lo), ctypes.byref(hi),
+                                   ctypes.byref(n)))
+        return t.value, lo.value, hi.value, n.value
+
+    def import_tbl(self, table, directory, schema, threads=0):
+        """Imports <directory>/<table>.tbl (pipe-separated; schema "name:type,..." with types int,
+        bigint, date, decN, char, or "-" to skip a field) through the <directory>/cached/ column
+        cache.  Returns the row count."""
+        n = ctypes.c_int64()
+        check(lib().vc_table_import(self._h, _b(table), _b(directory), _b(schema), threads, ctypes.byref(n)))
+        self.tables[table] = {"rows": n.value, "columns": {}}
+        for item in schema.split(","):
+            if item != "-":
+                name = item.split(":")[0]
+                self.tables[table]["columns"][name] = self.column_info(table, name)[0]
+        return n.value
 
     def device_ptr(self, table, name):
         p = ctypes.c_void_p()

@@ -123,6 +123,14 @@ def _check_int64(arrs):
             raise OverflowError("oracle value range close to int64 limits")
 
 
+def _exact(v):
+    """v as int64 when its sums cannot leave int64, else as Python ints (exact 128-bit sums,
+    the reference's i128 results, typing_pass.cpp:244-259)."""
+    if v.size and int(np.abs(v).max()) * v.size >= 2**62:
+        return v.astype(object)
+    return v
+
+
 def _pack_keys(cols):
     """Unique int64 code per key tuple (via np.unique on stacked keys)."""
     if len(cols) == 1:
@@ -169,8 +177,7 @@ def _aggregate(node, f):
     if f.n == 0:
         return [np.zeros(0, dtype=np.int64) for _ in keys], [np.zeros(0, dtype=np.int64) for _ in aggs]
     if glob:
-        return [], [np.array([f.n if kind == "count" else int(v.sum(dtype=np.int64))], dtype=np.int64)
-                    for kind, v in aggs]
+        return [], [np.array([f.n if kind == "count" else _exact(v).sum()], dtype=object) for kind, v in aggs]
     stacked = np.stack(keys, axis=1)
     uniq, inv = np.unique(stacked, axis=0, return_inverse=True)
     inv = inv.reshape(-1)
@@ -179,7 +186,10 @@ def _aggregate(node, f):
     counts = np.diff(np.concatenate([bounds, [f.n]]))
     out = []
     for kind, v in aggs:
-        out.append(counts.astype(np.int64) if kind == "count" else np.add.reduceat(v[order], bounds).astype(np.int64))
+        if kind == "count":
+            out.append(counts.astype(np.int64))
+        else:
+            out.append(np.add.reduceat(_exact(v)[order], bounds))
     return [uniq[:, i].astype(np.int64) for i in range(uniq.shape[1])], out
 
 

@@ -54,6 +54,10 @@ HAVING_EMIT = ("(select (fun > (col aggr_ht1.aggr_0) (const 200))"
                " (aggr hash ((col lineitem.l_orderkey)) ((fun sum (col lineitem.l_quantity)))"
                " (scan lineitem (l_orderkey l_quantity))))")
 
+# sums whose bound leaves int64: the reference types them i128
+WIDE_GLOBAL = ("(aggr global () ((fun sum (col fact.w)) (fun sum (col fact.v)) (fun count))"
+               " (scan fact (v w)))")
+
 CASES = [
     ("sel_aggr_1k", "sel_aggr:rows=1000,seed=11", None),
     ("sel_aggr_100k", "sel_aggr:rows=100000,seed=12", None),
@@ -77,6 +81,8 @@ CASES = [
     ("agg_of_agg", "groupby:rows=20000,keys=3000,zipf=0.8,seed=71", AGG_OF_AGG),
     ("having_global", "groupby:rows=20000,keys=3000,zipf=0.8,seed=72", HAVING_GLOBAL),
     ("having_emit", "groupby:rows=20000,keys=3000,zipf=0.8,seed=73", HAVING_EMIT),
+    ("wide_sums", "bigsum:rows=40000,seed=95", None),
+    ("wide_global", "bigsum:rows=40000,seed=96", WIDE_GLOBAL),
 ]
 
 

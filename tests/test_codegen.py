@@ -240,3 +240,22 @@ def test_sub_aggregations_are_not_batched_yet():
     with pytest.raises(VoilaError) as ex:
         Batch([e.query(m["plan"])])
     assert ex.value.code == 6
+
+
+def test_sums_beyond_int64_are_split_into_exact_chunk_sums():
+    """sum(w) over 40,000 values up to 2e15 can reach 8e19: it is computed as int64 sums of bit
+    chunks of w (recombined in 128 bits on the host), never rejected and never wrapped."""
+    w, e = offline("bigsum:rows=40000,seed=95")
+    q = e.query(w.plan)
+    src = q.source()
+    assert "& 1073741823ull" in src or "ull))" in src
+    assert ">> " in src
+    info = q.info()
+    # physical result columns: key, sum(v) in 2 chunks, sum(w) in 2 chunks, count
+    assert info["result_cols"] == 6
+    # a sub-aggregation cannot hand 128-bit values to a later pipeline: rejected, not wrapped
+    plan = ("(aggr global () ((fun count)) (select (fun > (col aggr_ht1.aggr_0) (const 0))"
+            " (aggr hash ((col fact.g)) ((fun sum (col fact.w))) (scan fact (g w)))))")
+    with pytest.raises(VoilaError) as ex:
+        e.query(plan)
+    assert ex.value.code == 6

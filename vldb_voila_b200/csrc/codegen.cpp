@@ -121,6 +121,13 @@ struct PipeGen {
 			static const std::map<std::string, std::string> ops = {
 				{"add", "+"}, {"sub", "-"}, {"mul", "*"}, {"lt", "<"}, {"le", "<="}, {"gt", ">"},
 				{"ge", ">="}, {"eq", "=="}, {"ne", "!="}, {"and", "&&"}, {"or", "||"}};
+			if (e->fn == "shr") {
+				return "((int64_t)(" + expr(e->args[0], v) + ") >> " + std::to_string(e->args[1]->cval) + ")";
+			}
+			if (e->fn == "lowbits") {
+				const unsigned long long m = (1ull << e->args[1]->cval) - 1ull;
+				return "((int64_t)((uint64_t)(" + expr(e->args[0], v) + ") & " + std::to_string(m) + "ull))";
+			}
 			if (e->fn == "mul" && fits32(e->args[0]->b) && fits32(e->args[1]->b)) {
 				return "vd::mulw(" + expr(e->args[0], v) + ", " + expr(e->args[1], v) + ")";
 			}

@@ -69,10 +69,14 @@ VC_GEN_FN uint64_t vc_gen_bits(uint64_t seed, uint64_t i)
 	return vc_gen_mix64(base + (i + 1) * UINT64_C(0x9e3779b97f4a7c15));
 }
 
-/* uniform in [0, range) for range <= 2^32, from the top 32 bits (multiply-shift) */
+/* uniform in [0, range): for range <= 2^32 from the top 32 bits (multiply-shift); wider
+ * ranges take the high half of the full 64 x 64-bit product */
 VC_GEN_FN uint64_t vc_gen_below(uint64_t bits, uint64_t range)
 {
-	return ((bits >> 32) * range) >> 32;
+	if (range <= (UINT64_C(1) << 32)) {
+		return ((bits >> 32) * range) >> 32;
+	}
+	return (uint64_t)(((unsigned __int128)bits * range) >> 64);
 }
 
 /* 4-round balanced Feistel bijection on [0, 4^h), cycle-walked into [0, n) */

@@ -621,25 +621,77 @@ void query_fetch(Query& q)
 	}
 }
 
+/* decimal text of a 128-bit integer */
+static void append_i128(std::string& s, __int128 v)
+{
+	char buf[48];
+	if (v >= (__int128)INT64_MIN && v <= (__int128)INT64_MAX) {
+		const int len = std::snprintf(buf, sizeof(buf), "%" PRId64, (int64_t)v);
+		s.append(buf, (size_t)len);
+		return;
+	}
+	const bool neg = v < 0;
+	unsigned __int128 u = neg ? (unsigned __int128)(-(v + 1)) + 1u : (unsigned __int128)v;
+	int i = 47;
+	buf[i] = 0;
+	while (u) {
+		buf[--i] = (char)('0' + (int)(u % 10u));
+		u /= 10u;
+	}
+	if (neg) {
+		buf[--i] = '-';
+	}
+	s.append(buf + i);
+}
+
+/* value of the caller's column c at row r: its physical parts, shifted and summed */
+static __int128 result_value(const Query& q, int c, int64_t r)
+{
+	const int64_t R = q.result_rows;
+	__int128 v = 0;
+	for (auto& pt : q.plan.out_cols[(size_t)c].parts) {
+		v += (__int128)q.result_host[(size_t)pt.first * R + r] * ((__int128)1 << pt.second);
+	}
+	return v;
+}
+
 std::string query_result_text(Query& q)
 {
 	query_fetch(q);
-	const int C = q.plan.result_cols;
+	const int C = (int)q.plan.out_cols.size();
 	const int64_t R = q.result_rows;
 	std::string s;
 	s.reserve((size_t)R * C * 12);
-	char buf[32];
 	for (int64_t r = 0; r < R; r++) {
 		for (int c = 0; c < C; c++) {
 			if (c) {
 				s.push_back('|');
 			}
-			int len = std::snprintf(buf, sizeof(buf), "%" PRId64, q.result_host[(size_t)c * R + r]);
-			s.append(buf, (size_t)len);
+			append_i128(s, result_value(q, c, r));
 		}
 		s.push_back('\n');
 	}
 	return s;
+}
+
+/* the caller's columns as int64, column-major; a value beyond int64 is an error */
+void query_result_int64(Query& q, int64_t* out, int64_t cap)
+{
+	query_fetch(q);
+	const int64_t R = q.result_rows;
+	const int C = (int)q.plan.out_cols.size();
+	if (R * C > cap) {
+		throw Error(1, "result buffer too small");
+	}
+	for (int c = 0; c < C; c++) {
+		for (int64_t r = 0; r < R; r++) {
+			const __int128 v = result_value(q, c, r);
+			if (v < (__int128)INT64_MIN || v > (__int128)INT64_MAX) {
+				throw Error(3, "a result value exceeds int64: read it with vc_query_result_text");
+			}
+			out[(size_t)c * R + r] = (int64_t)v;
+		}
+	}
 }
 
 } // namespace vc
@@ -1187,7 +1239,7 @@ int vc_query_result_shape(vc_query* q, int64_t* rows, int32_t* cols)
 			*rows = q->q.result_rows;
 		}
 		if (cols) {
-			*cols = q->q.plan.result_cols;
+			*cols = (int32_t)q->q.plan.out_cols.size();
 		}
 	});
 }
@@ -1198,12 +1250,7 @@ int vc_query_result_copy(vc_query* q, int64_t* out, int64_t cap)
 		if (!q || !out) {
 			throw Error(VC_ERR_INVALID, "null argument");
 		}
-		query_fetch(q->q);
-		const size_t n = q->q.result_host.size();
-		if ((int64_t)n > cap) {
-			throw Error(VC_ERR_INVALID, "result buffer too small");
-		}
-		std::memcpy(out, q->q.result_host.data(), n * 8);
+		query_result_int64(q->q, out, cap);
 	});
 }
 

@@ -227,12 +227,20 @@ struct Flavor {
 	static Flavor parse(const std::string& s);
 };
 
+/* A result column as the caller sees it: the sum of physical result-buffer columns, each
+ * shifted left by its amount.  Every column has one part except a sum whose bound leaves
+ * int64, which is computed as exact int64 sums of bit chunks and recombined in 128 bits. */
+struct OutCol {
+	std::vector<std::pair<int, int>> parts; /* (physical column, shift) */
+};
+
 struct LoweredPlan {
 	std::vector<Pipeline> pipes;
 	std::vector<JoinDesc> joins;
 	std::vector<InterTable> inters;
 	int result_pipe = -1;
-	int result_cols = 0;
+	int result_cols = 0;              /* physical columns of the result buffer */
+	std::vector<OutCol> out_cols;     /* the caller's columns */
 };
 
 LoweredPlan lower_plan(const RelOpP& root, std::map<std::string, Table>& tables, const Flavor& fl);

@@ -469,10 +469,66 @@ struct Lowerer {
 
 	/* The sink of an aggregation over pipeline pi's rows (visible columns in sc): global,
 	 * dense slots or a hash table (relalg_translator.cpp:380-656).  *vis = result columns. */
-	Sink make_agg_sink(const RelOpP& op, Scope& sc, int pi, int* vis) {
+	/* A sum whose bound leaves int64 (the reference types it i128, typing_pass.cpp:244-259)
+	 * becomes sums of bit chunks of its argument that each stay exact in int64: chunks
+	 * j < k-1 are the unsigned c-bit fields (v >> j*c) & (2^c - 1), the last is the signed
+	 * v >> (k-1)*c, and v is their sum shifted back (two's complement: v == sum over j of
+	 * chunk_j << j*c); c leaves room for `rows` additions.  Returns (chunk, shift) pairs. */
+	std::vector<std::pair<BExprP, int>> split_wide_sum(const BExprP& v, int64_t rows) {
+		const int L = bits_for((__int128)rows + 1);
+		const int c = std::max(1, 62 - L);
+		for (int k = 2; k <= 64; k++) {
+			std::vector<std::pair<BExprP, int>> parts;
+			bool fits = true;
+			for (int j = 0; j < k; j++) {
+				BExprP e = v;
+				if (j > 0) {
+					e = internal_fun("shr", e, j * c);
+				}
+				if (j + 1 < k) {
+					e = internal_fun("lowbits", e, c);
+				}
+				const Bounds sb = sum_bounds(e->b, rows);
+				fits = fits && sb.lo >= kI64Min && sb.hi <= kI64Max;
+				parts.push_back({e, j * c});
+			}
+			if (fits) {
+				return parts;
+			}
+		}
+		throw Error(kErrUnsupported, "sum cannot be split into int64 parts");
+	}
+
+	/* shr(x, s) = x >> s (arithmetic: floor(x / 2^s)), lowbits(x, b) = x & (2^b - 1) */
+	static BExprP internal_fun(const std::string& fn, const BExprP& x, int amount) {
+		auto c = std::make_shared<BExpr>();
+		c->kind = BExpr::Const;
+		c->cval = amount;
+		c->b.lo = c->b.hi = amount;
+		auto e = std::make_shared<BExpr>();
+		e->kind = BExpr::Fun;
+		e->fn = fn;
+		e->args = {x, c};
+		if (fn == "shr") {
+			const __int128 d = (__int128)1 << amount;
+			auto floordiv = [&](__int128 a) { return a >= 0 ? a / d : -((-a + d - 1) / d); };
+			e->b.lo = floordiv(x->b.lo);
+			e->b.hi = floordiv(x->b.hi);
+		} else {
+			const __int128 m = ((__int128)1 << amount) - 1;
+			const bool inside = x->b.lo >= 0 && x->b.hi <= m;
+			e->b.lo = inside ? x->b.lo : 0;
+			e->b.hi = inside ? x->b.hi : m;
+		}
+		return e;
+	}
+
+	Sink make_agg_sink(const RelOpP& op, Scope& sc, int pi, int* vis, bool allow_wide = false,
+		std::vector<OutCol>* outs = nullptr) {
 		Pipeline& p = out.pipes[pi];
 		Sink sink;
 		const int64_t rows = rows_bound(p);
+		std::vector<std::vector<int>> part_shifts; /* per plan aggregate: the shift of each sink part */
 		for (auto& k : op->exprs) {
 			BExprP e = bind(k, sc, p);
 			if (e->boolean) {
@@ -496,8 +552,21 @@ struct Lowerer {
 				if (ag.arg->boolean) {
 					throw Error(kErrUnsupported, "sum over a predicate is not supported");
 				}
-				check_range(sum_bounds(ag.arg->b, rows), "sum(...) over " + std::to_string(rows) + " rows");
+				const Bounds sb = sum_bounds(ag.arg->b, rows);
+				if (allow_wide && (sb.lo < kI64Min || sb.hi > kI64Max)) {
+					std::vector<int> shifts;
+					for (auto& pt : split_wide_sum(ag.arg, rows)) {
+						Sink::Agg pa;
+						pa.arg = pt.first;
+						sink.aggs.push_back(pa);
+						shifts.push_back(pt.second);
+					}
+					part_shifts.push_back(shifts);
+					continue;
+				}
+				check_range(sb, "sum(...) over " + std::to_string(rows) + " rows");
 			}
+			part_shifts.push_back({0});
 			sink.aggs.push_back(ag);
 		}
 		if (sink.count_idx < 0) {
@@ -558,6 +627,21 @@ struct Lowerer {
 			v += a.visible ? 1 : 0;
 		}
 		*vis = v;
+		if (outs) {
+			/* the caller's columns: keys, then each plan aggregate over its sink parts */
+			outs->clear();
+			int phys = 0;
+			for (size_t k = 0; k < sink.keys.size(); k++) {
+				outs->push_back(OutCol{{{phys++, 0}}});
+			}
+			for (size_t i = 0; i < op->aggregates.size(); i++) {
+				OutCol oc;
+				for (int sh : part_shifts[i]) {
+					oc.parts.push_back({phys++, sh});
+				}
+				outs->push_back(oc);
+			}
+		}
 		return sink;
 	}
 
@@ -573,7 +657,7 @@ struct Lowerer {
 		int pi = lower(op->left, sc);
 		name_counter += 2;
 		int vis = 0;
-		out.pipes[pi].sink = make_agg_sink(op, sc, pi, &vis);
+		out.pipes[pi].sink = make_agg_sink(op, sc, pi, &vis, true, &out.out_cols);
 		out.result_pipe = pi;
 		out.result_cols = vis;
 	}
@@ -701,6 +785,9 @@ struct Lowerer {
 		p.sink.groups_bound = rows_bound(p);
 		out.result_pipe = pi;
 		out.result_cols = (int)p.sink.outs.size();
+		for (int c = 0; c < out.result_cols; c++) {
+			out.out_cols.push_back(OutCol{{{c, 0}}});
+		}
 	}
 };
 

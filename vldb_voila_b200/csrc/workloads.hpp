@@ -10,6 +10,7 @@
  *   star       4-dimension probe chain + (year, region) group-by, SSB q4.1 shaped
  *              (db-engine-paradigms/src/benchmarks/sbb/queries/q41.cpp:21-46)
  *   batch      a seeded list of the first three with random sizes, selectivities and skews
+ *   bigsum     sums of 64-bit values that leave int64 (128-bit results)
  *
  * A workload is named by a spec string "<template>:key=value,...", e.g.
  * "join_aggr:build=1500000,probe=6000000,sel=0.2,seed=2".  Header-only C++ so that the
@@ -289,6 +290,23 @@ inline Workload make(const std::string& spec)
 		w.fact_rows = n;
 		w.algo_bytes = table_bytes(d) + table_bytes(c) + table_bytes(s) + table_bytes(pt) + table_bytes(f);
 		w.probe_bytes = table_bytes(f);
+	} else if (w.tmpl == "bigsum") {
+		/* sums whose bound leaves int64 (the reference types them i128): 64-bit values up to
+		 * +-2e15 (exact in a double, where the reference's min/max typing stays exact) grouped
+		 * by a 2-bit key; 10,000 of them per group already sum past 2^63 */
+		const int64_t n = param_i(p, "rows", 40000);
+		Table t{"fact", n, {}};
+		t.cols.push_back(make_col("g", VC_TYPE_U8, VC_GEN_UNIFORM, 0, 3, n, column_seed(seed, 0, 0)));
+		t.cols.push_back(make_col("v", VC_TYPE_I64, VC_GEN_UNIFORM, -2000000000000000ll, 2000000000000000ll, n,
+			column_seed(seed, 0, 1)));
+		t.cols.push_back(make_col("w", VC_TYPE_I64, VC_GEN_UNIFORM, 0, 2000000000000000ll, n, column_seed(seed, 0, 2)));
+		w.tables.push_back(t);
+		w.plan = "(aggr hash ((col fact.g)) ((fun sum (col fact.v)) (fun sum (col fact.w)) (fun count))"
+			" (scan fact (g v w)))";
+		w.fact_table = "fact";
+		w.fact_rows = n;
+		w.algo_bytes = table_bytes(t);
+		w.probe_bytes = w.algo_bytes;
 	} else {
 		throw std::invalid_argument("unknown workload template '" + w.tmpl + "'");
 	}

@@ -89,6 +89,8 @@ def _eval(e, frame, env):
     if head == "fun":
         f = _FUNS.get(e[1], e[1])
         a = [_eval(x, frame, env) for x in e[2:]]
+        if f == "extract_year":
+            return _julian_year(a[0])
         if f == "add":
             return a[0] + a[1]
         if f == "sub":
@@ -113,6 +115,19 @@ def _eval(e, frame, env):
             return a[0] | a[1]
         raise ValueError(f"unknown function {e[1]}")
     raise ValueError(f"bad expression {e}")
+
+
+def _julian_year(jd):
+    """Gregorian year of Julian day numbers, in the unsigned 32-bit steps of the reference's
+    splitJulianDay (runtime.hpp:128-148; the Calendar FAQ conversion)."""
+    u = np.uint64(0xffffffff)
+    a = (jd.astype(np.uint64) + np.uint64(32044)) & u
+    b = ((np.uint64(4) * a + np.uint64(3)) & u) // np.uint64(146097)
+    c = (a - ((np.uint64(146097) * b) & u) // np.uint64(4)) & u
+    d = ((np.uint64(4) * c + np.uint64(3)) & u) // np.uint64(1461)
+    e = (c - ((np.uint64(1461) * d) & u) // np.uint64(4)) & u
+    m = ((np.uint64(5) * e + np.uint64(2)) & u) // np.uint64(153)
+    return ((np.uint64(100) * b + d - np.uint64(4800) + m // np.uint64(10)) & u).astype(np.int64)
 
 
 def _check_int64(arrs):

@@ -58,6 +58,10 @@ HAVING_EMIT = ("(select (fun > (col aggr_ht1.aggr_0) (const 200))"
 WIDE_GLOBAL = ("(aggr global () ((fun sum (col fact.w)) (fun sum (col fact.v)) (fun count))"
                " (scan fact (v w)))")
 
+YEARS = ("(aggr hash ((col y) (col lineitem.l_returnflag)) ((fun sum (col lineitem.l_quantity)) (fun count))"
+         " (project ((assign y (fun extract_year (col lineitem.l_shipdate))) (col lineitem.l_returnflag)"
+         " (col lineitem.l_quantity)) (scan lineitem (l_shipdate l_returnflag l_quantity))))")
+
 CASES = [
     ("sel_aggr_1k", "sel_aggr:rows=1000,seed=11", None),
     ("sel_aggr_100k", "sel_aggr:rows=100000,seed=12", None),
@@ -83,6 +87,7 @@ CASES = [
     ("having_emit", "groupby:rows=20000,keys=3000,zipf=0.8,seed=73", HAVING_EMIT),
     ("wide_sums", "bigsum:rows=40000,seed=95", None),
     ("wide_global", "bigsum:rows=40000,seed=96", WIDE_GLOBAL),
+    ("extract_year", "sel_aggr:rows=30000,seed=57", YEARS),
 ]
 
 

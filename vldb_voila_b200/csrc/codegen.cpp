@@ -121,6 +121,9 @@ struct PipeGen {
 			static const std::map<std::string, std::string> ops = {
 				{"add", "+"}, {"sub", "-"}, {"mul", "*"}, {"lt", "<"}, {"le", "<="}, {"gt", ">"},
 				{"ge", ">="}, {"eq", "=="}, {"ne", "!="}, {"and", "&&"}, {"or", "||"}};
+			if (e->fn == "extract_year") {
+				return "((int64_t)vd::julian_year((uint32_t)(" + expr(e->args[0], v) + ")))";
+			}
 			if (e->fn == "shr") {
 				return "((int64_t)(" + expr(e->args[0], v) + ") >> " + std::to_string(e->args[1]->cval) + ")";
 			}

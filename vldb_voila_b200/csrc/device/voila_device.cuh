@@ -85,6 +85,19 @@ __device__ __forceinline__ uint64_t mix_hash64(uint64_t z)
 	return z ^ (z >> 31);
 }
 
+/* Gregorian year of a Julian day number (the Calendar FAQ conversion, as runtime.hpp:128-148
+ * computes it in unsigned 32-bit steps) */
+__device__ __forceinline__ uint32_t julian_year(uint32_t jd)
+{
+	const uint32_t a = jd + 32044u;
+	const uint32_t b = (4u * a + 3u) / 146097u;
+	const uint32_t c = a - (146097u * b) / 4u;
+	const uint32_t d = (4u * c + 3u) / 1461u;
+	const uint32_t e = c - (1461u * d) / 4u;
+	const uint32_t m = (5u * e + 2u) / 153u;
+	return 100u * b + d - 4800u + m / 10u;
+}
+
 /* product of two values whose ranges fit int32, as one 32x32->64 multiply */
 __device__ __forceinline__ int64_t mulw(int64_t a, int64_t b)
 {

@@ -144,6 +144,19 @@ RelOpP parse_plan(const std::string& text)
 static const __int128 kI64Max = (__int128)INT64_MAX;
 static const __int128 kI64Min = (__int128)INT64_MIN;
 
+/* Gregorian year of a Julian day number: the conversion of the Calendar FAQ (C. Tondering),
+ * in the unsigned 32-bit steps the reference uses (runtime.hpp:128-148) */
+static int64_t julian_year(int64_t jd)
+{
+	const uint32_t a = (uint32_t)jd + 32044u;
+	const uint32_t b = (4u * a + 3u) / 146097u;
+	const uint32_t c = a - (146097u * b) / 4u;
+	const uint32_t d = (4u * c + 3u) / 1461u;
+	const uint32_t e = c - (1461u * d) / 4u;
+	const uint32_t m = (5u * e + 2u) / 153u;
+	return (int64_t)(100u * b + d - 4800u + m / 10u);
+}
+
 static void check_range(const Bounds& b, const std::string& what)
 {
 	if (b.lo < kI64Min || b.hi > kI64Max) {
@@ -261,6 +274,24 @@ struct Lowerer {
 			throw Error(kErrInvalid, "assign is only allowed in a projection list");
 		case RelExpr::Fun:
 			break;
+		}
+		if (re->text == "extract_year") {
+			/* year of a date stored as its Julian day number (runtime.hpp:128-148); the
+			 * bounds are the years of the date bounds (the conversion is monotonic) */
+			if (re->args.size() != 1) {
+				throw Error(kErrInvalid, "extract_year takes one argument");
+			}
+			auto e = std::make_shared<BExpr>();
+			e->kind = BExpr::Fun;
+			e->fn = "extract_year";
+			e->args.push_back(bind(re->args[0], sc, p));
+			const Bounds& a = e->args[0]->b;
+			if (e->args[0]->boolean || a.lo < 0 || a.hi > 1000000000) {
+				throw Error(kErrUnsupported, "extract_year needs a day number in [0, 1e9]");
+			}
+			e->b.lo = julian_year((int64_t)a.lo);
+			e->b.hi = julian_year((int64_t)a.hi);
+			return e;
 		}
 		static const std::map<std::string, std::string> names = {
 			{"<=", "le"}, {"<", "lt"}, {">=", "ge"}, {">", "gt"}, {"=", "eq"}, {"!=", "ne"},

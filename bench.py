@@ -361,11 +361,55 @@ def main():
         d2h = res.nbytes + 16
         if i >= args.warmup:
             e2e_ms.append((t1 - t0) * 1e3)
-    e2e = statistics.mean(e2e_ms)
+    e2e_copy = statistics.mean(e2e_ms)
+
+    # e2e with host-resident columns: the same pinned buffers registered as the columns of a
+    # second engine, read in place by the kernels over PCIe (only the bytes a step touches
+    # cross the bus), and the result read back every step
+    engh = Engine(local)
+    for t, rows in w.tables.items():
+        engh.create_table(t, rows)
+    for c in w.columns:
+        engh.add_column(c.table, c.name, c.type, c.lo, c.hi)
+        t, n = pinned[(c.table, c.name)]
+        engh.attach_host(c.table, c.name, t.data_ptr())
+    qh = engh.query(w.plan, args.flavor)
+    e2eh_ms = []
+    for i in range(args.warmup + args.steps):
+        flush.fill_(i & 0xff)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        qh.run(stream)
+        resh = qh.result()
+        combine()
+        t1 = time.perf_counter()
+        if i >= args.warmup:
+            e2eh_ms.append((t1 - t0) * 1e3)
+    e2e_host = statistics.mean(e2eh_ms)
+    assert np.array_equal(np.sort(resh, axis=0), np.sort(q.result(), axis=0)), "host-resident result differs"
+    qh.close()
+    engh.close()
+    pcie = None
+    ppath = os.path.join(REPO, "profiles", "pcie.json")
+    if os.path.exists(ppath):
+        with open(ppath) as f:
+            pc = json.load(f).get(w.template)
+        if pc:
+            pcie = int(round(pc["read_bytes_per_fact_row"] * w.fact_rows))
     if world > 1:
-        tt = torch.tensor([e2e], dtype=torch.float64, device="cuda")
+        tt = torch.tensor([e2e_copy, e2e_host], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e = float(tt.item())
+        e2e_copy, e2e_host = float(tt[0].item()), float(tt[1].item())
+    e2e_modes = {
+        "copy": {"value": world * w.fact_rows / (e2e_copy / 1e3), "unit": "fact rows/s", "ms_per_step": e2e_copy,
+                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                 "mode": "every column copied from pinned host memory (cudaMemcpyAsync), then the query"},
+        "host_resident": {"value": world * w.fact_rows / (e2e_host / 1e3), "unit": "fact rows/s",
+                          "ms_per_step": e2e_host, "h2d_bytes_per_step": pcie if pcie is not None else h2d,
+                          "h2d_bytes_measured": pcie is not None, "d2h_bytes_per_step": d2h,
+                          "mode": "columns stay in pinned host memory; the kernels read what they need over PCIe"},
+    }
+    e2e_best = min(e2e_modes, key=lambda k: e2e_modes[k]["ms_per_step"])
 
     peaks = {}
     try:
@@ -413,8 +457,8 @@ def main():
             "config": {"workload": spec, "template": w.template, "fact_rows": w.fact_rows,
                        "flavor": info["flavor"], "l2": "flushed between timed steps (256 MiB write)",
                        "parallelism": f"dp{world}" if world > 1 else "single GPU"},
-            "e2e": {"value": world * w.fact_rows / (e2e / 1e3), "unit": "fact rows/s", "ms_per_step": e2e,
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": e2e_modes[e2e_best],
+            "e2e_modes": e2e_modes,
             "roofline": {"bound": "hbm", "kernel": kernels[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "basis": basis,
                          "algorithmic_bytes": w.probe_bytes,

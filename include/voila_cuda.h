@@ -49,6 +49,7 @@ extern "C" {
 #define VC_I16 2
 #define VC_I32 3
 #define VC_I64 4
+#define VC_STR 5 /* strings: 32-bit codes of the engine's string dictionary on the device */
 
 typedef struct vc_engine vc_engine;
 typedef struct vc_query vc_query;
@@ -81,6 +82,19 @@ int vc_table_drop(vc_engine* eng, const char* table);
  * its device storage. */
 int vc_column_add(vc_engine* eng, const char* table, const char* column, int type, int64_t lo, int64_t hi);
 
+/* Uploads a string column (VC_STR): row r is bytes[offsets[r], offsets[r+1]) (rows + 1
+ * offsets).  Strings are encoded into the engine's dictionary, shared by all its string
+ * columns so equal strings of different tables get equal codes (joins and group keys on
+ * strings compare codes); the column's domain becomes its codes' range.  Synchronous.
+ * Replaces the reference's varchar attributes (runtime.hpp:150-224). */
+int vc_column_upload_strings(vc_engine* eng, const char* table, const char* column, const char* bytes,
+	const int64_t* offsets, int64_t rows);
+
+/* Size of the engine's string dictionary, and the string of a code (string result columns
+ * hold codes in vc_query_result_copy; vc_query_result_text prints the strings). */
+int vc_dict_size(vc_engine* eng, int64_t* n);
+int vc_dict_string(vc_engine* eng, int64_t code, char* buf, size_t cap, size_t* len);
+
 /* A column's type, declared domain [lo, hi] and its table's row count (any pointer may be NULL). */
 int vc_column_info(vc_engine* eng, const char* table, const char* column, int32_t* type, int64_t* lo, int64_t* hi,
 	int64_t* rows);
@@ -97,6 +111,15 @@ int vc_column_download(vc_engine* eng, const char* table, const char* column, vo
 /* Uses caller-owned device memory (16-byte aligned, `rows` values) as the column; the
  * engine's own buffer is freed.  The memory must outlive every query that reads it. */
 int vc_column_attach(vc_engine* eng, const char* table, const char* column, void* device_ptr);
+
+/* Uses caller-owned pinned host memory (cudaHostAlloc / cudaHostRegister, 16-byte aligned,
+ * `rows` values) as the column: queries created afterwards read it in place over PCIe, so a
+ * step moves only the bytes its kernels touch (a probe chain gathers most columns only for
+ * the rows that survive its first probes) instead of copying whole columns first.  The memory
+ * must outlive every query that reads it; a later vc_column_attach makes the column
+ * device-resident again for queries created after it.  No counterpart in the reference, whose
+ * columns are host memory to begin with. */
+int vc_column_attach_host(vc_engine* eng, const char* table, const char* column, const void* host_ptr);
 
 /* Device address of the column's data. */
 int vc_column_device_ptr(vc_engine* eng, const char* table, const char* column, void** out);

@@ -4,6 +4,7 @@
  */
 #include "ref_plans.hpp"
 
+#include <cstring>
 #include <stdexcept>
 #include <thread>
 
@@ -102,6 +103,55 @@ static void fill(runtime::Attribute& attr, const vc_workload::Column& c, int64_t
 	attr = std::move(v);
 }
 
+/* A string column as the reference's varchar attribute: rows of a length byte and
+ * VC_GEN_STR_WIDTH - 1 characters (the layout varchar(data, idx, max_len) reads,
+ * runtime.hpp:192-204), the varchar views in attr.varchar_data that base-table scans use
+ * (runtime_struct.cpp:837-839), and MinMaxInfo with kVariableSize and max_len. */
+struct StrRow {
+	uint8_t len;
+	char chars[VC_GEN_STR_WIDTH - 1];
+};
+
+static void load_strings(runtime::Relation& rel, const vc_workload::Column& c, int64_t rows)
+{
+	std::vector<StrRow> v((size_t)rows);
+	char buf[VC_GEN_STR_WIDTH];
+	for (int64_t i = 0; i < rows; i++) {
+		const int n = vc_gen_string(&c.spec, i, buf);
+		StrRow& r = v[(size_t)i];
+		std::memset(&r, 0, sizeof(r));
+		r.len = (uint8_t)n;
+		std::memcpy(r.chars, buf, (size_t)n);
+	}
+	auto& attr = rel.insert(c.name, std::unique_ptr<algebra::Type>(new algebra::Varchar(VC_GEN_STR_WIDTH - 1)));
+	/* through the typed view: Attribute::operator= sizes its buffer for pointer-sized elements */
+	auto& vec = attr.typedAccessForChange<StrRow>();
+	vec.reset((size_t)rows);
+	for (auto& r : v) {
+		vec.push_back(r);
+	}
+	attr.varchar_data.reserve((size_t)rows);
+	for (int64_t i = 0; i < rows; i++) {
+		attr.varchar_data.emplace_back(varchar(attr.data(), (size_t)i, VC_GEN_STR_WIDTH - 1));
+	}
+	attr.minmax = new MinMaxInfo();
+	attr.minmax->lo = 0;
+	attr.minmax->hi = 0;
+	attr.minmax->max_len = VC_GEN_STR_WIDTH - 1;
+	attr.minmax->flags |= MinMaxInfo::kVariableSize;
+}
+
+/* FNV-1a (64-bit) of a string: a string column's contribution to the data checksum */
+static int64_t fnv1a(const char* s, size_t n)
+{
+	uint64_t h = UINT64_C(0xcbf29ce484222325);
+	for (size_t i = 0; i < n; i++) {
+		h ^= (unsigned char)s[i];
+		h *= UINT64_C(0x100000001b3);
+	}
+	return (int64_t)h;
+}
+
 size_t load_workload(runtime::Database& db, const vc_workload::Workload& w, int64_t max_rows, int threads)
 {
 	size_t values = 0;
@@ -121,6 +171,11 @@ size_t load_workload(runtime::Database& db, const vc_workload::Workload& w, int6
 			if (c.spec.kind == VC_GEN_ZIPF && c.spec.s != 0.0) {
 				cdf.resize((size_t)c.spec.b);
 				vc_gen_build_zipf_cdf(c.spec.s, c.spec.b, cdf.data());
+			}
+			if (c.spec.type == VC_TYPE_STR) {
+				load_strings(rel, c, rows);
+				values += (size_t)rows;
+				continue;
 			}
 			std::unique_ptr<algebra::Type> type;
 			switch (c.spec.type) {
@@ -157,6 +212,7 @@ uint64_t data_checksum(runtime::Database& db, const vc_workload::Workload& w)
 			for (size_t i = 0; i < rel.nrTuples; i++) {
 				int64_t v;
 				switch (c.spec.type) {
+				case VC_TYPE_STR: v = fnv1a(attr.varchar_data[i].arr, attr.varchar_data[i].len); break;
 				case VC_TYPE_U8: v = ((uint8_t*)attr.data())[i]; break;
 				case VC_TYPE_I64: v = ((int64_t*)attr.data())[i]; break;
 				default: v = ((int32_t*)attr.data())[i]; break;

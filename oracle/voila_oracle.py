@@ -81,7 +81,10 @@ class Frame:
 def _eval(e, frame, env):
     head = e[0]
     if head == "const":
-        return np.full(frame.n, int(e[1]), dtype=np.int64)
+        try:
+            return np.full(frame.n, int(e[1]), dtype=np.int64)
+        except ValueError:  # a string constant
+            return np.full(frame.n, e[1], dtype=object)
     if head == "col":
         if e[1] in env:
             return env[e[1]]
@@ -91,6 +94,8 @@ def _eval(e, frame, env):
         a = [_eval(x, frame, env) for x in e[2:]]
         if f == "extract_year":
             return _julian_year(a[0])
+        if f == "contains":  # substring test (runtime.hpp:150-224)
+            return np.fromiter((p in x for x, p in zip(a[0], a[1])), dtype=bool, count=frame.n)
         if f == "add":
             return a[0] + a[1]
         if f == "sub":
@@ -136,6 +141,16 @@ def _check_int64(arrs):
     for a in arrs:
         if a.dtype == np.int64 and a.size and (a.max() > 2**62 or a.min() < -2**62):
             raise OverflowError("oracle value range close to int64 limits")
+
+
+def _column(a):
+    """A base column: int64 values, or Python strings (object array) for a string column."""
+    a = np.asarray(a)
+    return a if a.dtype == object else a.astype(np.int64)
+
+
+def _py(x):
+    return x if isinstance(x, str) else int(x)
 
 
 def _exact(v):
@@ -193,7 +208,9 @@ def _aggregate(node, f):
         return [np.zeros(0, dtype=np.int64) for _ in keys], [np.zeros(0, dtype=np.int64) for _ in aggs]
     if glob:
         return [], [np.array([f.n if kind == "count" else _exact(v).sum()], dtype=object) for kind, v in aggs]
-    stacked = np.stack(keys, axis=1)
+    # keys as integer codes per column (strings too), grouped on the stacked codes
+    enc = [np.unique(k, return_inverse=True) for k in keys]
+    stacked = np.stack([inv.reshape(-1) for _, inv in enc], axis=1)
     uniq, inv = np.unique(stacked, axis=0, return_inverse=True)
     inv = inv.reshape(-1)
     order = np.argsort(inv, kind="stable")
@@ -205,7 +222,7 @@ def _aggregate(node, f):
             out.append(counts.astype(np.int64))
         else:
             out.append(np.add.reduceat(_exact(v)[order], bounds))
-    return [uniq[:, i].astype(np.int64) for i in range(uniq.shape[1])], out
+    return [enc[i][0][uniq[:, i]] for i in range(uniq.shape[1])], out
 
 
 def _op(node, db, names=None):
@@ -221,7 +238,7 @@ def _op(node, db, names=None):
         return Frame(cols, len(aggs[0]) if aggs else (len(keys[0]) if keys else 0))
     if head == "scan":
         table = node[1]
-        cols = [(f"{table}.{c}", np.asarray(db[table][c]).astype(np.int64)) for c in node[2]]
+        cols = [(f"{table}.{c}", _column(db[table][c])) for c in node[2]]
         n = len(cols[0][1]) if cols else 0
         return Frame(cols, n)
     if head == "select":
@@ -283,12 +300,12 @@ def run_plan(plan, db):
     names = _aggr_names(node)
     if node[0] != "aggr":
         f = _op(node, db, names)
-        return [tuple(int(v[i]) for _, v in f.cols) for i in range(f.n)]
+        return [tuple(_py(v[i]) for _, v in f.cols) for i in range(f.n)]
     f = _op(node[4], db, names)
     keys, aggs = _aggregate(node, f)
     cols = keys + aggs
     n = len(cols[0]) if cols else 0
-    return [tuple(int(c[i]) for c in cols) for i in range(n)]
+    return [tuple(_py(c[i]) for c in cols) for i in range(n)]
 
 
 def result_lines(rows):

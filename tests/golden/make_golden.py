@@ -62,6 +62,12 @@ YEARS = ("(aggr hash ((col y) (col lineitem.l_returnflag)) ((fun sum (col lineit
          " (project ((assign y (fun extract_year (col lineitem.l_shipdate))) (col lineitem.l_returnflag)"
          " (col lineitem.l_quantity)) (scan lineitem (l_shipdate l_returnflag l_quantity))))")
 
+# string columns: a string equality filter emitting strings, and string group keys
+STR_EMIT = ("(select (fun and (fun = (col part.p_brand) (const coral)) (fun contains (col part.p_name) (const red)))"
+            " (scan part (p_partkey p_name p_brand)))")
+STR_GROUP = ("(aggr hash ((col part.p_name)) ((fun count)) (select (fun != (col part.p_brand) (const amber))"
+             " (scan part (p_name p_brand))))")
+
 CASES = [
     ("sel_aggr_1k", "sel_aggr:rows=1000,seed=11", None),
     ("sel_aggr_100k", "sel_aggr:rows=100000,seed=12", None),
@@ -88,6 +94,9 @@ CASES = [
     ("wide_sums", "bigsum:rows=40000,seed=95", None),
     ("wide_global", "bigsum:rows=40000,seed=96", WIDE_GLOBAL),
     ("extract_year", "sel_aggr:rows=30000,seed=57", YEARS),
+    ("strings_contains", "strings:rows=50000,parts=3000,seed=58", None),
+    ("strings_emit", "strings:rows=1000,parts=4000,seed=59", STR_EMIT),
+    ("strings_group", "strings:rows=1000,parts=5000,seed=60", STR_GROUP),
 ]
 
 

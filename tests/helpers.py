@@ -25,13 +25,23 @@ def _mix64(z):
     return z ^ (z >> np.uint64(31))
 
 
+def _fnv1a(b):
+    h = 0xcbf29ce484222325
+    for x in b:
+        h = ((h ^ x) * 0x100000001b3) & 0xffffffffffffffff
+    return h
+
+
 def data_checksum(w, data):
     """Same order-insensitive checksum the reference harness prints (oracle/ref/ref_data.cpp)."""
     total = np.uint64(0)
     with np.errstate(over="ignore"):
         for ti, t in enumerate(w.tables):
             for ci, c in enumerate(w.table_columns(t)):
-                v = data[t][c.name].astype(np.int64).view(np.uint64)
+                a = data[t][c.name]
+                if a.dtype == object:  # strings: FNV-1a of their bytes, as the reference harness
+                    a = np.array([_fnv1a(x.encode()) for x in a], dtype=np.uint64).view(np.int64)
+                v = a.astype(np.int64).view(np.uint64)
                 i = np.arange(len(v), dtype=np.uint64)
                 x = v * np.uint64(31) + i * np.uint64(1000003) + np.uint64(ti * 131) + np.uint64(ci)
                 total = total + _mix64(x).sum(dtype=np.uint64)

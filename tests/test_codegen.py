@@ -199,7 +199,7 @@ def test_join_n_plans_compile(flavor):
     w, e = offline("star:rows=1000,custs=50")
     q = e.query(JOIN_N_PLAN, flavor)
     src = q.source()
-    assert "__any_sync" in src and "VD_MAX_PROBES * SPB" in src
+    assert "__any_sync" in src and "1ull) * SPB" in src  # the match loop may walk the whole table
     assert "vd::dense_test" not in src
 
 

@@ -38,6 +38,7 @@ static const char* ctype(int t)
 	case VC_TYPE_U8: return "uint8_t";
 	case VC_TYPE_I16: return "int16_t";
 	case VC_TYPE_I32: return "int32_t";
+	case VC_TYPE_STR: return "int32_t"; /* dictionary codes */
 	default: return "int64_t";
 	}
 }
@@ -121,6 +122,11 @@ struct PipeGen {
 			static const std::map<std::string, std::string> ops = {
 				{"add", "+"}, {"sub", "-"}, {"mul", "*"}, {"lt", "<"}, {"le", "<="}, {"gt", ">"},
 				{"ge", ">="}, {"eq", "=="}, {"ne", "!="}, {"and", "&&"}, {"or", "||"}};
+			if (e->fn == "inset") {
+				const CodeBitmap& bm = plan.bitmaps[(size_t)e->aux];
+				return "vd::code_in(" + Pptr(bm.dev, "const unsigned*") + ", (int64_t)(" + expr(e->args[0], v) + ") - " +
+					P((unsigned long long)bm.lo) + ", " + P((unsigned long long)(bm.bits.size() * 32)) + ")";
+			}
 			if (e->fn == "extract_year") {
 				return "((int64_t)vd::julian_year((uint32_t)(" + expr(e->args[0], v) + ")))";
 			}
@@ -324,7 +330,11 @@ struct PipeGen {
 		for (size_t c = 0; c < p.cols.size(); c++) {
 			any_eager = any_eager || eager[c];
 		}
-		const bool tma = fl.load == "tma" && any_eager && !item;
+		bool any_host = false; /* bulk copies do not read host-resident columns */
+		for (auto& pc : p.cols) {
+			any_host = any_host || pc.host;
+		}
+		const bool tma = fl.load == "tma" && any_eager && !item && !any_host;
 		if (tma) {
 			emit_pdl_wait();
 			gen_tma_loop();
@@ -557,7 +567,8 @@ struct PipeGen {
 				o << "    vd::load_rows_smem<" << ct << ", " << V << ">((const " << ct << "*)(stage + " << tile_region(c)
 				  << ") + threadIdx.x * " << V << ", " << dst << c << ");\n";
 			} else {
-				o << "    vd::load_rows<" << ct << ", " << V << ">(c" << c << ", " << r0 << ", n, " << dst << c << ");\n";
+				o << "    vd::load_rows<" << ct << ", " << V << (p.cols[c].host ? ", true" : "") << ">(c" << c << ", " << r0
+				  << ", n, " << dst << c << ");\n";
 			}
 		}
 	}
@@ -574,17 +585,35 @@ struct PipeGen {
 		}
 	}
 
+	/* lazy gathers (the compaction flush): column c is loaded before op lazy_first_use[c] */
+	bool lazy_rows = false;
+	std::vector<int> lazy_first_use;
+
+	void emit_lazy_loads(int at) {
+		if (!lazy_rows) {
+			return;
+		}
+		for (size_t c = 0; c < p.cols.size(); c++) {
+			if (lazy_first_use[c] == at) {
+				o << "      if (act[0]) { x" << c << "[0] = vd::load_one<" << ctype(p.cols[c].type) << (p.cols[c].host ? ", true" : "")
+				  << ">(c" << c << ", row); }\n";
+			}
+		}
+	}
+
 	/* ops [from, end) and the sink; a JoinN probe turns the rest of the pipeline into the body
 	 * of its loop over matches */
 	void emit_rest(int from) {
 		for (int i = from; i < (int)p.ops.size(); i++) {
 			const Op& op = p.ops[i];
+			emit_lazy_loads(i);
 			if (op.kind == Op::Probe && !plan.joins[op.join].join01) {
 				gen_probe_n(i, op);
 				return;
 			}
 			emit_ops(i, i + 1);
 		}
+		emit_lazy_loads((int)p.ops.size());
 		sink_row();
 	}
 
@@ -622,7 +651,7 @@ struct PipeGen {
 			  << ")[1];\n";
 		}
 		o << "      constexpr int SPB" << j << " = vd::slots_per_bucket<" << S << ">();\n";
-		o << "      uint64_t nb" << j << "[" << V << "]; int ns" << j << "[" << V << "]; int ng" << j << "[" << V << "]; "
+		o << "      uint64_t nb" << j << "[" << V << "]; int ns" << j << "[" << V << "]; uint64_t ng" << j << "[" << V << "]; "
 		  << KT << " nk" << j << "[" << V << "]; bool np" << j << "[" << V << "];\n";
 		o << "#pragma unroll\n      for (int v = 0; v < " << V << "; v++) {\n";
 		std::string inrange = "act[v]";
@@ -652,7 +681,8 @@ struct PipeGen {
 		o << "          uint64_t raw = 0;\n";
 		o << "          act[v] = false;\n";
 		o << "          while (np" << j << "[v]) {\n";
-		o << "            if (++ng" << j << "[v] > VD_MAX_PROBES * SPB" << j << ") { atomicOr(err, VD_ERR_TABLE_FULL); np" << j
+		/* duplicates cluster: a probe may walk the whole table, which always holds a free slot */
+		o << "            if (++ng" << j << "[v] > (bmask" << j << " + 1ull) * SPB" << j << ") { atomicOr(err, VD_ERR_TABLE_FULL); np" << j
 		  << "[v] = false; break; }\n";
 		o << "            const " << S << "* sp = jt" << j << " + nb" << j << "[v] * SPB" << j << " + ns" << j << "[v];\n";
 		o << "            const " << KT << " sk = vd::table_ld(&sp->key);\n";
@@ -723,15 +753,41 @@ struct PipeGen {
 		const int saveV = V;
 		V = 1;
 		o << "      bool act[1] = {live};\n";
+		/* every column is gathered just before the first op (or the sink) that reads it, and
+		 * only for rows still alive there: a row that fails a probe never touches the columns
+		 * of the later ones */
+		lazy_first_use.assign(p.cols.size(), INT32_MAX);
+		for (size_t i = compact_at + 1; i < p.ops.size(); i++) {
+			std::vector<bool> used(p.cols.size(), false);
+			if (p.ops[i].pred) cols_of(p.ops[i].pred, used);
+			for (auto& k : p.ops[i].keys) cols_of(k, used);
+			for (size_t c = 0; c < p.cols.size(); c++) {
+				if (used[c] && lazy_first_use[c] == INT32_MAX) {
+					lazy_first_use[c] = (int)i;
+				}
+			}
+		}
+		{
+			std::vector<bool> used(p.cols.size(), false);
+			for (auto& e : sink_exprs()) cols_of(e, used);
+			for (size_t c = 0; c < p.cols.size(); c++) {
+				if (used[c] && lazy_first_use[c] == INT32_MAX) {
+					lazy_first_use[c] = (int)p.ops.size();
+				}
+			}
+		}
 		for (size_t c = 0; c < p.cols.size(); c++) {
-			const char* ct = ctype(p.cols[c].type);
-			o << "      " << ct << " x" << c << "[1] = {live ? vd::load_one(c" << c << ", row) : (" << ct << ")0};\n";
+			if (lazy_first_use[c] != INT32_MAX) {
+				o << "      " << ctype(p.cols[c].type) << " x" << c << "[1] = {0};\n";
+			}
 		}
 		for (size_t k = 0; k < carried.size(); k++) {
 			o << "      int64_t pay" << carried[k].first << "_" << carried[k].second << "[1] = {live ? ccar" << k
 			  << "[ci] : 0};\n";
 		}
+		lazy_rows = true;
 		emit_rest(compact_at + 1);
+		lazy_rows = false;
 		V = saveV;
 		o << "    }\n";
 		o << "    vd::block_sync();\n";
@@ -1120,7 +1176,7 @@ struct PipeGen {
 				o << "      if (act[v]) {\n";
 				o << "        const uint64_t pkb = " << pk << ";\n";
 				o << "        vd::join_insert(jt, bmask, " << table_hash(s.keys, "pkb", jd.key_bits, "v") << ", (" << KT
-				  << ")(pkb + 1ull), (" << PT << ")(" << pp << "), err);\n";
+				  << ")(pkb + 1ull), (" << PT << ")(" << pp << "), err" << (jd.join01 ? "" : ", bmask + 1ull") << ");\n";
 				o << "      }\n    }\n";
 			} else {
 				o << "      const int64_t pos = vd::block_append(&words[0], act[v], app);\n";
@@ -1289,7 +1345,8 @@ struct PipeGen {
 		k << "  const uint64_t cnt = words[0];\n";
 		k << "  const uint64_t bmask = vd::join_buckets<" << S << ">(cnt) - 1;\n";
 		k << "  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (uint64_t)gridDim.x * blockDim.x) {\n";
-		k << "    vd::join_insert(jt, bmask, shash[i], skeys[i], spay[i], err);\n  }\n}\n\n";
+		k << "    vd::join_insert(jt, bmask, shash[i], skeys[i], spay[i], err" << (jd.join01 ? "" : ", bmask + 1ull")
+		  << ");\n  }\n}\n\n";
 		return k.str();
 	}
 
@@ -1316,41 +1373,46 @@ struct PipeGen {
 		k << "  " << K << "* const gkeys = " << Pptr(st.sink_dev, K + "*") << ";\n";
 		k << "  unsigned long long* const gacc = " << Pptr(st.sink_acc, "unsigned long long*") << ";\n";
 		k << "  const int64_t nslots = " << P((unsigned long long)st.sink_cap) << ";\n";
-		/* each warp covers kExtractK groups of 32 slots per step: all their keys are loaded
-		 * (from L2, coherent) before any is used */
+		/* a block takes chunks of blockDim.x * kExtractK slots (slot q * blockDim.x + thread of
+		 * the chunk); all keys of a chunk are loaded (from L2, coherent) before any is used, and
+		 * the chunk's result rows are reserved with one atomic */
+		k << "  __shared__ unsigned long long xres[33];\n";
+		k << "  const int64_t chunk = (int64_t)blockDim.x * " << kExtractK << ";\n";
 		if (item) {
-			/* one item = slot groups [t_begin, t_end) of blockDim.x * kExtractK slots */
-			k << "  const int64_t stride = (int64_t)blockDim.x * " << kExtractK << ";\n";
-			k << "  const int64_t slim = t_end * stride < nslots ? t_end * stride : nslots;\n";
-			k << "  for (int64_t base = t_begin * stride + (int64_t)(threadIdx.x & ~31) * " << kExtractK
-			  << "; base < slim; base += stride) {\n";
+			/* one item = chunks [t_begin, t_end) */
+			k << "  const int64_t clim = (nslots + chunk - 1) / chunk;\n";
+			k << "  for (int64_t ch = t_begin; ch < (t_end < clim ? t_end : clim); ch++) {\n";
 		} else {
-			k << "  const int64_t stride = (int64_t)gridDim.x * blockDim.x * " << kExtractK << ";\n";
-			k << "  for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * " << kExtractK
-			  << "; base < nslots; base += stride) {\n";
+			k << "  for (int64_t ch = blockIdx.x; ch * chunk < nslots; ch += gridDim.x) {\n";
 		}
+		k << "    const int64_t cb = ch * chunk;\n";
 		k << "    " << K << " kw[" << kExtractK << "];\n";
 		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
-		k << "      const int64_t i = base + q * 32 + (threadIdx.x & 31);\n";
+		k << "      const int64_t i = cb + (int64_t)q * blockDim.x + threadIdx.x;\n";
 		k << "      kw[q] = i < nslots ? __ldcg(&gkeys[i]) : (" << K << ")0;\n";
 		k << "    }\n";
-		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
-		k << "    const int64_t i = base + q * 32 + (threadIdx.x & 31);\n";
-		k << "    uint64_t w[" << W << "];\n";
-		k << "#pragma unroll\n    for (int a = 0; a < " << W << "; a++) { w[a] = kw[q] != 0 ? __ldcg(&gacc[i * " << W
-		  << " + a]) : 0ull; }\n";
+		k << "    uint64_t w[" << kExtractK << "][" << W << "];\n";
+		k << "    bool take[" << kExtractK << "];\n    int ntake = 0;\n";
 		auto field = [&](int a) {
 			const int bits = s.agg_bits[a];
 			const unsigned long long mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
-			return "((w[" + std::to_string(s.agg_word[a]) + "] >> " + std::to_string(s.agg_shift[a]) + ") & " +
+			return "((w[q][" + std::to_string(s.agg_word[a]) + "] >> " + std::to_string(s.agg_shift[a]) + ") & " +
 				std::to_string(mask) + "ull)";
 		};
-		k << "    const int64_t cnt = (int64_t)" << field(s.count_idx) << ";\n";
-		k << "    const bool take = kw[q] != 0 && cnt > 0;\n";
-		k << "    if (kw[q] != 0) {\n      gkeys[i] = 0;\n";
-		k << "#pragma unroll\n      for (int a = 0; a < " << W << "; a++) { gacc[i * " << W << " + a] = 0ull; }\n    }\n";
-		k << "    const int64_t pos = vd::warp_append(ocount, take);\n";
-		k << "    if (take && pos < ocap) {\n";
+		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
+		k << "      const int64_t i = cb + (int64_t)q * blockDim.x + threadIdx.x;\n";
+		k << "#pragma unroll\n      for (int a = 0; a < " << W << "; a++) { w[q][a] = kw[q] != 0 ? __ldcg(&gacc[i * " << W
+		  << " + a]) : 0ull; }\n";
+		k << "      take[q] = kw[q] != 0 && (int64_t)" << field(s.count_idx) << " > 0;\n";
+		k << "      ntake += take[q] ? 1 : 0;\n";
+		k << "      if (kw[q] != 0) {\n        gkeys[i] = 0;\n";
+		k << "#pragma unroll\n        for (int a = 0; a < " << W << "; a++) { gacc[i * " << W << " + a] = 0ull; }\n      }\n";
+		k << "    }\n";
+		k << "    int64_t pos = vd::block_reserve(ocount, ntake, xres);\n";
+		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
+		k << "    if (take[q]) {\n";
+		k << "    if (pos < ocap) {\n";
+		k << "      const int64_t cnt = (int64_t)" << field(s.count_idx) << ";\n";
 		int col = 0;
 		for (size_t kk = 0; kk < s.keys.size(); kk++, col++) {
 			const std::string lo = P((unsigned long long)(int64_t)s.keys[kk]->b.lo);
@@ -1372,7 +1434,7 @@ struct PipeGen {
 			}
 			col++;
 		}
-		k << "    }\n    }\n  }\n}\n\n";
+		k << "    }\n    pos++;\n    }\n    }\n  }\n}\n\n";
 		return k.str();
 	}
 };

@@ -30,8 +30,12 @@ enum {
 	VC_TYPE_U8 = 1,
 	VC_TYPE_I16 = 2,
 	VC_TYPE_I32 = 3,
-	VC_TYPE_I64 = 4
+	VC_TYPE_I64 = 4,
+	VC_TYPE_STR = 5 /* variable-length string; on the device a 32-bit dictionary code */
 };
+
+/* longest generated string (host output rows are VC_GEN_STR_WIDTH bytes, NUL-padded) */
+#define VC_GEN_STR_WIDTH 32
 
 /* generator kinds */
 enum {
@@ -41,7 +45,8 @@ enum {
 	VC_GEN_ZIPF = 3,    /* key in [1, b] with P(k) ~ k^-s; s == 0 means uniform */
 	VC_GEN_CHOICE = 4,  /* one of b byte values packed little-endian into a (b <= 8) */
 	VC_GEN_DIV = 5,     /* a + (row * c) / b */
-	VC_GEN_MOD = 6      /* a + row % b */
+	VC_GEN_MOD = 6,     /* a + row % b */
+	VC_GEN_WORDS = 7    /* a words (1..4) drawn from the first b (1..24) of a word list, space-separated */
 };
 
 typedef struct vc_gen_spec {
@@ -148,7 +153,7 @@ VC_GEN_FN int64_t vc_gen_value(const vc_gen_spec* spec, const double* zipf_cdf, 
 
 VC_GEN_FN int vc_gen_type_size(int32_t type)
 {
-	return type == VC_TYPE_U8 ? 1 : type == VC_TYPE_I16 ? 2 : type == VC_TYPE_I32 ? 4 : 8;
+	return type == VC_TYPE_U8 ? 1 : type == VC_TYPE_I16 ? 2 : (type == VC_TYPE_I32 || type == VC_TYPE_STR) ? 4 : 8;
 }
 
 VC_GEN_FN void vc_gen_store(int32_t type, void* out, int64_t i, int64_t v)
@@ -163,6 +168,31 @@ VC_GEN_FN void vc_gen_store(int32_t type, void* out, int64_t i, int64_t v)
 
 #if !defined(__CUDACC_RTC__) && !defined(__CUDA_ARCH__)
 #include <math.h>
+#include <string.h>
+
+/* String of row `row` of a VC_GEN_WORDS column, NUL-terminated, at most VC_GEN_STR_WIDTH - 1
+ * characters; returns its length.  Host only: strings are dictionary-encoded when uploaded. */
+static inline int vc_gen_string(const vc_gen_spec* spec, int64_t row, char* out)
+{
+	static const char* const words[24] = {"amber", "azure", "beige", "black", "blue", "coral", "cream", "cyan",
+		"gold", "green", "grey", "indigo", "ivory", "khaki", "lime", "navy", "olive", "orange", "pink", "plum",
+		"red", "rose", "tan", "white"};
+	const uint64_t bits = vc_gen_bits(spec->seed, (uint64_t)row);
+	const int64_t nwords = spec->a < 1 ? 1 : (spec->a > 4 ? 4 : spec->a);
+	const uint64_t choices = (uint64_t)(spec->b < 1 ? 1 : (spec->b > 24 ? 24 : spec->b));
+	int len = 0;
+	for (int64_t j = 0; j < nwords; j++) {
+		const char* w = words[((bits >> (16 * j)) & 0xffff) % choices];
+		const int wl = (int)strlen(w);
+		if (j) {
+			out[len++] = ' ';
+		}
+		memcpy(out + len, w, (size_t)wl);
+		len += wl;
+	}
+	out[len] = 0;
+	return len;
+}
 /*
  * Inverse-CDF table for VC_GEN_ZIPF: cdf[k-1] = sum_{j<=k} j^-s / sum_{j<=n} j^-s.
  * Host only; the device generator receives the finished table.  Built with one left-to-right

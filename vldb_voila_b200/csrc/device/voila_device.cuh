@@ -98,6 +98,12 @@ __device__ __forceinline__ uint32_t julian_year(uint32_t jd)
 	return 100u * b + d - 4800u + m / 10u;
 }
 
+/* whether code offset i is in a code set (a bitmap of n bits) */
+__device__ __forceinline__ bool code_in(const unsigned* __restrict__ bits, int64_t i, int64_t n)
+{
+	return (uint64_t)i < (uint64_t)n && ((__ldg(&bits[i >> 5]) >> (unsigned)(i & 31)) & 1u) != 0u;
+}
+
 /* product of two values whose ranges fit int32, as one 32x32->64 multiply */
 __device__ __forceinline__ int64_t mulw(int64_t a, int64_t b)
 {
@@ -109,7 +115,19 @@ __device__ __forceinline__ int64_t mulw(int64_t a, int64_t b)
 /* Loads rows [r0, r0+V) of a column into registers.  Whole tiles use vector loads through
  * the read-only path (the column base is 16-byte aligned and r0 is a multiple of V);
  * the ragged tail falls back to bounds-checked scalar loads. */
-template <typename T, int V>
+/* One read of column data: through the read-only path from HBM, or a coherent L2 load
+ * (ld.global.cg) from a column that lives in pinned host memory (SYS). */
+template <bool SYS, typename T>
+__device__ __forceinline__ T col_ld(const T* p)
+{
+	if constexpr (SYS) {
+		return __ldcg(p);
+	} else {
+		return __ldg(p);
+	}
+}
+
+template <typename T, int V, bool SYS = false>
 __device__ __forceinline__ void load_rows(const T* __restrict__ col, int64_t r0, int64_t n, T (&out)[V])
 {
 	constexpr int bytes = V * (int)sizeof(T);
@@ -119,20 +137,20 @@ __device__ __forceinline__ void load_rows(const T* __restrict__ col, int64_t r0,
 			uint4 tmp[bytes / 16];
 #pragma unroll
 			for (int i = 0; i < bytes / 16; i++) {
-				tmp[i] = __ldg(reinterpret_cast<const uint4*>(p) + i);
+				tmp[i] = col_ld<SYS>(reinterpret_cast<const uint4*>(p) + i);
 			}
 #pragma unroll
 			for (int i = 0; i < V; i++) {
 				out[i] = reinterpret_cast<const T*>(tmp)[i];
 			}
 		} else if constexpr (bytes == 8) {
-			uint2 tmp = __ldg(reinterpret_cast<const uint2*>(p));
+			uint2 tmp = col_ld<SYS>(reinterpret_cast<const uint2*>(p));
 #pragma unroll
 			for (int i = 0; i < V; i++) {
 				out[i] = reinterpret_cast<const T*>(&tmp)[i];
 			}
 		} else if constexpr (bytes == 4) {
-			unsigned int tmp = __ldg(reinterpret_cast<const unsigned int*>(p));
+			unsigned int tmp = col_ld<SYS>(reinterpret_cast<const unsigned int*>(p));
 #pragma unroll
 			for (int i = 0; i < V; i++) {
 				out[i] = reinterpret_cast<const T*>(&tmp)[i];
@@ -140,21 +158,21 @@ __device__ __forceinline__ void load_rows(const T* __restrict__ col, int64_t r0,
 		} else {
 #pragma unroll
 			for (int i = 0; i < V; i++) {
-				out[i] = __ldg(p + i);
+				out[i] = col_ld<SYS>(p + i);
 			}
 		}
 	} else {
 #pragma unroll
 		for (int i = 0; i < V; i++) {
-			out[i] = (r0 + i < n) ? __ldg(col + r0 + i) : (T)0;
+			out[i] = (r0 + i < n) ? col_ld<SYS>(col + r0 + i) : (T)0;
 		}
 	}
 }
 
-template <typename T>
+template <typename T, bool SYS = false>
 __device__ __forceinline__ T load_one(const T* __restrict__ col, int64_t row)
 {
-	return __ldg(col + row);
+	return col_ld<SYS>(col + row);
 }
 
 /* Reads this thread's V consecutive rows of a column tile staged in shared memory. */
@@ -398,6 +416,39 @@ __device__ __forceinline__ int64_t block_append(unsigned long long* cursor, bool
 	}
 	block_sync();
 	const int64_t pos = (int64_t)(scratch[32] + scratch[warp]) + __popc(mask & ((1u << lane) - 1u));
+	block_sync();
+	return pos;
+}
+
+/* Reserves `cnt` consecutive output positions per thread with one atomic per block: returns
+ * this thread's first position (threads in order).  All threads call it; `scratch` holds 33
+ * words of shared memory. */
+__device__ __forceinline__ int64_t block_reserve(unsigned long long* cursor, int cnt, unsigned long long* scratch)
+{
+	const unsigned lane = lane_id(), warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+	int x = cnt;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const int y = __shfl_up_sync(0xffffffffu, x, o);
+		if ((int)lane >= o) {
+			x += y;
+		}
+	}
+	if (lane == 31) {
+		scratch[warp] = (unsigned long long)x;
+	}
+	block_sync();
+	if (threadIdx.x == 0) {
+		unsigned long long run = 0;
+		for (unsigned w = 0; w < nw; w++) {
+			const unsigned long long c = scratch[w];
+			scratch[w] = run;
+			run += c;
+		}
+		scratch[32] = run ? atomicAdd(cursor, run) : 0ull;
+	}
+	block_sync();
+	const int64_t pos = (int64_t)(scratch[32] + scratch[warp]) + x - cnt;
 	block_sync();
 	return pos;
 }
@@ -679,13 +730,16 @@ __device__ __forceinline__ int join_probe_bucket(const JoinSlot<KeyT, PayT>* __r
 	return 2;
 }
 
+/* Inserts into the first free slot of the key's probe sequence.  A table keeps its load at
+ * most one half, so a sequence of bucket_mask + 1 buckets always meets a free slot: JoinN
+ * tables (duplicate keys cluster) pass that as max_probes, Join01 tables VD_MAX_PROBES. */
 template <typename KeyT, typename PayT>
 __device__ __forceinline__ bool join_insert(JoinSlot<KeyT, PayT>* __restrict__ slots, uint64_t bucket_mask,
-	uint64_t h, KeyT key, PayT pay, unsigned* err)
+	uint64_t h, KeyT key, PayT pay, unsigned* err, uint64_t max_probes = VD_MAX_PROBES)
 {
 	constexpr int SPB = slots_per_bucket<JoinSlot<KeyT, PayT>>();
 	uint64_t b = h & bucket_mask;
-	for (int probe = 0; probe < VD_MAX_PROBES; probe++) {
+	for (uint64_t probe = 0; probe < max_probes; probe++) {
 		JoinSlot<KeyT, PayT>* bucket = slots + b * SPB;
 #pragma unroll
 		for (int s = 0; s < SPB; s++) {

@@ -257,7 +257,7 @@ void query_prepare(Query& q)
 		VC_CHECK_CUDA(cudaSetDevice(e.device));
 	}
 	RelOpP root = parse_plan(q.plan_text);
-	q.plan = lower_plan(root, e.tables, q.flavor);
+	q.plan = lower_plan(root, e.tables, q.flavor, e.dict);
 	LoweredPlan& plan = q.plan;
 	QueryState& st = state_of(q);
 	st.pipes.assign(plan.pipes.size(), PipeDeviceState());
@@ -277,6 +277,14 @@ void query_prepare(Query& q)
 	};
 	q.err = (unsigned*)arena_take(8);
 	q.out_count = (unsigned long long*)arena_take(8);
+	/* code sets of `contains` predicates */
+	for (auto& bm : plan.bitmaps) {
+		const size_t bytes = bm.bits.size() * sizeof(uint32_t);
+		bm.dev = dev_alloc(q, bytes);
+		if (!e.offline) {
+			VC_CHECK_CUDA(cudaMemcpy(bm.dev, bm.bits.data(), bytes, cudaMemcpyHostToDevice));
+		}
+	}
 
 	for (auto& jd : plan.joins) {
 		const int64_t rows = std::max<int64_t>(jd.build_rows, 1);
@@ -667,7 +675,15 @@ std::string query_result_text(Query& q)
 			if (c) {
 				s.push_back('|');
 			}
-			append_i128(s, result_value(q, c, r));
+			const __int128 v = result_value(q, c, r);
+			if (q.plan.out_cols[(size_t)c].str) {
+				if (v < 0 || v >= (__int128)q.eng->dict.strings.size()) {
+					throw Error(3, "a string result holds an unknown dictionary code");
+				}
+				s += q.eng->dict.strings[(size_t)v];
+			} else {
+				append_i128(s, v);
+			}
 		}
 		s.push_back('\n');
 	}
@@ -933,14 +949,19 @@ int vc_column_add(vc_engine* eng, const char* table, const char* column, int typ
 {
 	return guarded([&] {
 		Table& t = table_of(eng, table);
-		if (!column || !*column || type < VC_U8 || type > VC_I64 || lo > hi) {
+		if (!column || !*column || type < VC_U8 || type > VC_STR || lo > hi) {
 			throw Error(VC_ERR_INVALID, "bad column arguments");
+		}
+		if (type == VC_STR) {
+			lo = hi = 0; /* a string column's domain is its dictionary codes, set by its upload */
 		}
 		if (t.find(column)) {
 			throw Error(VC_ERR_INVALID, std::string("column '") + column + "' exists");
 		}
-		const int64_t tmin = type == VC_U8 ? 0 : type == VC_I16 ? INT16_MIN : type == VC_I32 ? INT32_MIN : INT64_MIN;
-		const int64_t tmax = type == VC_U8 ? 255 : type == VC_I16 ? INT16_MAX : type == VC_I32 ? INT32_MAX : INT64_MAX;
+		const int64_t tmin = type == VC_U8 ? 0 : type == VC_I16 ? INT16_MIN : (type == VC_I32 || type == VC_STR) ? INT32_MIN
+			: INT64_MIN;
+		const int64_t tmax = type == VC_U8 ? 255 : type == VC_I16 ? INT16_MAX : (type == VC_I32 || type == VC_STR) ? INT32_MAX
+			: INT64_MAX;
 		if (lo < tmin || hi > tmax) {
 			throw Error(VC_ERR_INVALID, "column domain does not fit its type");
 		}
@@ -984,11 +1005,83 @@ int vc_column_upload(vc_engine* eng, const char* table, const char* column, cons
 		if (!host || rows != t.rows) {
 			throw Error(VC_ERR_INVALID, "upload must provide exactly the table's rows");
 		}
+		if (c.type == VC_STR) {
+			throw Error(VC_ERR_INVALID, "string columns are uploaded with vc_column_upload_strings");
+		}
 		VC_CHECK_CUDA(cudaSetDevice(eng->e.device));
 		if (rows) {
 			VC_CHECK_CUDA(cudaMemcpyAsync(c.dev, host, (size_t)rows * vc_gen_type_size(c.type), cudaMemcpyHostToDevice,
 				(cudaStream_t)stream));
 		}
+	});
+}
+
+namespace vc {
+/* encodes a string column's rows into the engine dictionary and uploads the codes; the
+ * column's domain becomes the codes' range */
+static void upload_codes(Engine& e, Column& c, int64_t rows, const std::function<std::string(int64_t)>& row)
+{
+	std::vector<int32_t> codes((size_t)rows);
+	int32_t lo = 0, hi = 0;
+	{
+		std::lock_guard<std::mutex> g(e.mu);
+		for (int64_t r = 0; r < rows; r++) {
+			codes[(size_t)r] = e.dict.encode(row(r));
+			lo = r == 0 ? codes[(size_t)r] : std::min(lo, codes[(size_t)r]);
+			hi = r == 0 ? codes[(size_t)r] : std::max(hi, codes[(size_t)r]);
+		}
+	}
+	c.lo = lo;
+	c.hi = hi;
+	if (!e.offline && rows) {
+		VC_CHECK_CUDA(cudaSetDevice(e.device));
+		VC_CHECK_CUDA(cudaMemcpy(c.dev, codes.data(), (size_t)rows * 4, cudaMemcpyHostToDevice));
+	}
+}
+} // namespace vc
+
+int vc_column_upload_strings(vc_engine* eng, const char* table, const char* column, const char* bytes,
+	const int64_t* offsets, int64_t rows)
+{
+	return guarded([&] {
+		Table& t = table_of(eng, table);
+		Column& c = column_of(eng, table, column);
+		if (c.type != VC_STR || rows != t.rows || (rows && (!bytes || !offsets))) {
+			throw Error(VC_ERR_INVALID, "a string upload needs a string column, its rows, bytes and rows+1 offsets");
+		}
+		for (int64_t r = 0; r < rows; r++) {
+			if (offsets[r + 1] < offsets[r] || offsets[r] < 0) {
+				throw Error(VC_ERR_INVALID, "string offsets must not decrease");
+			}
+		}
+		upload_codes(eng->e, c, rows, [&](int64_t r) {
+			return std::string(bytes + offsets[r], (size_t)(offsets[r + 1] - offsets[r]));
+		});
+	});
+}
+
+int vc_dict_size(vc_engine* eng, int64_t* n)
+{
+	return guarded([&] {
+		if (!eng || !n) {
+			throw Error(VC_ERR_INVALID, "null argument");
+		}
+		std::lock_guard<std::mutex> g(eng->e.mu);
+		*n = (int64_t)eng->e.dict.strings.size();
+	});
+}
+
+int vc_dict_string(vc_engine* eng, int64_t code, char* buf, size_t cap, size_t* len)
+{
+	return guarded([&] {
+		if (!eng) {
+			throw Error(VC_ERR_INVALID, "null engine");
+		}
+		std::lock_guard<std::mutex> g(eng->e.mu);
+		if (code < 0 || code >= (int64_t)eng->e.dict.strings.size()) {
+			throw Error(VC_ERR_INVALID, "no such string code");
+		}
+		copy_out(eng->e.dict.strings[(size_t)code], buf, cap, len);
 	});
 }
 
@@ -1023,6 +1116,34 @@ int vc_column_attach(vc_engine* eng, const char* table, const char* column, void
 		}
 		c.dev = device_ptr;
 		c.owned = false;
+		c.host = false;
+	});
+}
+
+int vc_column_attach_host(vc_engine* eng, const char* table, const char* column, const void* host_ptr)
+{
+	return guarded([&] {
+		Column& c = column_of(eng, table, column);
+		if (!host_ptr || ((uintptr_t)host_ptr & 15u)) {
+			throw Error(VC_ERR_INVALID, "host column memory must be non-null and 16-byte aligned");
+		}
+		if (eng->e.offline) {
+			throw Error(VC_ERR_NO_DEVICE, "an offline engine only generates and compiles code");
+		}
+		VC_CHECK_CUDA(cudaSetDevice(eng->e.device));
+		cudaPointerAttributes pa;
+		VC_CHECK_CUDA(cudaPointerGetAttributes(&pa, host_ptr));
+		if (pa.type != cudaMemoryTypeHost) {
+			throw Error(VC_ERR_INVALID, "host column memory must be pinned (cudaHostAlloc or cudaHostRegister)");
+		}
+		void* dev = nullptr;
+		VC_CHECK_CUDA(cudaHostGetDevicePointer(&dev, const_cast<void*>(host_ptr), 0));
+		if (c.owned && c.dev) {
+			VC_CHECK_CUDA(cudaFree(c.dev));
+		}
+		c.dev = dev;
+		c.owned = false;
+		c.host = true;
 	});
 }
 
@@ -1052,14 +1173,26 @@ int vc_column_generate(vc_engine* eng, const char* table, const char* column, in
 		spec.s = s;
 		spec.seed = seed;
 		spec.n = t.rows;
-		if (kind < VC_GEN_UNIFORM || kind > VC_GEN_MOD) {
+		if (kind < VC_GEN_UNIFORM || kind > VC_GEN_WORDS) {
 			throw Error(VC_ERR_INVALID, "unknown generator kind");
+		}
+		if ((kind == VC_GEN_WORDS) != (col.type == VC_STR)) {
+			throw Error(VC_ERR_INVALID, "string columns take the words generator, and only they do");
+		}
+		if (kind == VC_GEN_WORDS) {
+			/* strings are made on the host and dictionary-encoded; the codes are uploaded */
+			char buf[VC_GEN_STR_WIDTH];
+			upload_codes(eng->e, col, t.rows, [&](int64_t r) {
+				const int n = vc_gen_string(&spec, r, buf);
+				return std::string(buf, (size_t)n);
+			});
+			return;
 		}
 		if ((kind == VC_GEN_DIV || kind == VC_GEN_MOD) && b <= 0) {
 			throw Error(VC_ERR_INVALID, "generator divisor must be positive");
 		}
-		if (kind == VC_GEN_UNIFORM && (b < a || (uint64_t)(b - a) >= (1ull << 32))) {
-			throw Error(VC_ERR_INVALID, "uniform range must be non-empty and below 2^32");
+		if (kind == VC_GEN_UNIFORM && (b < a || (__int128)b - a >= (__int128)INT64_MAX)) {
+			throw Error(VC_ERR_INVALID, "uniform range must be non-empty and below 2^63");
 		}
 		const bool skew = kind == VC_GEN_ZIPF && s != 0.0;
 		if (skew && (!zipf_cdf || b < 1)) {
@@ -1085,10 +1218,20 @@ int vc_gen_host(int32_t kind, int32_t type, int64_t a, int64_t b, int64_t c, dou
 	const double* zipf_cdf, int64_t begin, int64_t count, void* out)
 {
 	return guarded([&] {
-		if (!out || count < 0 || begin < 0 || type < VC_U8 || type > VC_I64) {
+		if (!out || count < 0 || begin < 0 || type < VC_U8 || type > VC_STR || (type == VC_STR) != (kind == VC_GEN_WORDS)) {
 			throw Error(VC_ERR_INVALID, "bad generator arguments");
 		}
 		vc_gen_spec spec{kind, type, a, b, c, s, seed, n};
+		if (type == VC_STR) {
+			/* fixed-width rows of VC_GEN_STR_WIDTH bytes, NUL-padded */
+			char* o = (char*)out;
+			for (int64_t i = 0; i < count; i++) {
+				char* row = o + (size_t)i * VC_GEN_STR_WIDTH;
+				std::memset(row, 0, VC_GEN_STR_WIDTH);
+				vc_gen_string(&spec, begin + i, row);
+			}
+			return;
+		}
 		for (int64_t i = 0; i < count; i++) {
 			vc_gen_store(type, out, i, vc_gen_value(&spec, zipf_cdf, begin + i));
 		}
@@ -1308,7 +1451,7 @@ int vc_plan_describe(vc_engine* eng, const char* plan, const char* flavor, char*
 		}
 		const Flavor fl = Flavor::parse(flavor ? flavor : "");
 		std::lock_guard<std::mutex> g(eng->e.mu);
-		LoweredPlan lp = lower_plan(parse_plan(plan), eng->e.tables, fl);
+		LoweredPlan lp = lower_plan(parse_plan(plan), eng->e.tables, fl, eng->e.dict);
 		copy_out("{\"pipelines\": " + describe_pipelines(lp) + "}", buf, cap, len);
 	});
 }

@@ -67,9 +67,11 @@ RelOpP parse_plan(const std::string& text);
 struct Column {
 	std::string name;
 	int type = VC_TYPE_I32;
-	int64_t lo = 0, hi = 0;   /* declared domain (the reference's MinMaxInfo) */
+	int64_t lo = 0, hi = 0;   /* declared domain (the reference's MinMaxInfo); strings: their codes */
 	void* dev = nullptr;      /* device data */
 	bool owned = false;
+	bool str = false;         /* holds string dictionary codes (VC_STR, or a key of one carried on) */
+	bool host = false;        /* pinned host memory the kernels read in place over PCIe */
 };
 
 struct Table {
@@ -83,6 +85,31 @@ struct Table {
 			}
 		}
 		return nullptr;
+	}
+};
+
+/* Engine-wide string dictionary: every string column of an engine is stored on the device as
+ * 32-bit codes of one dictionary, so string equality, joins and group keys compare codes and
+ * results are decoded on the host. */
+struct StringDict {
+	std::vector<std::string> strings;
+	std::unordered_map<std::string, int32_t> codes;
+	int32_t encode(const std::string& s) {
+		auto it = codes.find(s);
+		if (it != codes.end()) {
+			return it->second;
+		}
+		if (strings.size() >= (size_t)INT32_MAX) {
+			throw std::runtime_error("string dictionary is full");
+		}
+		const int32_t c = (int32_t)strings.size();
+		strings.push_back(s);
+		codes.emplace(s, c);
+		return c;
+	}
+	int32_t find(const std::string& s) const {
+		auto it = codes.find(s);
+		return it == codes.end() ? -1 : it->second;
 	}
 };
 
@@ -100,10 +127,13 @@ struct BExpr {
 	int col = -1;              /* Col: index into Pipeline::cols */
 	int64_t cval = 0;          /* Const */
 	int probe = -1, pidx = -1; /* ProbeOut: op index, payload index */
-	std::string fn;            /* Fun: lt le gt ge eq ne and or add sub mul */
+	std::string fn;            /* Fun: lt le gt ge eq ne and or add sub mul; inset; shr lowbits extract_year */
 	std::vector<BExprP> args;
 	Bounds b;
 	bool boolean = false;
+	bool str = false;          /* a string: a dictionary code (Col, ProbeOut) or a string constant */
+	std::string sval;          /* string constant */
+	int aux = -1;              /* inset: index of the code bitmap in LoweredPlan::bitmaps */
 };
 
 struct JoinDesc {
@@ -181,6 +211,7 @@ struct PipeColumn {
 	std::string table, name;
 	int type;
 	int64_t lo, hi;
+	bool host = false;        /* read from pinned host memory (coherent loads, no bulk copies) */
 };
 
 struct Pipeline {
@@ -232,6 +263,15 @@ struct Flavor {
  * int64, which is computed as exact int64 sums of bit chunks and recombined in 128 bits. */
 struct OutCol {
 	std::vector<std::pair<int, int>> parts; /* (physical column, shift) */
+	bool str = false;                       /* a string dictionary code, printed as its string */
+};
+
+/* Code set of a `contains` predicate: bit (code - lo) is set when the code's string holds the
+ * pattern.  Uploaded at query creation; `dev` is its device copy. */
+struct CodeBitmap {
+	int64_t lo = 0;
+	std::vector<uint32_t> bits;
+	void* dev = nullptr;
 };
 
 struct LoweredPlan {
@@ -241,9 +281,11 @@ struct LoweredPlan {
 	int result_pipe = -1;
 	int result_cols = 0;              /* physical columns of the result buffer */
 	std::vector<OutCol> out_cols;     /* the caller's columns */
+	std::vector<CodeBitmap> bitmaps;  /* code sets of `contains` predicates */
 };
 
-LoweredPlan lower_plan(const RelOpP& root, std::map<std::string, Table>& tables, const Flavor& fl);
+LoweredPlan lower_plan(const RelOpP& root, std::map<std::string, Table>& tables, const Flavor& fl,
+	const StringDict& dict);
 
 /* ------------------------------------------------------------------ generated code ----- */
 
@@ -305,6 +347,7 @@ struct Engine {
 	bool offline = false;       /* code generation and compilation only, no device */
 	uintptr_t fake_next = 0x100000;
 	std::map<std::string, Table> tables;
+	StringDict dict;
 	std::mutex mu;
 	~Engine();
 };

@@ -200,12 +200,13 @@ struct Scope {
 struct Lowerer {
 	std::map<std::string, Table>& tables;
 	const Flavor& fl;
+	const StringDict& dict;
 	LoweredPlan out;
 
 	std::map<std::string, Table> inter_tables; /* intermediate tables by name */
 	int name_counter = 0; /* the reference translator's id counter (relalg_translator.hpp:26-30) */
 
-	Lowerer(std::map<std::string, Table>& t, const Flavor& f) : tables(t), fl(f) {}
+	Lowerer(std::map<std::string, Table>& t, const Flavor& f, const StringDict& d) : tables(t), fl(f), dict(d) {}
 
 	Table& table(const std::string& n) {
 		auto ii = inter_tables.find(n);
@@ -238,10 +239,11 @@ struct Lowerer {
 		}
 		if (e->col < 0) {
 			e->col = (int)p.cols.size();
-			p.cols.push_back(PipeColumn{s.table, s.column, c->type, c->lo, c->hi});
+			p.cols.push_back(PipeColumn{s.table, s.column, c->type, c->lo, c->hi, c->host});
 		}
 		e->b.lo = c->lo;
 		e->b.hi = c->hi;
+		e->str = c->str || c->type == VC_TYPE_STR;
 		s.e = e;
 		return e;
 	}
@@ -251,6 +253,7 @@ struct Lowerer {
 		case RelExpr::Const: {
 			auto e = std::make_shared<BExpr>();
 			e->kind = BExpr::Const;
+			e->sval = re->text;
 			try {
 				size_t used = 0;
 				e->cval = std::stoll(re->text, &used);
@@ -258,7 +261,9 @@ struct Lowerer {
 					throw std::invalid_argument("trailing");
 				}
 			} catch (const std::exception&) {
-				throw Error(kErrUnsupported, "constant '" + re->text + "' is not an int64 literal");
+				/* not an integer: a string constant, usable against string columns */
+				e->str = true;
+				e->cval = 0;
 			}
 			e->b.lo = e->b.hi = e->cval;
 			return e;
@@ -274,6 +279,40 @@ struct Lowerer {
 			throw Error(kErrInvalid, "assign is only allowed in a projection list");
 		case RelExpr::Fun:
 			break;
+		}
+		if (re->text == "contains") {
+			/* contains(string column, pattern) (runtime.hpp:150-224, kernel_generator.py:435-437):
+			 * the set of dictionary codes whose strings hold the pattern, as a bitmap over the
+			 * column's code range; the kernel tests the row's code */
+			if (re->args.size() != 2) {
+				throw Error(kErrInvalid, "contains takes two arguments");
+			}
+			BExprP col = bind(re->args[0], sc, p);
+			BExprP pat = bind(re->args[1], sc, p);
+			if (!col->str || col->kind == BExpr::Const || pat->kind != BExpr::Const) {
+				throw Error(kErrUnsupported, "contains needs a string column and a constant pattern");
+			}
+			CodeBitmap bm;
+			bm.lo = (int64_t)col->b.lo;
+			const int64_t n = (int64_t)(col->b.hi - col->b.lo) + 1;
+			bm.bits.assign((size_t)std::max<int64_t>((n + 31) / 32, 1), 0u);
+			for (int64_t i = 0; i < n; i++) {
+				const int64_t code = bm.lo + i;
+				if (code >= 0 && code < (int64_t)dict.strings.size() &&
+					dict.strings[(size_t)code].find(pat->sval) != std::string::npos) {
+					bm.bits[(size_t)(i >> 5)] |= 1u << (i & 31);
+				}
+			}
+			auto e = std::make_shared<BExpr>();
+			e->kind = BExpr::Fun;
+			e->fn = "inset";
+			e->args.push_back(col);
+			e->aux = (int)out.bitmaps.size();
+			out.bitmaps.push_back(std::move(bm));
+			e->boolean = true;
+			e->b.lo = 0;
+			e->b.hi = 1;
+			return e;
 		}
 		if (re->text == "extract_year") {
 			/* year of a date stored as its Julian day number (runtime.hpp:128-148); the
@@ -310,6 +349,24 @@ struct Lowerer {
 		}
 		if (e->args.size() != 2) {
 			throw Error(kErrInvalid, "function '" + re->text + "' takes two arguments");
+		}
+		if (e->args[0]->str || e->args[1]->str) {
+			/* strings compare by dictionary code: only (in)equality, and a string constant is
+			 * its code (-1, equal to no row, when the dictionary does not hold it) */
+			if (e->fn != "eq" && e->fn != "ne") {
+				throw Error(kErrUnsupported, "strings support =, != and contains only");
+			}
+			for (auto& x : e->args) {
+				if (x->kind == BExpr::Const) {
+					auto c = std::make_shared<BExpr>();
+					c->kind = BExpr::Const;
+					c->cval = dict.find(x->sval);
+					c->b.lo = c->b.hi = c->cval;
+					x = c;
+				} else if (!x->str) {
+					throw Error(kErrUnsupported, "a string compares only with a string");
+				}
+			}
 		}
 		const Bounds& a = e->args[0]->b;
 		const Bounds& b = e->args[1]->b;
@@ -478,6 +535,7 @@ struct Lowerer {
 				e->probe = opi;
 				e->pidx = (int)k;
 				e->b = jd.pay_b[k];
+				e->str = sink.pay[k]->str;
 				sc.cols.push_back(ScopeEntry{op->right_payl[k]->text, e, "", ""});
 			}
 			return pi;
@@ -580,6 +638,9 @@ struct Lowerer {
 					throw Error(kErrInvalid, "sum takes one argument");
 				}
 				ag.arg = bind(a->args[0], sc, p);
+				if (ag.arg->str) {
+					throw Error(kErrUnsupported, "sum over a string is not supported");
+				}
 				if (ag.arg->boolean) {
 					throw Error(kErrUnsupported, "sum over a predicate is not supported");
 				}
@@ -663,7 +724,7 @@ struct Lowerer {
 			outs->clear();
 			int phys = 0;
 			for (size_t k = 0; k < sink.keys.size(); k++) {
-				outs->push_back(OutCol{{{phys++, 0}}});
+				outs->push_back(OutCol{{{phys++, 0}}, sink.keys[k]->str});
 			}
 			for (size_t i = 0; i < op->aggregates.size(); i++) {
 				OutCol oc;
@@ -723,6 +784,7 @@ struct Lowerer {
 			c.type = VC_TYPE_I64;
 			c.lo = (int64_t)sink.keys[i]->b.lo;
 			c.hi = (int64_t)sink.keys[i]->b.hi;
+			c.str = sink.keys[i]->str;
 			t.cols.push_back(c);
 		}
 		int j = 0;
@@ -817,16 +879,17 @@ struct Lowerer {
 		out.result_pipe = pi;
 		out.result_cols = (int)p.sink.outs.size();
 		for (int c = 0; c < out.result_cols; c++) {
-			out.out_cols.push_back(OutCol{{{c, 0}}});
+			out.out_cols.push_back(OutCol{{{c, 0}}, p.sink.outs[(size_t)c]->str});
 		}
 	}
 };
 
 } // namespace
 
-LoweredPlan lower_plan(const RelOpP& root, std::map<std::string, Table>& tables, const Flavor& fl)
+LoweredPlan lower_plan(const RelOpP& root, std::map<std::string, Table>& tables, const Flavor& fl,
+	const StringDict& dict)
 {
-	Lowerer l(tables, fl);
+	Lowerer l(tables, fl, dict);
 	l.root(root);
 	if (l.out.result_cols == 0) {
 		throw Error(kErrInvalid, "the plan produces no columns");

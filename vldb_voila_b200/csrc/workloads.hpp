@@ -11,6 +11,7 @@
  *              (db-engine-paradigms/src/benchmarks/sbb/queries/q41.cpp:21-46)
  *   batch      a seeded list of the first three with random sizes, selectivities and skews
  *   bigsum     sums of 64-bit values that leave int64 (128-bit results)
+ *   strings    string columns (dictionary codes on the device): contains, string group keys
  *
  * A workload is named by a spec string "<template>:key=value,...", e.g.
  * "join_aggr:build=1500000,probe=6000000,sel=0.2,seed=2".  Header-only C++ so that the
@@ -135,6 +136,7 @@ inline Column make_col(const std::string& name, int type, int kind, int64_t a, i
 	}
 	case VC_GEN_DIV: col.lo = a; col.hi = a + (last * c) / b; break;
 	case VC_GEN_MOD: col.lo = a; col.hi = a + (rows < b ? last : b - 1); break;
+	case VC_GEN_WORDS: col.lo = 0; col.hi = 0; break; /* strings: the domain is their dictionary codes */
 	default: throw std::invalid_argument("bad generator kind");
 	}
 	return col;
@@ -289,6 +291,30 @@ inline Workload make(const std::string& spec)
 		w.fact_table = "lineorder";
 		w.fact_rows = n;
 		w.algo_bytes = table_bytes(d) + table_bytes(c) + table_bytes(s) + table_bytes(pt) + table_bytes(f);
+		w.probe_bytes = table_bytes(f);
+	} else if (w.tmpl == "strings") {
+		/* string columns: part names of three words from a 24-word list, one-word brands from
+		 * the first six; a fact table of part references (TPC-H q9's `contains` shape) */
+		const int64_t n = param_i(p, "rows", 200000);
+		const int64_t np = param_i(p, "parts", 20000);
+		if (np < 1) {
+			throw std::invalid_argument("strings needs parts >= 1");
+		}
+		Table pt{"part", np, {}};
+		pt.cols.push_back(make_col("p_partkey", VC_TYPE_I32, VC_GEN_SEQ, 1, 0, np, column_seed(seed, 0, 0)));
+		pt.cols.push_back(make_col("p_name", VC_TYPE_STR, VC_GEN_WORDS, 3, 24, np, column_seed(seed, 0, 1)));
+		pt.cols.push_back(make_col("p_brand", VC_TYPE_STR, VC_GEN_WORDS, 1, 6, np, column_seed(seed, 0, 2)));
+		Table f{"lineitem", n, {}};
+		f.cols.push_back(make_col("l_partkey", VC_TYPE_I32, VC_GEN_UNIFORM, 1, np, n, column_seed(seed, 1, 0)));
+		f.cols.push_back(make_col("l_extendedprice", VC_TYPE_I64, VC_GEN_UNIFORM, 1, 1000000, n, column_seed(seed, 1, 1)));
+		w.tables = {pt, f};
+		w.plan = "(aggr hash ((col part.p_brand)) ((fun sum (col lineitem.l_extendedprice)) (fun count))"
+			" (join join01 ((col lineitem.l_partkey)) () (scan lineitem (l_partkey l_extendedprice))"
+			" ((col part.p_partkey)) ((col part.p_brand))"
+			" (select (fun contains (col part.p_name) (const green)) (scan part (p_partkey p_name p_brand)))))";
+		w.fact_table = "lineitem";
+		w.fact_rows = n;
+		w.algo_bytes = table_bytes(pt) + table_bytes(f);
 		w.probe_bytes = table_bytes(f);
 	} else if (w.tmpl == "bigsum") {
 		/* sums whose bound leaves int64 (the reference types them i128): 64-bit values up to

@@ -20,10 +20,13 @@ LIB_PATH = os.path.join(_HERE, "libvoila_cuda.so")
 VC_OK = 0
 ERRORS = {1: "invalid", 2: "cuda", 3: "capacity", 4: "timeout", 5: "compile", 6: "unsupported", 7: "no device"}
 
-TYPES = {"u8": 1, "i16": 2, "i32": 3, "i64": 4}
-NP_TYPES = {1: np.uint8, 2: np.int16, 3: np.int32, 4: np.int64}
+TYPES = {"u8": 1, "i16": 2, "i32": 3, "i64": 4, "str": 5}
+STR = 5
+# host arrays per column type (strings: Python str objects; on the device they are codes)
+NP_TYPES = {1: np.uint8, 2: np.int16, 3: np.int32, 4: np.int64, 5: object}
+STR_WIDTH = 32  # rows of a host-generated string column (NUL-padded)
 
-GEN_KINDS = {"uniform": 0, "seq": 1, "perm": 2, "zipf": 3, "choice": 4, "div": 5, "mod": 6}
+GEN_KINDS = {"uniform": 0, "seq": 1, "perm": 2, "zipf": 3, "choice": 4, "div": 5, "mod": 6, "words": 7}
 
 _lib_handle = None
 
@@ -98,6 +101,10 @@ def lib():
         "vc_query_timings": (c.c_int, [P, c.POINTER(c.c_float), c.c_int, c.POINTER(c.c_int), P, c.c_size_t]),
         "vc_stream_read": (c.c_int, [P, c.c_int64, P, P]),
         "vc_plan_columns": (c.c_int, [c.c_char_p, P, c.c_size_t, c.POINTER(c.c_size_t)]),
+        "vc_column_upload_strings": (c.c_int, [P, c.c_char_p, c.c_char_p, P, P, c.c_int64]),
+        "vc_column_attach_host": (c.c_int, [P, c.c_char_p, c.c_char_p, P]),
+        "vc_dict_size": (c.c_int, [P, c.POINTER(c.c_int64)]),
+        "vc_dict_string": (c.c_int, [P, c.c_int64, P, c.c_size_t, c.POINTER(c.c_size_t)]),
         "vc_table_import": (c.c_int, [P, c.c_char_p, c.c_char_p, c.c_char_p, c.c_int, c.POINTER(c.c_int64)]),
         "vc_column_info": (c.c_int, [P, c.c_char_p, c.c_char_p, c.POINTER(c.c_int32), c.POINTER(c.c_int64),
                                      c.POINTER(c.c_int64), c.POINTER(c.c_int64)]),
@@ -225,6 +232,12 @@ def zipf_cdf(s, n):
 def generate_host(col, begin=0, count=None, cdf=None):
     """The column's values for rows [begin, begin+count), generated on the host."""
     count = col.n - begin if count is None else count
+    if col.type == STR:
+        raw = np.zeros(count * STR_WIDTH, dtype=np.uint8)
+        check(lib().vc_gen_host(col.kind, col.type, col.a, col.b, col.c, col.s, col.seed, col.n, None, begin, count,
+                                raw.ctypes.data))
+        rows = raw.reshape(count, STR_WIDTH).view(f"S{STR_WIDTH}").reshape(count)
+        return np.array([r.decode() for r in rows], dtype=object)
     out = np.empty(count, dtype=col.dtype)
     if col.kind == GEN_KINDS["zipf"] and col.s != 0.0 and cdf is None:
         cdf = zipf_cdf(col.s, col.b)
@@ -286,9 +299,24 @@ class Engine:
 
     def upload(self, table, name, array, stream=None):
         t = self.tables[table]["columns"][name]
+        if t == STR:
+            return self.upload_strings(table, name, array)
         a = np.ascontiguousarray(array, dtype=NP_TYPES[t])
         check(lib().vc_column_upload(self._h, _b(table), _b(name), a.ctypes.data, len(a), _stream_ptr(stream)))
         return a
+
+    def upload_strings(self, table, name, strings):
+        """Uploads a string column (dictionary-encoded by the engine)."""
+        enc = [x.encode() if isinstance(x, str) else bytes(x) for x in strings]
+        offsets = np.zeros(len(enc) + 1, dtype=np.int64)
+        offsets[1:] = np.cumsum([len(x) for x in enc]) if enc else []
+        blob = b"".join(enc) or b"\0"
+        check(lib().vc_column_upload_strings(self._h, _b(table), _b(name), blob, offsets.ctypes.data, len(enc)))
+        return strings
+
+    def dict_string(self, code):
+        """String of a dictionary code (string result columns hold codes in Query.result())."""
+        return _text_call(lambda *a: lib().vc_dict_string(self._h, int(code), *a))
 
     def upload_ptr(self, table, name, host_ptr, rows, stream=None):
         check(lib().vc_column_upload(self._h, _b(table), _b(name), ctypes.c_void_p(host_ptr), rows,
@@ -323,6 +351,10 @@ class Engine:
                 self.tables[table]["columns"][name] = self.column_info(table, name)[0]
         return n.value
 
+    def attach_host(self, table, name, host_ptr):
+        """Reads the column in place from pinned host memory (queries created afterwards)."""
+        check(lib().vc_column_attach_host(self._h, _b(table), _b(name), ctypes.c_void_p(host_ptr)))
+
     def device_ptr(self, table, name):
         p = ctypes.c_void_p()
         check(lib().vc_column_device_ptr(self._h, _b(table), _b(name), ctypes.byref(p)))
@@ -342,6 +374,8 @@ class Engine:
         for c in w.columns:
             self.add_column(c.table, c.name, c.type, c.lo, c.hi)
             if self.offline:
+                if c.type == STR:
+                    self.generate(c)  # strings are encoded on the host: their codes type the plan
                 continue
             if data is not None:
                 self.upload(c.table, c.name, data[c.table][c.name], stream)

@@ -65,7 +65,7 @@ def test_hash_group_aggregates_share_accumulator_words():
     w, e = offline("groupby:rows=6000000,keys=1500000,zipf=0.0,seed=3")
     src = e.query(w.plan).source()
     assert "uint64_t w[2]" in src and "gt_add<2>" in src
-    assert "gt_find_or_insert<uint32_t>" in src
+    assert "gt_find_or_insert_pre<uint32_t>" in src  # first buckets of all rows loaded ahead
 
 
 @pytest.mark.parametrize("plan,code", [

@@ -1137,6 +1137,32 @@ struct PipeGen {
 			}
 			const std::string K = gkey_type();
 			const int W = s.nwords;
+			if (fl.aggr != "cache") {
+				/* three phases so each thread keeps V bucket loads in flight: warp pre-sums of
+				 * every row, then the first bucket of every leader's probe, then the inserts
+				 * and atomics */
+				o << "    uint64_t hk[" << V << "]; " << K << " kk[" << V << "]; bool ldr[" << V << "]; uint64_t ww[" << V
+				  << "][" << W << "];\n";
+				o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
+				o << "      const uint64_t pk = act[v] ? (" << packed_key(s.keys, kb, s.key_shift, "v") << ") : 0ull;\n";
+				emit_packed_words("act[v] ? (unsigned long long)pk : ~0ull", "v");
+				o << "      ldr[v] = lead;\n      kk[v] = (" << K << ")(pk + 1ull);\n";
+				o << "      hk[v] = " << table_hash(s.keys, "pk", s.key_bits, "v") << ";\n";
+				o << "#pragma unroll\n      for (int a = 0; a < " << W << "; a++) { ww[v][a] = w[a]; }\n";
+				o << "    }\n";
+				o << "    uint4 bq0[" << V << "], bq1[" << V << "];\n";
+				o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
+				o << "      if (ldr[v]) {\n";
+				o << "        const uint4* bp = reinterpret_cast<const uint4*>(gkeys + (hk[v] & gbmask) * "
+				  << 32 / gkey_bytes() << ");\n";
+				o << "        bq0[v] = __ldcg(bp);\n        bq1[v] = __ldcg(bp + 1);\n      }\n    }\n";
+				o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
+				o << "      if (ldr[v]) {\n";
+				o << "        const int64_t slot = vd::gt_find_or_insert_pre<" << K << ">(gkeys, gbmask, hk[v], kk[v], bq0[v], bq1[v], err);\n";
+				o << "        if (slot >= 0) { vd::gt_add<" << W << ">(gacc, slot, ww[v]); }\n";
+				o << "      }\n    }\n";
+				break;
+			}
 			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
 			o << "      const uint64_t pk = act[v] ? (" << packed_key(s.keys, kb, s.key_shift, "v") << ") : 0ull;\n";
 			emit_packed_words("act[v] ? (unsigned long long)pk : ~0ull", "v");

@@ -845,6 +845,41 @@ __device__ __forceinline__ int64_t gt_find_or_insert(K* __restrict__ keys, uint6
 	return -1;
 }
 
+/* gt_find_or_insert whose first bucket (b0, b1: its two 16-byte halves) was loaded ahead */
+template <typename K>
+__device__ __forceinline__ int64_t gt_find_or_insert_pre(K* __restrict__ keys, uint64_t bmask, uint64_t h, K key,
+	uint4 b0, uint4 b1, unsigned* err)
+{
+	constexpr int KPB = 32 / (int)sizeof(K);
+	const uint64_t b = h & bmask;
+	K k[KPB];
+	reinterpret_cast<uint4*>(k)[0] = b0;
+	reinterpret_cast<uint4*>(k)[1] = b1;
+	K* bk = keys + b * KPB;
+#pragma unroll
+	for (int i = 0; i < KPB; i++) {
+		if (k[i] == key) {
+			return (int64_t)(b * KPB + i);
+		}
+	}
+#pragma unroll
+	for (int i = 0; i < KPB; i++) {
+		if (k[i] == 0) {
+			K prev;
+			if constexpr (sizeof(K) == 4) {
+				prev = (K)atomicCAS((unsigned int*)&bk[i], 0u, (unsigned int)key);
+			} else {
+				prev = (K)atomicCAS((unsigned long long*)&bk[i], 0ull, (unsigned long long)key);
+			}
+			if (prev == 0 || prev == key) {
+				return (int64_t)(b * KPB + i);
+			}
+		}
+	}
+	/* the bucket is full of other keys: continue from the next one */
+	return gt_find_or_insert<K>(keys, bmask, (b + 1) & bmask, key, err);
+}
+
 /* adds W packed accumulator words into a slot of the split group table */
 template <int W>
 __device__ __forceinline__ void gt_add(unsigned long long* __restrict__ acc, int64_t slot, const uint64_t (&w)[W])

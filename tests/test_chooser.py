@@ -44,3 +44,17 @@ def test_explorer_samples_and_logs_to_the_runs_table(tmp_path):
     assert n == 2 * len(times)
     best = con.execute("SELECT full_blend, MIN(time_ms) FROM runs WHERE result = 'OK'").fetchone()
     assert best[0] in times
+
+
+def test_per_pipeline_backtracking_never_loses_to_its_start(tmp_path):
+    from vldb_voila_b200 import chooser as ch
+    db = str(tmp_path / "voila.db")
+    spec = "star:rows=2000000,custs=30000,supps=2000,parts=140000,seed=7"
+    base = "cuda()"
+    best, ms = ch.backtrack(spec, base=base, reps=3, sqlite_path=db)
+    assert best.startswith(base)
+    con = sqlite3.connect(db)
+    base_ms = [r[0] for r in con.execute("SELECT time_ms FROM runs WHERE full_blend = ? AND result = 'OK'", (base,))]
+    assert ms <= float(np.median(base_ms)) + 1e-9
+    n, = con.execute("SELECT COUNT(*) FROM runs WHERE mode = 'backtrack'").fetchone()
+    assert n >= 3 * len(ch.PIPE_GRID)

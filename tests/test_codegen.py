@@ -259,3 +259,18 @@ def test_sums_beyond_int64_are_split_into_exact_chunk_sums():
     with pytest.raises(VoilaError) as ex:
         e.query(plan)
     assert ex.value.code == 6
+
+
+def test_per_pipeline_flavor_overrides():
+    """"cuda(...);p<id>=cuda(...)" gives single pipelines their own knobs (the reference's
+    per-pipeline blends); hash and graph stay query-wide."""
+    w, e = offline("star:rows=1000")
+    q = e.query(w.plan, "cuda(threads=256);p4=cuda(rows=8,threads=128);p1=cuda(build=staged)")
+    info = q.info()
+    assert info["flavor"].endswith(";p4=cuda(rows=8,threads=128);p1=cuda(build=staged)")
+    ks = {k["name"]: k["threads"] for k in info["kernels"]}
+    assert ks["vc_p4_main"] == 128 and ks["vc_p3_main"] == 256
+    assert "vc_p1_insert" in ks and "vc_p2_insert" not in ks
+    for bad in ["cuda();p4=cuda(hash=voila)", "cuda();q4=cuda(rows=2)", "cuda();p4=cuda(rows=3)"]:
+        with pytest.raises(VoilaError):
+            e.query(w.plan, bad)

@@ -13,7 +13,8 @@ logged to the SQLite `runs` table, compiler.cpp:91-256).  Here:
     run); candidates the device cannot run (shared memory) are skipped;
   * `explore` is the reference explorer's counterpart: the full grid or a seeded random sample
     of it, every run logged to a JSONL file and/or the reference's SQLite `runs` schema
-    (backend 'cuda', the flavor string as the blend);
+    (backend 'cuda', the flavor string as the blend); `backtrack` is its per-pipeline
+    backtracking, over "p<id>=cuda(...)" overrides of single pipelines;
   * `Chooser` is the learned part: a small MLP, trained and evaluated on the GPU by the
     library's own kernels (csrc/mlp.cu), maps a pipeline's features -- taken from the lowered
     plan (vc_plan_describe: rows, probes, rows of the probed builds, key domain, groups bound,
@@ -258,6 +259,54 @@ def explore(spec, mode="full", sample=16, seed=1, reps=3, sqlite_path=None, log_
         raise ValueError("mode must be full or sample")
     return autotune(spec, candidates=cands, reps=reps, log_path=log_path, engine=engine,
                     sqlite_path=sqlite_path, mode=mode)
+
+
+# knobs a single pipeline may take (hash and graph stay query-wide)
+PIPE_GRID = [f"cuda(threads={t},rows={r},prefetch={pf})" for t in (128, 256, 512) for r in (2, 4, 8) for pf in (0, 1)]
+
+
+def backtrack(spec, base=None, reps=3, sqlite_path=None, log_path=None, engine=None, device=0):
+    """The reference explorer's per-pipeline backtracking (explorer.cpp:111-134) over CUDA
+    flavors: starting from `base` (default: the best of the workload kind's grid), each pipeline in
+    turn tries every PIPE_GRID setting as a "p<id>=cuda(...)" override while the others keep
+    their current choice, and keeps the fastest.  Returns (flavor string, ms)."""
+    own = engine is None
+    eng = engine or Engine(device)
+    w = workload(spec)
+    if own:
+        eng.load_workload(w, on_device=True)
+    log = RunLog(sqlite_path, log_path)
+    if base is None:
+        times = autotune(spec, reps=reps, engine=eng)
+        base = min(times, key=times.get)
+
+    def timed(fl):
+        try:
+            q = eng.query(w.plan, fl)
+        except VoilaError as e:
+            log.record("backtrack", spec, fl, f"EXCEPT '{e}'", 0, None, w.fact_rows)
+            return None
+        q.time(1)
+        ts = q.time(reps)
+        q.close()
+        for r, t in enumerate(ts):
+            log.record("backtrack", spec, fl, "OK", r, float(t), w.fact_rows)
+        return float(np.median(ts))
+
+    best, best_ms = base, timed(base)
+    overrides = {}
+    for pipe in range(len(eng.describe(w.plan, base)["pipelines"])):
+        for cand in PIPE_GRID:
+            trial = dict(overrides)
+            trial[pipe] = cand
+            fl = base + "".join(f";p{k}={v}" for k, v in sorted(trial.items()))
+            ms = timed(fl)
+            if ms is not None and ms < best_ms:
+                best, best_ms, overrides = fl, ms, trial
+    log.close()
+    if own:
+        eng.close()
+    return best, best_ms
 
 
 def load_log(path):

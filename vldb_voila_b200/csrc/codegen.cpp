@@ -1484,7 +1484,8 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 			target.out_cap = it.cap;
 			target.out_count = it.count;
 		}
-		PipeGen g(p, plan, fl, st[p.id], target, prm);
+		const Flavor pfl = fl.for_pipe(p.id);
+		PipeGen g(p, plan, pfl, st[p.id], target, prm);
 		std::string main = g.gen_main();
 		std::string extra;
 		if (p.sink.kind == Sink::JoinBuild && !plan.joins[p.sink.join].direct) {
@@ -1502,8 +1503,8 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 		m.pipe = p.id;
 		m.stage = 0;
 		m.smem = g.smem_total;
-		m.threads = fl.threads;
-		const int64_t tile = (int64_t)fl.threads * fl.rows;
+		m.threads = pfl.threads;
+		const int64_t tile = (int64_t)pfl.threads * pfl.rows;
 		m.grid_items = std::max<int64_t>((p.rows + tile - 1) / tile, 1);
 		m.dominant = p.id == plan.result_pipe;
 		if (p.sink.kind == Sink::AggGlobal || p.sink.kind == Sink::AggDense) {
@@ -1588,23 +1589,29 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 		Query& q = *queries[qi];
 		QueryState& st = state_of(q);
 		bc.query_params_begin.push_back((int64_t)bc.params.size());
-		Flavor fl = flavors[qi];
-		fl.threads = threads;
-		fl.load = "ldg";
 		/* every CTA of the persistent kernel reserves the largest shape's shared memory, so
 		 * the knobs that need much of it run as their lean equivalents inside a batch */
-		if (fl.lowcard == "private") {
-			fl.lowcard = "combine";
-		}
-		fl.cache_slots = std::min(fl.cache_slots, 256);
-		fl.sink_smem = std::min(fl.sink_smem, 16 * 1024);
+		auto batch_flavor = [&](int pipe) {
+			Flavor f = flavors[qi].for_pipe(pipe);
+			f.threads = threads;
+			f.load = "ldg";
+			if (f.lowcard == "private") {
+				f.lowcard = "combine";
+			}
+			f.cache_slots = std::min(f.cache_slots, 256);
+			f.sink_smem = std::min(f.sink_smem, 16 * 1024);
+			return f;
+		};
 		QueryDeviceState qs;
 		qs.out = q.out;
 		qs.out_cap = q.out_cap;
 		qs.out_count = q.out_count;
-		const int64_t tile = (int64_t)fl.threads * fl.rows;
+		auto tile_of = [&](const Pipeline& p) {
+			const Flavor f = batch_flavor(p.id);
+			return (int64_t)f.threads * f.rows;
+		};
 		auto items_of = [&](const Pipeline& p) {
-			const int64_t ntiles = std::max<int64_t>((p.rows + tile - 1) / tile, 1);
+			const int64_t ntiles = std::max<int64_t>((p.rows + tile_of(p) - 1) / tile_of(p), 1);
 			return (ntiles + tiles_per_item - 1) / tiles_per_item;
 		};
 		if (!q.plan.inters.empty()) {
@@ -1649,7 +1656,8 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 			/* the query keeps its own parameter layout for standalone runs */
 			const int saved_err = p.err_slot;
 			const std::vector<int> saved_cols = p.col_slots;
-			PipeGen g(p, q.plan, fl, st.pipes[p.id], qs, prm);
+			const Flavor pfl = batch_flavor(p.id);
+			PipeGen g(p, q.plan, pfl, st.pipes[p.id], qs, prm);
 			g.item = true;
 			g.name = "VCSHAPE";
 			const std::string main_src = g.gen_main();
@@ -1665,7 +1673,7 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 			bc.params.insert(bc.params.end(), prm.begin(), prm.end());
 
 			const int sid = add_shape(main_src, "_main");
-			const int64_t ntiles = std::max<int64_t>((p.rows + tile - 1) / tile, 1);
+			const int64_t ntiles = std::max<int64_t>((p.rows + tile_of(p) - 1) / tile_of(p), 1);
 			const int64_t nit = items_of(p);
 			const bool is_build = p.sink.kind == Sink::JoinBuild;
 			/* phase (position in the queue), the counter waited for and its target */

@@ -64,16 +64,71 @@ std::string Flavor::str() const
 		o << ",probe=" << probe_lanes;
 	}
 	o << ")";
+	for (auto& ov : overrides) {
+		o << ";p" << ov.first << "=" << ov.second;
+	}
 	return o.str();
 }
 
 Flavor Flavor::parse(const std::string& s0)
 {
+	/* "cuda(...)" for every pipeline, then ";p<id>=cuda(...)" overrides for single pipelines */
 	Flavor f;
 	std::string s = s0;
 	s.erase(std::remove_if(s.begin(), s.end(), ::isspace), s.end());
-	if (s.empty() || s == "cuda" || s == "cuda()") {
+	std::vector<std::string> parts;
+	std::stringstream ss(s);
+	std::string part;
+	while (std::getline(ss, part, ';')) {
+		parts.push_back(part);
+	}
+	if (parts.empty()) {
 		return f;
+	}
+	apply(f, parts[0]);
+	for (size_t i = 1; i < parts.size(); i++) {
+		const std::string& ov = parts[i];
+		const size_t eq = ov.find('=');
+		if (ov.size() < 3 || ov[0] != 'p' || eq == std::string::npos) {
+			throw Error(1, "pipeline flavor overrides look like p<id>=cuda(...), got '" + ov + "'");
+		}
+		int id = -1;
+		try {
+			id = std::stoi(ov.substr(1, eq - 1));
+		} catch (...) {
+			throw Error(1, "bad pipeline id in '" + ov + "'");
+		}
+		const std::string body = ov.substr(eq + 1);
+		Flavor probe = f;
+		apply(probe, body); /* validates the knobs */
+		if (body.find("hash=") != std::string::npos || body.find("graph=") != std::string::npos) {
+			throw Error(1, "hash and graph are knobs of the whole query, not of one pipeline");
+		}
+		if (id < 0) {
+			throw Error(1, "bad pipeline id in '" + ov + "'");
+		}
+		f.overrides.push_back({id, body});
+	}
+	return f;
+}
+
+Flavor Flavor::for_pipe(int id) const
+{
+	Flavor f = *this;
+	f.overrides.clear();
+	for (auto& ov : overrides) {
+		if (ov.first == id) {
+			apply(f, ov.second);
+		}
+	}
+	return f;
+}
+
+void Flavor::apply(Flavor& f, const std::string& s0)
+{
+	std::string s = s0;
+	if (s.empty() || s == "cuda" || s == "cuda()") {
+		return;
 	}
 	if (s.rfind("computation_type=", 0) == 0) {
 		s = s.substr(17);
@@ -170,7 +225,6 @@ Flavor Flavor::parse(const std::string& s0)
 			throw Error(1, "unknown flavor knob '" + k + "'");
 		}
 	}
-	return f;
 }
 
 /* ------------------------------------------------------------------ engine ------------- */
@@ -293,7 +347,15 @@ void query_prepare(Query& q)
 		const int64_t slots = std::max<int64_t>(pow2_at_least(2 * rows), 2 * spb);
 		jd.max_buckets = slots / spb;
 		jd.table_bytes = (size_t)slots * sb;
-		const std::string& bm = q.flavor.build;
+		/* the build pipeline's knobs size its table */
+		int build_pipe = 0;
+		for (auto& p : plan.pipes) {
+			if (p.sink.kind == Sink::JoinBuild && p.sink.join == jd.id) {
+				build_pipe = p.id;
+			}
+		}
+		const Flavor jf = q.flavor.for_pipe(build_pipe);
+		const std::string& bm = jf.build;
 		/* a dense table when the packed key space is small: one access per probe and no
 		 * larger than the hash table would be (a bitmap when there is no payload) */
 		size_t dense_bytes = 0;
@@ -315,7 +377,7 @@ void query_prepare(Query& q)
 		if (jd.dense) {
 			jd.table_bytes = dense_bytes;
 		}
-		jd.direct = jd.dense || bm == "direct" || (bm == "auto" && (int64_t)jd.table_bytes <= q.flavor.direct_limit);
+		jd.direct = jd.dense || bm == "direct" || (bm == "auto" && (int64_t)jd.table_bytes <= jf.direct_limit);
 		jd.direct_bmask = (uint64_t)(jd.max_buckets - 1);
 		jd.table = dev_alloc(q, jd.table_bytes);
 		jd.words = (unsigned long long*)arena_take(32);
@@ -356,9 +418,12 @@ void query_prepare(Query& q)
 		case Sink::AggHash:
 			/* a user-set capacity (gcap) is taken as given: too small a table fails the run
 			 * with VC_ERR_CAPACITY (bounded probe sequences), it never returns wrong rows */
-			ps.sink_cap = q.flavor.group_slots > 0 ? pow2_at_least(q.flavor.group_slots)
-				: std::max<int64_t>(pow2_at_least((std::max<int64_t>(p.sink.groups_bound, 1) * 100 + q.flavor.fill - 1) /
-					q.flavor.fill), 1024);
+			{
+				const Flavor pf = q.flavor.for_pipe(p.id);
+				ps.sink_cap = pf.group_slots > 0 ? pow2_at_least(pf.group_slots)
+					: std::max<int64_t>(pow2_at_least((std::max<int64_t>(p.sink.groups_bound, 1) * 100 + pf.fill - 1) /
+						pf.fill), 1024);
+			}
 			/* split layout: the keys (4 or 8 bytes per slot) in 32-byte buckets, then the
 			 * packed accumulator words */
 			ps.sink_bytes = (size_t)ps.sink_cap * (p.sink.key_bits <= 31 ? 4 : 8);
@@ -398,7 +463,8 @@ void query_prepare(Query& q)
 		if (rp.sink.kind == Sink::Emit) {
 			/* joinN can multiply rows up to probe rows x build rows: the buffer is bounded, and a
 			 * result beyond it fails the run with VC_ERR_CAPACITY (raise it with ocap=) */
-			const int64_t cap = q.flavor.out_rows > 0 ? q.flavor.out_rows : 4 * rp.rows + (1 << 20);
+			const int64_t orows = q.flavor.for_pipe(rp.id).out_rows;
+			const int64_t cap = orows > 0 ? orows : 4 * rp.rows + (1 << 20);
 			q.out_cap = std::max<int64_t>(std::min(q.out_cap, cap), 1);
 		}
 		break;
@@ -495,7 +561,8 @@ static void launch_all(Query& q, cudaStream_t stream, bool capturing = false)
 	for (size_t i = 0; i < n; i++) {
 		const Launch& l = q.code.launches[i];
 		const int occ = st.occupancy[i];
-		int64_t per_sm = q.flavor.grid > 0 ? std::min(q.flavor.grid, occ) : occ;
+		const int g = q.flavor.for_pipe(l.pipe).grid;
+		int64_t per_sm = g > 0 ? std::min(g, occ) : occ;
 		int64_t grid = (int64_t)q.eng->sms * per_sm;
 		if (l.grid_items > 0) {
 			grid = std::min<int64_t>(grid, l.grid_items);

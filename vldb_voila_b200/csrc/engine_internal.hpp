@@ -254,8 +254,17 @@ struct Flavor {
 	int64_t out_rows = 0;     /* result row capacity of an emitting pipeline (0 = from its bound, at
 	                           * most 4 rows per input row + 2^20 when joinN probes multiply rows) */
 
+	/* per-pipeline overrides "p<id>=cuda(...)" applied on top of these knobs (the reference's
+	 * per-pipeline blends, QueryConfig::pipeline_default_blend) */
+	std::vector<std::pair<int, std::string>> overrides;
+
 	std::string str() const;
 	static Flavor parse(const std::string& s);
+	/* the knobs pipeline `id` runs with */
+	Flavor for_pipe(int id) const;
+
+private:
+	static void apply(Flavor& f, const std::string& s);
 };
 
 /* A result column as the caller sees it: the sum of physical result-buffer columns, each

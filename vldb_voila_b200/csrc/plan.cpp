@@ -615,6 +615,7 @@ struct Lowerer {
 	Sink make_agg_sink(const RelOpP& op, Scope& sc, int pi, int* vis, bool allow_wide = false,
 		std::vector<OutCol>* outs = nullptr) {
 		Pipeline& p = out.pipes[pi];
+		const Flavor pf = fl.for_pipe(pi);
 		Sink sink;
 		const int64_t rows = rows_bound(p);
 		std::vector<std::vector<int>> part_shifts; /* per plan aggregate: the shift of each sink part */
@@ -700,11 +701,11 @@ struct Lowerer {
 			sink.domain = domain;
 			__int128 gb = std::min<__int128>(domain, std::max<int64_t>(rows, 1));
 			sink.groups_bound = (int64_t)gb;
-			const bool dense_ok = domain <= (__int128)fl.dense_limit;
-			if (fl.aggr == "dense" && domain > (__int128)(1 << 22)) {
+			const bool dense_ok = domain <= (__int128)pf.dense_limit;
+			if (pf.aggr == "dense" && domain > (__int128)(1 << 22)) {
 				throw Error(kErrUnsupported, "aggr=dense needs a key domain of at most 2^22 slots");
 			}
-			if (fl.aggr == "dense" || (fl.aggr == "auto" && dense_ok)) {
+			if (pf.aggr == "dense" || (pf.aggr == "auto" && dense_ok)) {
 				sink.kind = Sink::AggDense;
 			} else {
 				if (sink.key_bits > 62) {

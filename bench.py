@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--flavor", default="")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--host-resident-only", action="store_true",
+                    help="run only the query over host-resident columns, --steps times (for a profiler)")
     return ap.parse_args()
 
 
@@ -228,10 +230,38 @@ def run_reference_arm(args):
 # ---------------------------------------------------------------------------- our arm
 
 
+def run_host_resident_only(args):
+    """The workload's query over columns left in pinned host memory, run --steps times: what a
+    profiler captures to measure the PCIe bytes of a host-resident step."""
+    import numpy as np
+    import torch
+
+    from vldb_voila_b200 import Engine, generate_workload_host, workload
+    w = workload(spec_of(args.workload))
+    host = generate_workload_host(w)
+    eng = Engine(0)
+    keep = []
+    for t, rows in w.tables.items():
+        eng.create_table(t, rows)
+    for c in w.columns:
+        eng.add_column(c.table, c.name, c.type, c.lo, c.hi)
+        a = np.ascontiguousarray(host[c.table][c.name])
+        keep.append(torch.from_numpy(a.view(np.uint8) if a.dtype != np.uint8 else a).pin_memory())
+        eng.attach_host(c.table, c.name, keep[-1].data_ptr())
+    q = eng.query(w.plan, args.flavor)
+    for _ in range(args.steps):
+        q.run()
+        res = q.result()
+    print(json.dumps({"workload": w.spec, "steps": args.steps, "result_rows": int(len(res))}))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.host_resident_only:
+        return run_host_resident_only(args)
 
     import numpy as np
     import torch

@@ -276,6 +276,9 @@ Query::~Query()
 	for (void* p : allocations) {
 		cudaFree(p);
 	}
+	if (result_host) {
+		cudaFreeHost(result_host);
+	}
 }
 
 static std::map<Query*, QueryState> g_state;
@@ -688,10 +691,23 @@ void query_fetch(Query& q)
 			VC_CHECK_CUDA(cudaEventElapsedTime(&q.last_ms[i], q.ev[2 * i], q.ev[2 * i + 1]));
 		}
 	}
+	/* the result columns land in a pinned staging buffer (kept and grown across runs): a
+	 * pageable destination would take the driver's slower staged copy */
 	const int C = q.plan.result_cols;
-	q.result_host.assign((size_t)C * cnt, 0);
-	for (int c = 0; c < C && cnt > 0; c++) {
-		VC_CHECK_CUDA(cudaMemcpy(q.result_host.data() + (size_t)c * cnt, q.out + (size_t)c * q.out_cap, cnt * 8,
+	const size_t words = std::max<size_t>((size_t)C * cnt, 1);
+	if (words > q.result_host_cap) {
+		if (q.result_host) {
+			VC_CHECK_CUDA(cudaFreeHost(q.result_host));
+			q.result_host = nullptr;
+			q.result_host_cap = 0;
+		}
+		VC_CHECK_CUDA(cudaMallocHost((void**)&q.result_host, words * 8));
+		q.result_host_cap = words;
+	}
+	if (cnt > 0 && (int64_t)cnt == q.out_cap) {
+		VC_CHECK_CUDA(cudaMemcpy(q.result_host, q.out, (size_t)C * cnt * 8, cudaMemcpyDeviceToHost));
+	} else if (cnt > 0) {
+		VC_CHECK_CUDA(cudaMemcpy2D(q.result_host, cnt * 8, q.out, (size_t)q.out_cap * 8, cnt * 8, (size_t)C,
 			cudaMemcpyDeviceToHost));
 	}
 }
@@ -767,6 +783,12 @@ void query_result_int64(Query& q, int64_t* out, int64_t cap)
 		throw Error(1, "result buffer too small");
 	}
 	for (int c = 0; c < C; c++) {
+		const auto& parts = q.plan.out_cols[(size_t)c].parts;
+		if (parts.size() == 1 && parts[0].second == 0) {
+			/* a plain int64 column: copied as is */
+			std::memcpy(out + (size_t)c * R, q.result_host + (size_t)parts[0].first * R, (size_t)R * 8);
+			continue;
+		}
 		for (int64_t r = 0; r < R; r++) {
 			const __int128 v = result_value(q, c, r);
 			if (v < (__int128)INT64_MIN || v > (__int128)INT64_MAX) {
@@ -1421,7 +1443,6 @@ int vc_query_reset(vc_query* q)
 			throw Error(VC_ERR_INVALID, "null query");
 		}
 		q->q.result_rows = -1;
-		q->q.result_host.clear();
 	});
 }
 

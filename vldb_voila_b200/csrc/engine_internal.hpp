@@ -384,7 +384,8 @@ struct Query {
 	bool ran = false;
 	bool dirty = false;                  /* self-cleaning state may be left set: clear before the next run */
 	int64_t result_rows = -1;
-	std::vector<int64_t> result_host;    /* column-major copy of the last result */
+	int64_t* result_host = nullptr;      /* column-major copy of the last result (pinned host memory) */
+	size_t result_host_cap = 0;          /* int64 words allocated at result_host */
 	~Query();
 };
 

@@ -10,7 +10,8 @@ SPECS = ["sel_aggr:rows=1000", "join_aggr:build=100,probe=1000", "groupby:rows=1
 FLAVORS = ["", "cuda(load=tma,stages=2)", "cuda(lowcard=private,prefetch=0)", "cuda(aggr=cache,build=staged)",
            "cuda(compact=0,rows=8,threads=128)", "cuda(hash=voila,compact=-1)", "cuda(build=direct,prefetch=0)",
            "cuda(lowcard=redux,aggr=cache,cache=64)", "cuda(lowcard=atomic,sinksmem=4096)",
-           "cuda(build=direct,probe=8)"]
+           "cuda(build=direct,probe=8)", "cuda(aggr=part)", "cuda(aggr=part,parts=16,stage=2048,threads=128,rows=8)",
+           "cuda(aggr=part,load=tma,stages=2,compact=0)"]
 
 
 def offline(spec):
@@ -199,7 +200,9 @@ def test_join_n_plans_compile(flavor):
     w, e = offline("star:rows=1000,custs=50")
     q = e.query(JOIN_N_PLAN, flavor)
     src = q.source()
-    assert "__any_sync" in src and "1ull) * SPB" in src  # the match loop may walk the whole table
+    # the match loop may walk the whole table; it is block-uniform when the sink stages rows
+    loop = "vd::block_any(anyp)" if "aggr=part" in flavor else "__any_sync"
+    assert loop in src and "1ull) * SPB" in src
     assert "vd::dense_test" not in src
 
 
@@ -274,3 +277,41 @@ def test_per_pipeline_flavor_overrides():
     for bad in ["cuda();p4=cuda(hash=voila)", "cuda();q4=cuda(rows=2)", "cuda();p4=cuda(rows=3)"]:
         with pytest.raises(VoilaError):
             e.query(w.plan, bad)
+
+
+def test_partitioned_aggregation_plan():
+    """aggr=part: pass 1 stages records and flushes partition-ordered runs, pass 2 is a
+    persistent kernel over partitions that writes the result rows itself (no group table, no
+    extraction scan)."""
+    w, e = offline("groupby:rows=6000000,keys=1500000,zipf=0,seed=3")
+    q = e.query(w.plan, "cuda(aggr=part)")
+    src = q.source()
+    info = q.info()
+    assert "pflush()" in src and "vd::block_excl_scan(shist, soff, 1024" in src  # 2 x 1.5M / 4096 slots
+    assert "vd::st_find_or_insert(skeys, 4096" in src and "gt_find_or_insert" not in src
+    k = {x["name"]: x for x in info["kernels"]}
+    assert k["vc_p0_extract"]["threads"] == 512
+    # records of key + two value fields fit one word; 8192 staged records + 1024 x 2 counters
+    assert k["vc_p0_main"]["smem"] == 8192 * 8 + 8192 * 4 + 1024 * 8
+    # an explicit partition count and stage size
+    src2 = e.query(w.plan, "cuda(aggr=part,parts=2048,stage=4096,threads=512)").source()
+    assert "vd::block_excl_scan(shist, soff, 2048" in src2 and "+ 2048u > 4096u" in src2
+    # too few partitions for the groups bound: falls back to the global table
+    assert "gt_find_or_insert" in e.query(w.plan, "cuda(aggr=part,parts=16)").source()
+
+
+@pytest.mark.parametrize("flavor", ["cuda(parts=24)", "cuda(parts=8)", "cuda(stage=1000)", "cuda(stage=32768)"])
+def test_bad_partition_knobs_are_rejected(flavor):
+    w, e = offline("groupby:rows=1000,keys=100000")
+    with pytest.raises(VoilaError) as ex:
+        e.query(w.plan, flavor)
+    assert ex.value.code == 1
+
+
+def test_partitioned_aggregation_is_not_batched():
+    from vldb_voila_b200.engine import Batch
+    w, e = offline("groupby:rows=100000,keys=100000")
+    q = e.query(w.plan, "cuda(aggr=part)")
+    with pytest.raises(VoilaError) as ex:
+        Batch([q])
+    assert ex.value.code == 6 and "aggr=part" in str(ex.value)

@@ -17,7 +17,8 @@ FLAVORS = ["", "cuda(rows=8,threads=128,load=tma,stages=3)", "cuda(aggr=cache,ca
            "cuda(load=tma,build=staged,rows=2,lowcard=atomic)", "cuda(compact=0,lowcard=private,rows=8)",
            "cuda(hash=voila,lowcard=private,threads=128,fill=75)", "cuda(build=direct,prefetch=0)",
            "cuda(lowcard=redux,aggr=cache,cache=64)", "cuda(build=direct,probe=4,rows=2)",
-           "cuda(build=staged,probe=32,compact=-1)"]
+           "cuda(build=staged,probe=32,compact=-1)", "cuda(aggr=part)",
+           "cuda(aggr=part,parts=16,stage=2048,threads=128,rows=8,load=tma,stages=2)"]
 
 
 def run_gpu(w, plan, flavor="", on_device=False, data=None):
@@ -58,7 +59,8 @@ def test_full_size_vs_oracle(spec):
     # the device generator produces the same columns; run from them (no host upload)
     e = Engine(0)
     e.load_workload(w, on_device=True)
-    for flavor in ["", "cuda(load=tma)", "cuda(build=staged,aggr=cache)", "cuda(build=direct)"]:
+    for flavor in ["", "cuda(load=tma)", "cuda(build=staged,aggr=cache)", "cuda(build=direct)", "cuda(aggr=part)",
+                   "cuda(aggr=part,threads=512,parts=256)"]:
         q = e.query(w.plan, flavor)
         q.run()
         assert q.result_lines() == expect, flavor
@@ -98,7 +100,7 @@ EDGE_SPECS = [
 
 @pytest.mark.parametrize("spec", EDGE_SPECS)
 @pytest.mark.parametrize("flavor", ["", "cuda(rows=2,threads=32,aggr=global)", "cuda(load=tma,build=staged)",
-                                    "cuda(build=direct,rows=1)"])
+                                    "cuda(build=direct,rows=1)", "cuda(aggr=part,rows=1,threads=64)"])
 def test_edge_cases_vs_oracle(spec, flavor):
     """Empty and ragged inputs, no matches, single keys (the reference itself asserts on
     empty base tables, codegen.cpp:445, so the oracle is the only checker there)."""
@@ -114,11 +116,13 @@ def test_rerun_and_reset_are_idempotent():
     expect = result_lines(run_plan(w.plan, data))
     e = Engine(0)
     e.load_workload(w, data=data)
-    q = e.query(w.plan, "cuda(aggr=cache)")
-    for _ in range(3):
-        q.run()
-        assert q.result_lines() == expect
-        q.reset()
+    for flavor in ["cuda(aggr=cache)", "cuda(aggr=part)"]:
+        q = e.query(w.plan, flavor)
+        for _ in range(3):
+            q.run()
+            assert q.result_lines() == expect, flavor
+            q.reset()
+        q.close()
 
 
 def test_capacity_error_is_reported_not_faulted():

@@ -57,6 +57,108 @@ static int64_t pow2_at_least(int64_t x)
 	return p;
 }
 
+/* bits of hi - lo for a value of bounds b (64 when the span does not fit 64 bits) */
+static int span_bits(const Bounds& b)
+{
+	const __int128 span = b.hi - b.lo;
+	if (span < 0 || span >= ((__int128)1 << 64)) {
+		return 64;
+	}
+	int bits = 0;
+	for (unsigned __int128 x = (unsigned __int128)span; x; x >>= 1) {
+		bits++;
+	}
+	return std::max(bits, 1);
+}
+
+/* segments an aggregation item loads into shared memory at a time */
+static constexpr int kPartSegs = 1024;
+
+PartPlan part_plan(const Pipeline& p, const LoweredPlan& plan, const Flavor& f, int sms)
+{
+	PartPlan pp;
+	const Sink& s = p.sink;
+	if (f.aggr != "part" || s.kind != Sink::AggHash || s.key_bits > 31 || s.count_idx < 0) {
+		return PartPlan();
+	}
+	/* record: the packed key in the low bits of word 0, then each summed value (minus its
+	 * lower bound) in a field of its span's width; a field never straddles two words */
+	int word = 0, off = s.key_bits;
+	pp.rec_word.assign(s.aggs.size(), -1);
+	pp.rec_off.assign(s.aggs.size(), 0);
+	for (size_t a = 0; a < s.aggs.size(); a++) {
+		if (s.aggs[a].count) {
+			continue;
+		}
+		const int bits = span_bits(s.aggs[a].arg->b);
+		if (bits >= 64) {
+			return PartPlan();
+		}
+		if (off + bits > 64) {
+			word++;
+			off = 0;
+		}
+		if (word >= 2) {
+			return PartPlan();
+		}
+		pp.rec_word[a] = word;
+		pp.rec_off[a] = off;
+		off += bits;
+	}
+	pp.rec_words = word + 1;
+	const int W = s.nwords;
+	/* a partition's table: the most slots whose keys and words fit 96 KiB */
+	int S = 16384;
+	while (S > 1024 && (size_t)S * (4 + 8 * (size_t)W) > 96 * 1024) {
+		S >>= 1;
+	}
+	if ((size_t)S * (4 + 8 * (size_t)W) > 96 * 1024) {
+		return PartPlan();
+	}
+	const int64_t groups = std::max<int64_t>(s.groups_bound, 1);
+	int64_t P = f.parts ? f.parts : std::min<int64_t>(2048, std::max<int64_t>(16, pow2_at_least((groups * 2 + S - 1) / S)));
+	/* on average a partition's table is at most three quarters full */
+	if (groups > P * S * 3 / 4) {
+		return PartPlan();
+	}
+	pp.P = (int)P;
+	while ((1 << pp.log2P) < pp.P) {
+		pp.log2P++;
+	}
+	pp.S = S;
+	const int TV = f.threads * f.rows;
+	int C = f.stage ? f.stage : 8192;
+	while (C < 2 * TV) {
+		C <<= 1;
+	}
+	if (C > 16384) {
+		return PartPlan();
+	}
+	pp.C = C;
+	pp.smem1 = (size_t)C * 8 * pp.rec_words + (size_t)C * 4 + (size_t)P * 8;
+	if (pp.smem1 > 200 * 1024) {
+		return PartPlan();
+	}
+	bool joinn = false;
+	for (auto& op : p.ops) {
+		joinn = joinn || (op.kind == Op::Probe && !plan.joins[op.join].join01);
+	}
+	const int64_t rows = std::max<int64_t>(p.rows, 1);
+	pp.cap = joinn ? 4 * rows + (1 << 20) : rows;
+	/* every flush but a CTA's last holds more than C - TV records */
+	const int64_t grid_max = (int64_t)sms * std::max(1, 2048 / f.threads);
+	pp.fmax = (pp.cap + (C - TV) - 1) / (C - TV) + grid_max + 1;
+	pp.R = std::max<int64_t>(4 * (int64_t)S, (pp.cap + 2047) / 2048);
+	pp.max_items = P + pp.cap / pp.R + 1;
+	/* a split item leaves at most min(S, its records) groups; split items hold at least R / 2
+	 * records each */
+	pp.scratch = std::min<int64_t>(pp.cap, (2 * pp.cap / pp.R + 1) * S) + S;
+	pp.smem2 = (size_t)S * 4 + (size_t)S * W * 8 + (size_t)kPartSegs * 8 + (size_t)kPartSegs * 4 +
+		(size_t)(kPartSegs + 1) * 4 + (size_t)P * 12;
+	pp.smem2 = (pp.smem2 + 15) & ~(size_t)15;
+	return pp;
+}
+
 namespace {
 
 struct PipeGen {
@@ -78,12 +180,12 @@ struct PipeGen {
 	bool leader_plain = false; /* each warp owns a copy: group leaders update it without atomics */
 	std::map<const BExpr*, int> const_slot; /* parameter slot of each constant node */
 	bool private_acc = false;  /* per-thread private accumulators (lowcard=private) */
-	static constexpr int kGmax = 8; /* distinct groups per block held in private accumulators */
+	int kGmax = 8;             /* distinct groups per block held in private accumulators (pgroups) */
 	static constexpr int kExtractK = 4; /* slot groups per warp step of the group extraction */
 
 	PipeGen(Pipeline& pp, LoweredPlan& pl, const Flavor& f, const PipeDeviceState& s, const QueryDeviceState& q,
 		std::vector<unsigned long long>& prm)
-		: p(pp), plan(pl), fl(f), st(s), qs(q), params(prm), V(f.rows), T(f.threads) {
+		: p(pp), plan(pl), fl(f), st(s), qs(q), params(prm), V(f.rows), T(f.threads), kGmax(f.private_groups) {
 		name = "vc_p" + std::to_string(p.id);
 	}
 
@@ -151,6 +253,9 @@ struct PipeGen {
 	}
 
 	int A() const { return (int)p.sink.aggs.size(); }
+	/* partitioned aggregation (aggr=part) of a standalone pipeline */
+	bool part() const { return st.part.P > 0 && !item; }
+	std::string rec_type() const { return st.part.rec_words == 2 ? "ulonglong2" : "unsigned long long"; }
 	/* stored key width of the split hash group table */
 	int gkey_bytes() const { return p.sink.key_bits <= 31 ? 4 : 8; }
 	std::string gkey_type() const { return p.sink.key_bits <= 31 ? "uint32_t" : "uint64_t"; }
@@ -620,7 +725,7 @@ struct PipeGen {
 	/* sinks whose rows use block-wide collectives (appends): loops around them must be
 	 * uniform over the block, not just the warp */
 	bool sink_block_collective() const {
-		return p.sink.kind == Sink::Emit ||
+		return p.sink.kind == Sink::Emit || (p.sink.kind == Sink::AggHash && part()) ||
 			(p.sink.kind == Sink::JoinBuild && !plan.joins[p.sink.join].direct && !plan.joins[p.sink.join].dense);
 	}
 
@@ -1025,6 +1130,10 @@ struct PipeGen {
 			break;
 		}
 		case Sink::AggHash: {
+			if (part()) {
+				part_prologue();
+				break;
+			}
 			const std::string K = gkey_type();
 			const int W = s.nwords;
 			o << "  " << K << "* const gkeys = " << Pptr(st.sink_dev, K + "*") << ";\n";
@@ -1134,6 +1243,10 @@ struct PipeGen {
 			std::vector<Bounds> kb;
 			for (auto& k : s.keys) {
 				kb.push_back(k->b);
+			}
+			if (part()) {
+				part_row(kb);
+				break;
 			}
 			const std::string K = gkey_type();
 			const int W = s.nwords;
@@ -1262,6 +1375,345 @@ struct PipeGen {
 		o << "      }\n    }\n  }\n";
 	}
 
+	/* ------------------------------------------------------- partitioned aggregation ---- */
+
+	/* pass 1 state: the CTA's staged records (shared memory: records, then per record its
+	 * partition << 16 | rank, then per partition its staged count and its offset in the
+	 * flush) and the flush that writes them out as one partition-ordered run */
+	void part_prologue() {
+		const PartPlan& pp = st.part;
+		const int NP = pp.P;
+		const std::string RT = rec_type();
+		smem_sink = pp.smem1;
+		o << "  unsigned long long* const pctl = " << Pptr(pp.ctl, "unsigned long long*") << ";\n";
+		o << "  unsigned long long* const ptot = pctl + 4;\n";
+		o << "  " << RT << "* const pbuf = " << Pptr(pp.buf, RT + "*") << ";\n";
+		o << "  unsigned long long* const pseg = " << Pptr(pp.seg, "unsigned long long*") << ";\n";
+		o << "  const unsigned long long pcap = " << Pu((unsigned long long)pp.cap) << ";\n";
+		o << "  const unsigned long long pfmax = " << Pu((unsigned long long)pp.fmax) << ";\n";
+		o << "  " << RT << "* const srec = (" << RT << "*)vd_smem;\n";
+		o << "  uint32_t* const smeta = (uint32_t*)(vd_smem + " << (size_t)pp.C * 8 * pp.rec_words << ");\n";
+		o << "  uint32_t* const shist = smeta + " << pp.C << ";\n";
+		o << "  uint32_t* const soff = shist + " << NP << ";\n";
+		o << "  __shared__ uint32_t pscan[33];\n";
+		o << "  __shared__ unsigned long long pfl[2];\n";
+		o << "  __shared__ uint32_t pcount;\n";
+		o << "  for (int i = threadIdx.x; i < " << NP << "; i += blockDim.x) { shist[i] = 0u; }\n";
+		o << "  if (threadIdx.x == 0) { pcount = 0u; }\n";
+		o << "  vd::block_sync();\n";
+		o << "  auto pflush = [&]() {\n";
+		o << "    const uint32_t pn = *(volatile uint32_t*)&pcount;\n";
+		o << "    vd::block_excl_scan(shist, soff, " << NP << ", pscan);\n";
+		o << "    if (threadIdx.x == 0) {\n";
+		o << "      pfl[0] = atomicAdd(&pctl[0], (unsigned long long)pn);\n";
+		o << "      pfl[1] = atomicAdd(&pctl[1], 1ull);\n";
+		o << "    }\n";
+		o << "    vd::block_sync();\n";
+		o << "    const unsigned long long pb = pfl[0], pf = pfl[1];\n";
+		o << "    if (pb + pn <= pcap && pf < pfmax) {\n";
+		o << "      for (uint32_t i = threadIdx.x; i < pn; i += blockDim.x) {\n";
+		o << "        const uint32_t m = smeta[i];\n";
+		o << "        pbuf[pb + soff[m >> 16] + (m & 0xffffu)] = srec[i];\n";
+		o << "      }\n";
+		o << "      for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) {\n";
+		o << "        const uint32_t c = shist[q];\n";
+		o << "        pseg[pf * " << NP << "ull + q] = ((pb + soff[q]) << 16) | c;\n";
+		o << "        if (c) { atomicAdd(&ptot[q], (unsigned long long)c); }\n";
+		o << "        shist[q] = 0u;\n";
+		o << "      }\n";
+		o << "    } else {\n";
+		o << "      if (threadIdx.x == 0) { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
+		o << "      for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) { shist[q] = 0u; }\n";
+		o << "    }\n";
+		o << "    if (threadIdx.x == 0) { pcount = 0u; }\n";
+		o << "    vd::block_sync();\n";
+		o << "  };\n";
+	}
+
+	/* pass 1 per row: the record, its partition (the top log2 P bits of the key's hash) and
+	 * its staging position; a stage without room for another round of rows is flushed first */
+	void part_row(const std::vector<Bounds>& kb) {
+		const PartPlan& pp = st.part;
+		const Sink& s = p.sink;
+		o << "    vd::block_sync();\n";
+		o << "    if (*(volatile uint32_t*)&pcount + " << T * V << "u > " << pp.C << "u) { pflush(); }\n";
+		o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
+		o << "      uint64_t rw[2] = {0ull, 0ull};\n";
+		o << "      uint32_t pt = 0u;\n";
+		o << "      if (act[v]) {\n";
+		o << "        const uint64_t pk = " << packed_key(s.keys, kb, s.key_shift, "v") << ";\n";
+		o << "        rw[0] = pk;\n";
+		for (int a = 0; a < A(); a++) {
+			if (s.aggs[a].count) {
+				continue;
+			}
+			const std::string lo = P((unsigned long long)(int64_t)s.aggs[a].arg->b.lo);
+			o << "        rw[" << pp.rec_word[a] << "] |= ((uint64_t)(" << expr(s.aggs[a].arg, "v") << ") - (uint64_t)" << lo
+			  << ") << " << pp.rec_off[a] << ";\n";
+		}
+		o << "        pt = (uint32_t)vd::mix_hash32((uint32_t)pk) >> " << 32 - pp.log2P << ";\n";
+		o << "      }\n";
+		o << "      const unsigned bm = __ballot_sync(0xffffffffu, act[v]);\n";
+		o << "      uint32_t wb = 0u;\n";
+		o << "      if (vd::lane_id() == 0u && bm) { wb = atomicAdd(&pcount, (uint32_t)__popc(bm)); }\n";
+		o << "      wb = __shfl_sync(0xffffffffu, wb, 0);\n";
+		o << "      if (act[v]) {\n";
+		o << "        const uint32_t pos = wb + (uint32_t)__popc(bm & vd::lanemask_lt());\n";
+		o << "        const uint32_t rank = atomicAdd(&shist[pt], 1u);\n";
+		if (pp.rec_words == 2) {
+			o << "        srec[pos] = make_ulonglong2(rw[0], rw[1]);\n";
+		} else {
+			o << "        srec[pos] = rw[0];\n";
+		}
+		o << "        smeta[pos] = (pt << 16) | rank;\n";
+		o << "      }\n";
+		o << "    }\n";
+	}
+
+	/* pass 2: the persistent aggregation kernel over work items (one partition, or a share of
+	 * the flushes of a partition holding more than R records) */
+	std::string gen_part_aggregate() {
+		const PartPlan& pp = st.part;
+		const Sink& s = p.sink;
+		const int NP = pp.P, S = pp.S, W = s.nwords, AT = pp.agg_threads;
+		const int U = 4; /* record loads in flight per thread */
+		const std::string RT = rec_type();
+		std::ostringstream k;
+		k << "extern \"C\" __global__ void __launch_bounds__(" << AT << ") " << name << "_extract(const VcParams p) {\n";
+		k << "  vd::pdl_launch_dependents();\n  vd::pdl_wait();\n";
+		k << "  unsigned* const err = (unsigned*)p.v[" << p.err_slot << "];\n";
+		k << "  int64_t* const out = " << Pptr(qs.out, "int64_t*") << ";\n";
+		k << "  const int64_t ocap = " << P((unsigned long long)qs.out_cap) << ";\n";
+		k << "  unsigned long long* const ocount = " << Pptr(qs.out_count, "unsigned long long*") << ";\n";
+		k << "  unsigned long long* const pctl = " << Pptr(pp.ctl, "unsigned long long*") << ";\n";
+		k << "  const unsigned long long* const ptot = pctl + 4;\n";
+		k << "  unsigned* const pdone = (unsigned*)(pctl + 4 + " << NP << ");\n";
+		k << "  const " << RT << "* __restrict__ pbuf = " << Pptr(pp.buf, "const " + RT + "*") << ";\n";
+		k << "  const unsigned long long* __restrict__ pseg = " << Pptr(pp.seg, "const unsigned long long*") << ";\n";
+		k << "  uint32_t* const xkeys = " << Pptr(pp.skeys, "uint32_t*") << ";\n";
+		k << "  unsigned long long* const xacc = " << Pptr(pp.sacc, "unsigned long long*") << ";\n";
+		k << "  unsigned long long* const xitems = " << Pptr(pp.items, "unsigned long long*") << ";\n";
+		k << "  const unsigned long long R = " << Pu((unsigned long long)pp.R) << ";\n";
+		k << "  const unsigned long long fmax = " << Pu((unsigned long long)pp.fmax) << ";\n";
+		k << "  const unsigned long long xcap = " << Pu((unsigned long long)pp.scratch) << ";\n";
+		k << "  extern __shared__ __align__(128) unsigned char vd_smem[];\n";
+		k << "  uint32_t* const skeys = (uint32_t*)vd_smem;\n";
+		k << "  unsigned long long* const sacc = (unsigned long long*)(vd_smem + " << (size_t)S * 4 << ");\n";
+		k << "  unsigned long long* const sseg = sacc + " << (size_t)S * W << ";\n";
+		k << "  uint32_t* const scnt = (uint32_t*)(sseg + " << kPartSegs << ");\n";
+		k << "  uint32_t* const spre = scnt + " << kPartSegs << ";\n";
+		k << "  uint32_t* const sk = spre + " << kPartSegs + 1 << ";\n";
+		k << "  uint32_t* const sa = sk + " << NP << ";\n";
+		k << "  uint32_t* const sb = sa + " << NP << ";\n";
+		k << "  __shared__ uint32_t xscan[33];\n";
+		k << "  __shared__ unsigned long long xres[33];\n";
+		k << "  __shared__ uint32_t xitem, xlast;\n";
+		k << "  __shared__ unsigned long long xrun;\n";
+		k << "  for (int i = threadIdx.x; i < " << S << "; i += blockDim.x) { skeys[i] = 0u; }\n";
+		k << "  for (int i = threadIdx.x; i < " << S * W << "; i += blockDim.x) { sacc[i] = 0ull; }\n";
+		/* items: every split partition's items first (by partition), then the partitions
+		 * that fit one item; the two counts' inputs borrow the segment arrays */
+		k << "  uint32_t* const ka = (uint32_t*)sseg;\n";
+		k << "  uint32_t* const kb1 = ka + " << NP << ";\n";
+		k << "  for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) {\n";
+		k << "    const unsigned long long t = __ldcg(&ptot[q]);\n";
+		k << "    const uint32_t kq = (uint32_t)((t + R - 1ull) / R);\n";
+		k << "    sk[q] = kq;\n    ka[q] = kq >= 2u ? kq : 0u;\n    kb1[q] = kq == 1u ? 1u : 0u;\n";
+		k << "  }\n";
+		k << "  vd::block_sync();\n";
+		k << "  const uint32_t nA = vd::block_excl_scan(ka, sa, " << NP << ", xscan);\n";
+		k << "  const uint32_t nB = vd::block_excl_scan(kb1, sb, " << NP << ", xscan);\n";
+		k << "  const unsigned long long nf = __ldcg(&pctl[1]);\n";
+		k << "  const uint32_t F = (uint32_t)(nf < fmax ? nf : fmax);\n";
+		k << "  for (;;) {\n";
+		k << "    if (threadIdx.x == 0) { xitem = (uint32_t)atomicAdd(&pctl[2], 1ull); }\n";
+		k << "    vd::block_sync();\n";
+		k << "    const uint32_t item = xitem;\n";
+		k << "    if (item >= nA + nB) { break; }\n";
+		k << "    int q;\n    uint32_t j, kq;\n";
+		k << "    if (item < nA) { q = vd::last_at_most(sa, " << NP << ", item); j = item - sa[q]; kq = sk[q]; }\n";
+		k << "    else { q = vd::last_at_most(sb, " << NP << ", item - nA); j = 0u; kq = 1u; }\n";
+		k << "    const uint32_t f0 = (uint32_t)((uint64_t)j * F / kq), f1 = (uint32_t)((uint64_t)(j + 1u) * F / kq);\n";
+		k << "    for (uint32_t fb = f0; fb < f1; fb += " << kPartSegs << "u) {\n";
+		k << "      const int nseg = (int)min((uint32_t)" << kPartSegs << ", f1 - fb);\n";
+		k << "      for (int i = threadIdx.x; i < nseg; i += blockDim.x) {\n";
+		k << "        const unsigned long long sw = __ldcg(&pseg[(uint64_t)(fb + (uint32_t)i) * " << NP << "ull + (uint64_t)q]);\n";
+		k << "        sseg[i] = sw;\n        scnt[i] = (uint32_t)(sw & 0xffffull);\n";
+		k << "      }\n";
+		k << "      vd::block_sync();\n";
+		k << "      const uint32_t tot = vd::block_excl_scan(scnt, spre, nseg, xscan);\n";
+		k << "      for (uint32_t base = 0; base < tot; base += blockDim.x * " << U << "u) {\n";
+		k << "        " << RT << " r[" << U << "];\n        bool live[" << U << "];\n";
+		k << "#pragma unroll\n        for (int u = 0; u < " << U << "; u++) {\n";
+		k << "          const uint32_t jj = base + (uint32_t)u * blockDim.x + threadIdx.x;\n";
+		k << "          live[u] = jj < tot;\n";
+		k << "          if (live[u]) {\n";
+		k << "            const int sg = vd::seg_of(spre, nseg, jj);\n";
+		k << "            r[u] = __ldcs(&pbuf[(sseg[sg] >> 16) + (jj - spre[sg])]);\n";
+		k << "          }\n";
+		k << "        }\n";
+		const std::string w0 = pp.rec_words == 2 ? "r[u].x" : "r[u]";
+		const std::string w1 = pp.rec_words == 2 ? "r[u].y" : "r[u]";
+		const unsigned long long kmask = (1ull << s.key_bits) - 1ull;
+		k << "#pragma unroll\n        for (int u = 0; u < " << U << "; u++) {\n";
+		k << "          const uint32_t pk = live[u] ? (uint32_t)(" << w0 << " & " << kmask << "ull) : 0xffffffffu;\n";
+		k << "          const unsigned gm = __match_any_sync(0xffffffffu, pk);\n";
+		k << "          const bool lead = live[u] && (gm & vd::lanemask_lt()) == 0u;\n";
+		k << "          uint64_t w[" << W << "] = {";
+		for (int i = 0; i < W; i++) {
+			k << (i ? ", " : "") << "0ull";
+		}
+		k << "};\n";
+		for (int a = 0; a < A(); a++) {
+			const std::string sh = std::to_string(s.agg_shift[a]);
+			if (s.aggs[a].count) {
+				k << "          w[" << s.agg_word[a] << "] += (uint64_t)__popc(gm) << " << sh << ";\n";
+				continue;
+			}
+			const int bits = span_bits(s.aggs[a].arg->b);
+			const unsigned long long fmask = (1ull << bits) - 1ull;
+			k << "          w[" << s.agg_word[a] << "] += vd::group_sum_u<" << bits << ">(gm, live[u] ? (("
+			  << (pp.rec_word[a] == 1 ? w1 : w0) << " >> " << pp.rec_off[a] << ") & " << fmask << "ull) : 0ull) << " << sh
+			  << ";\n";
+		}
+		k << "          if (lead) {\n";
+		k << "            const int sl = vd::st_find_or_insert(skeys, " << S << ", (uint32_t)vd::mix_hash32(pk), pk + 1u);\n";
+		k << "            if (sl >= 0) {\n";
+		k << "#pragma unroll\n              for (int a = 0; a < " << W << "; a++) { if (w[a]) { atomicAdd(&sacc[sl * " << W
+		  << " + a], (unsigned long long)w[a]); } }\n";
+		k << "            } else { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
+		k << "          }\n";
+		k << "        }\n";
+		k << "      }\n";
+		k << "      vd::block_sync();\n";
+		k << "    }\n";
+		/* a split partition's item: leave the groups in a scratch run; the last item merges */
+		k << "    bool emit = kq == 1u;\n";
+		k << "    if (kq > 1u) {\n";
+		k << "      uint32_t ng = 0u;\n";
+		k << "      for (int s0 = 0; s0 < " << S << "; s0 += blockDim.x) {\n";
+		k << "        uint32_t n1;\n";
+		k << "        vd::block_rank(skeys[s0 + threadIdx.x] != 0u, xscan, &n1);\n";
+		k << "        ng += n1;\n";
+		k << "      }\n";
+		k << "      if (threadIdx.x == 0) {\n";
+		k << "        const unsigned long long x0 = atomicAdd(&pctl[3], (unsigned long long)ng);\n";
+		k << "        if (x0 + ng > xcap) { atomicOr(err, VD_ERR_TABLE_FULL); ng = 0u; }\n";
+		k << "        xrun = (x0 << 16) | ng;\n";
+		k << "        xitems[item] = xrun;\n";
+		k << "      }\n";
+		k << "      vd::block_sync();\n";
+		k << "      const unsigned long long x0 = xrun >> 16;\n";
+		k << "      const uint32_t nrun = (uint32_t)(xrun & 0xffffull);\n";
+		k << "      uint32_t wpos = 0u;\n";
+		k << "      for (int s0 = 0; s0 < " << S << "; s0 += blockDim.x) {\n";
+		k << "        const int sl = s0 + (int)threadIdx.x;\n";
+		k << "        const uint32_t key = skeys[sl];\n";
+		k << "        uint32_t n1;\n";
+		k << "        const uint32_t rk = vd::block_rank(key != 0u, xscan, &n1);\n";
+		k << "        if (key != 0u && wpos + rk < nrun) {\n";
+		k << "          xkeys[x0 + wpos + rk] = key;\n";
+		k << "#pragma unroll\n          for (int a = 0; a < " << W << "; a++) { xacc[(x0 + wpos + rk) * " << W << "ull + a] = sacc[sl * "
+		  << W << " + a]; }\n";
+		k << "        }\n";
+		k << "        wpos += n1;\n";
+		k << "      }\n";
+		k << "      __threadfence();\n";
+		k << "      vd::block_sync();\n";
+		k << "      if (threadIdx.x == 0) { xlast = atomicAdd(&pdone[q], 1u) == kq - 1u ? 1u : 0u; }\n";
+		k << "      vd::block_sync();\n";
+		k << "      if (xlast) {\n";
+		k << "        __threadfence();\n";
+		k << "        for (uint32_t it = sa[q]; it < sa[q] + kq; it++) {\n";
+		k << "          if (it == item) { continue; }\n";
+		k << "          const unsigned long long run = __ldcg(&xitems[it]);\n";
+		k << "          const unsigned long long b2 = run >> 16;\n";
+		k << "          const uint32_t n2 = (uint32_t)(run & 0xffffull);\n";
+		k << "          for (uint32_t e = threadIdx.x; e < n2; e += blockDim.x) {\n";
+		k << "            const uint32_t key = __ldcg(&xkeys[b2 + e]);\n";
+		k << "            const int sl = vd::st_find_or_insert(skeys, " << S << ", (uint32_t)vd::mix_hash32(key - 1u), key);\n";
+		k << "            if (sl >= 0) {\n";
+		k << "#pragma unroll\n              for (int a = 0; a < " << W << "; a++) {\n";
+		k << "                const unsigned long long wv = __ldcg(&xacc[(b2 + e) * " << W << "ull + a]);\n";
+		k << "                if (wv) { atomicAdd(&sacc[sl * " << W << " + a], wv); }\n";
+		k << "              }\n";
+		k << "            } else { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
+		k << "          }\n";
+		k << "        }\n";
+		k << "        vd::block_sync();\n";
+		k << "        emit = true;\n";
+		k << "      } else {\n";
+		k << "        for (int i = threadIdx.x; i < " << S << "; i += blockDim.x) {\n";
+		k << "          if (skeys[i] != 0u) {\n            skeys[i] = 0u;\n";
+		k << "#pragma unroll\n            for (int a = 0; a < " << W << "; a++) { sacc[i * " << W << " + a] = 0ull; }\n";
+		k << "          }\n        }\n";
+		k << "        vd::block_sync();\n";
+		k << "      }\n";
+		k << "    }\n";
+		/* the partition's result rows; the table is left clear for the next item */
+		auto field = [&](int a) {
+			const int bits = s.agg_bits[a];
+			const unsigned long long mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
+			return "((w[" + std::to_string(s.agg_word[a]) + "] >> " + std::to_string(s.agg_shift[a]) + ") & " +
+				std::to_string(mask) + "ull)";
+		};
+		/* one reservation of result rows per item: count the groups, then write them */
+		k << "    if (emit) {\n";
+		k << "      uint32_t ng = 0u;\n";
+		k << "      for (int s0 = 0; s0 < " << S << "; s0 += blockDim.x) {\n";
+		k << "        uint32_t n1;\n";
+		k << "        vd::block_rank(skeys[s0 + threadIdx.x] != 0u, xscan, &n1);\n";
+		k << "        ng += n1;\n";
+		k << "      }\n";
+		k << "      if (threadIdx.x == 0) { xres[0] = ng ? atomicAdd(ocount, (unsigned long long)ng) : 0ull; }\n";
+		k << "      vd::block_sync();\n";
+		k << "      const int64_t obase = (int64_t)xres[0];\n";
+		k << "      uint32_t wpos = 0u;\n";
+		k << "      for (int s0 = 0; s0 < " << S << "; s0 += blockDim.x) {\n";
+		k << "        const int sl = s0 + (int)threadIdx.x;\n";
+		k << "        const uint32_t key = skeys[sl];\n";
+		k << "        uint32_t n1;\n";
+		k << "        const uint32_t rk = vd::block_rank(key != 0u, xscan, &n1);\n";
+		k << "        const int64_t pos = obase + (int64_t)(wpos + rk);\n";
+		k << "        wpos += n1;\n";
+		k << "        uint64_t w[" << W << "];\n";
+		k << "#pragma unroll\n        for (int a = 0; a < " << W << "; a++) { w[a] = key != 0u ? sacc[sl * " << W << " + a] : 0ull; }\n";
+		k << "        const bool take = key != 0u && (int64_t)" << field(s.count_idx) << " > 0;\n";
+		k << "        if (take && pos < ocap) {\n";
+		k << "          const int64_t cnt = (int64_t)" << field(s.count_idx) << ";\n";
+		int col = 0;
+		for (size_t kk = 0; kk < s.keys.size(); kk++, col++) {
+			const std::string lo = P((unsigned long long)(int64_t)s.keys[kk]->b.lo);
+			const int bits = (kk + 1 < s.keys.size() ? s.key_shift[kk + 1] : s.key_bits) - s.key_shift[kk];
+			const unsigned long long mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
+			k << "          out[" << col << " * ocap + pos] = " << lo << " + (int64_t)((((uint64_t)key - 1ull) >> "
+			  << s.key_shift[kk] << ") & " << mask << "ull);\n";
+		}
+		for (int a = 0; a < A(); a++) {
+			if (!s.aggs[a].visible) {
+				continue;
+			}
+			if (s.aggs[a].count) {
+				k << "          out[" << col << " * ocap + pos] = cnt;\n";
+			} else {
+				const std::string lo = P((unsigned long long)(int64_t)s.aggs[a].arg->b.lo);
+				k << "          out[" << col << " * ocap + pos] = (int64_t)(" << field(a) << " + (uint64_t)" << lo
+				  << " * (uint64_t)cnt);\n";
+			}
+			col++;
+		}
+		k << "        }\n";
+		k << "        if (key != 0u) {\n          skeys[sl] = 0u;\n";
+		k << "#pragma unroll\n          for (int a = 0; a < " << W << "; a++) { sacc[sl * " << W << " + a] = 0ull; }\n";
+		k << "        }\n";
+		k << "      }\n";
+		k << "      vd::block_sync();\n";
+		k << "    }\n";
+		k << "  }\n";
+		k << "}\n\n";
+		return k.str();
+	}
+
 	void sink_epilogue() {
 		Sink& s = p.sink;
 		switch (s.kind) {
@@ -1309,6 +1761,11 @@ struct PipeGen {
 			publish_slots("g", (int64_t)s.domain);
 			break;
 		case Sink::AggHash:
+			if (part()) {
+				o << "  vd::block_sync();\n";
+				o << "  if (*(volatile uint32_t*)&pcount > 0u) { pflush(); }\n";
+				break;
+			}
 			if (fl.aggr == "cache") {
 				const std::string K = gkey_type();
 				const int W = s.nwords;
@@ -1491,7 +1948,7 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 		if (p.sink.kind == Sink::JoinBuild && !plan.joins[p.sink.join].direct) {
 			extra = g.gen_join_build();
 		} else if (p.sink.kind == Sink::AggHash) {
-			extra = g.gen_extract();
+			extra = g.part() ? g.gen_part_aggregate() : g.gen_extract();
 		}
 		src << "#define VcParams VcParams" << p.id << "\n";
 		src << "struct VcParams" << p.id << " { unsigned long long v[" << std::max<size_t>(prm.size(), 1) << "]; };\n";
@@ -1529,8 +1986,15 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 			e.kernel = g.name + "_extract";
 			e.pipe = p.id;
 			e.stage = 1;
-			e.threads = 256;
-			e.grid_items = (st[p.id].sink_cap + 256 * 4 - 1) / (256 * 4);
+			if (g.part()) {
+				/* persistent: work items are taken from a counter */
+				e.threads = st[p.id].part.agg_threads;
+				e.smem = st[p.id].part.smem2;
+				e.grid_items = 0;
+			} else {
+				e.threads = 256;
+				e.grid_items = (st[p.id].sink_cap + 256 * 4 - 1) / (256 * 4);
+			}
 			gc.launches.push_back(e);
 		}
 	}
@@ -1656,6 +2120,10 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 			/* the query keeps its own parameter layout for standalone runs */
 			const int saved_err = p.err_slot;
 			const std::vector<int> saved_cols = p.col_slots;
+			if (st.pipes[p.id].part.P > 0) {
+				throw Error(6, "batched queries cannot hold a partitioned aggregation (aggr=part): create the query "
+					"with another aggr");
+			}
 			const Flavor pfl = batch_flavor(p.id);
 			PipeGen g(p, q.plan, pfl, st.pipes[p.id], qs, prm);
 			g.item = true;

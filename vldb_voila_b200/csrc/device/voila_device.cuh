@@ -975,6 +975,150 @@ __device__ __forceinline__ bool cache_add(unsigned long long* cache, int S, uint
 	return false;
 }
 
+/* ------------------------------------------------------------------------------------------
+ * Partitioned hash aggregation (flavor aggr=part).
+ *
+ * Pass 1 (the pipeline's main kernel) turns every surviving row into a record -- the packed
+ * group key and each aggregate's value minus its lower bound, bit fields of one or two
+ * 64-bit words -- and stages the records of its CTA in shared memory, each with its
+ * partition (high bits of the key's hash) and its rank within that partition.  A full stage
+ * is flushed as one run ordered by partition: the CTA reserves the run and a flush index
+ * with one atomic each, scatters the records to run start + partition offset + rank, and
+ * writes the flush's row of the segment table, seg[f * P + p] = (run position << 16) |
+ * records of partition p.
+ *
+ * Pass 2 (a persistent kernel) takes work items, each one partition or, for a partition
+ * holding more than R records, a share of its flushes.  An item aggregates its records into
+ * a shared-memory table (keys, then packed accumulator words) and writes the partition's
+ * result rows; the items of a split partition leave their groups in a scratch run, and the
+ * last of them to finish merges the others' runs before writing the rows.
+ * ------------------------------------------------------------------------------------------ */
+
+/* Exclusive prefix sums out[i] = in[0] + ... + in[i-1] over n values held in shared memory
+ * (in and out distinct); returns the total.  All threads of the block call it; `scratch`
+ * holds 33 words of shared memory. */
+__device__ __forceinline__ uint32_t block_excl_scan(const uint32_t* in, uint32_t* out, int n, uint32_t* scratch)
+{
+	const int T = (int)blockDim.x;
+	const int per = (n + T - 1) / T;
+	const int b = (int)threadIdx.x * per;
+	uint32_t s = 0;
+	for (int i = 0; i < per && b + i < n; i++) {
+		s += in[b + i];
+	}
+	const unsigned lane = lane_id(), warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+	uint32_t x = s;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+		if ((int)lane >= o) {
+			x += y;
+		}
+	}
+	if (lane == 31) {
+		scratch[warp] = x;
+	}
+	block_sync();
+	if (threadIdx.x == 0) {
+		uint32_t run = 0;
+		for (unsigned w = 0; w < nw; w++) {
+			const uint32_t c = scratch[w];
+			scratch[w] = run;
+			run += c;
+		}
+		scratch[32] = run;
+	}
+	block_sync();
+	uint32_t pre = scratch[warp] + x - s;
+	for (int i = 0; i < per && b + i < n; i++) {
+		const uint32_t v = in[b + i];
+		out[b + i] = pre;
+		pre += v;
+	}
+	const uint32_t total = scratch[32];
+	block_sync();
+	return total;
+}
+
+/* Rank of each thread's `take` among the block's takers (exclusive), and their number in
+ * *total.  All threads call it; `scratch` holds 33 words of shared memory. */
+__device__ __forceinline__ uint32_t block_rank(bool take, uint32_t* scratch, uint32_t* total)
+{
+	const unsigned lane = lane_id(), warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+	const unsigned m = __ballot_sync(0xffffffffu, take);
+	if (lane == 0) {
+		scratch[warp] = (uint32_t)__popc(m);
+	}
+	block_sync();
+	if (threadIdx.x == 0) {
+		uint32_t run = 0;
+		for (unsigned w = 0; w < nw; w++) {
+			const uint32_t c = scratch[w];
+			scratch[w] = run;
+			run += c;
+		}
+		scratch[32] = run;
+	}
+	block_sync();
+	const uint32_t r = scratch[warp] + (uint32_t)__popc(m & lanemask_lt());
+	*total = scratch[32];
+	block_sync();
+	return r;
+}
+
+/* Slot of stored key `key` (packed key + 1) in a shared-memory table of S (power of two)
+ * slots, inserting it at the first free slot of its linear probe sequence from h; -1 when
+ * every slot holds another key. */
+__device__ __forceinline__ int st_find_or_insert(uint32_t* skeys, int S, uint32_t h, uint32_t key)
+{
+	uint32_t i = h & (uint32_t)(S - 1);
+	for (int probe = 0; probe < S; probe++) {
+		uint32_t cur = *(volatile uint32_t*)&skeys[i];
+		if (cur == 0u) {
+			cur = atomicCAS(&skeys[i], 0u, key);
+			if (cur == 0u) {
+				return (int)i;
+			}
+		}
+		if (cur == key) {
+			return (int)i;
+		}
+		i = (i + 1) & (uint32_t)(S - 1);
+	}
+	return -1;
+}
+
+/* index of the segment holding virtual record j: the largest s < nseg with pre[s] <= j
+ * (pre: exclusive prefix of the segments' record counts, pre[0] = 0) */
+__device__ __forceinline__ int seg_of(const uint32_t* pre, int nseg, uint32_t j)
+{
+	int lo = 0, hi = nseg - 1;
+	while (lo < hi) {
+		const int mid = (lo + hi + 1) >> 1;
+		if (pre[mid] <= j) {
+			lo = mid;
+		} else {
+			hi = mid - 1;
+		}
+	}
+	return lo;
+}
+
+/* the largest p < n with pre[p] <= x (pre non-decreasing, pre[0] = 0 <= x) */
+__device__ __forceinline__ int last_at_most(const uint32_t* pre, int n, uint32_t x)
+{
+	int lo = 0, hi = n - 1;
+	while (lo < hi) {
+		const int mid = (lo + hi + 1) >> 1;
+		if (pre[mid] <= x) {
+			lo = mid;
+		} else {
+			hi = mid - 1;
+		}
+	}
+	return lo;
+}
+
 } // namespace vd
 
 #endif

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cinttypes>
 #include <cstring>
+#include <thread>
 #include <functional>
 #include <sstream>
 
@@ -62,6 +63,15 @@ std::string Flavor::str() const
 	}
 	if (probe_lanes != 1) {
 		o << ",probe=" << probe_lanes;
+	}
+	if (private_groups != 8) {
+		o << ",pgroups=" << private_groups;
+	}
+	if (parts) {
+		o << ",parts=" << parts;
+	}
+	if (stage) {
+		o << ",stage=" << stage;
 	}
 	o << ")";
 	for (auto& ov : overrides) {
@@ -170,8 +180,8 @@ void Flavor::apply(Flavor& f, const std::string& s0)
 				throw Error(1, "rows must be a power of two");
 			}
 		} else if (k == "aggr") {
-			if (v != "auto" && v != "dense" && v != "global" && v != "cache") {
-				throw Error(1, "aggr must be auto, dense, global or cache");
+			if (v != "auto" && v != "dense" && v != "global" && v != "cache" && v != "part") {
+				throw Error(1, "aggr must be auto, dense, global, cache or part");
 			}
 			f.aggr = v;
 		} else if (k == "cache") {
@@ -184,6 +194,18 @@ void Flavor::apply(Flavor& f, const std::string& s0)
 			f.probe_lanes = num(1, 32);
 			if (f.probe_lanes & (f.probe_lanes - 1)) {
 				throw Error(1, "probe lanes must be a power of two");
+			}
+		} else if (k == "pgroups") {
+			f.private_groups = num(1, 16);
+		} else if (k == "parts") {
+			f.parts = num(0, 2048);
+			if (f.parts && (f.parts < 16 || (f.parts & (f.parts - 1)))) {
+				throw Error(1, "parts must be 0 or a power of two from 16 to 2048");
+			}
+		} else if (k == "stage") {
+			f.stage = num(0, 16384);
+			if (f.stage && (f.stage < 2048 || (f.stage & (f.stage - 1)))) {
+				throw Error(1, "stage must be 0 or a power of two from 2048 to 16384");
 			}
 		} else if (k == "ocap") {
 			f.out_rows = num(0, 1 << 30);
@@ -419,6 +441,22 @@ void query_prepare(Query& q)
 			ps.sink_bytes = (size_t)p.sink.domain * A * 8;
 			break;
 		case Sink::AggHash:
+			ps.part = part_plan(p, plan, q.flavor.for_pipe(p.id), e.sms);
+			if (ps.part.P > 0) {
+				/* partitioned aggregation: records, segment table, partial groups of split
+				 * partitions and per-item runs; its per-run counters live in the arena */
+				PartPlan& pp = ps.part;
+				pp.buf = dev_alloc(q, (size_t)pp.cap * 8 * pp.rec_words);
+				pp.seg = dev_alloc(q, (size_t)pp.fmax * pp.P * 8);
+				pp.skeys = dev_alloc(q, (size_t)pp.scratch * 4);
+				pp.sacc = dev_alloc(q, (size_t)pp.scratch * p.sink.nwords * 8);
+				pp.items = dev_alloc(q, (size_t)pp.max_items * 8);
+				pp.ctl = (unsigned long long*)arena_take(32 + (size_t)pp.P * 12);
+				if (!pp.ctl) {
+					throw Error(VC_ERR_UNSUPPORTED, "aggr=part: too many partitions for the per-run state");
+				}
+				break;
+			}
 			/* a user-set capacity (gcap) is taken as given: too small a table fails the run
 			 * with VC_ERR_CAPACITY (bounded probe sequences), it never returns wrong rows */
 			{
@@ -452,7 +490,7 @@ void query_prepare(Query& q)
 				}
 			}
 		}
-		if (p.sink.kind == Sink::AggHash) {
+		if (p.sink.kind == Sink::AggHash && ps.part.P == 0) {
 			const size_t kb = (((size_t)ps.sink_cap * (p.sink.key_bits <= 31 ? 4 : 8)) + 255) & ~(size_t)255;
 			ps.sink_acc = (char*)ps.sink_dev + kb;
 		}
@@ -785,8 +823,26 @@ void query_result_int64(Query& q, int64_t* out, int64_t cap)
 	for (int c = 0; c < C; c++) {
 		const auto& parts = q.plan.out_cols[(size_t)c].parts;
 		if (parts.size() == 1 && parts[0].second == 0) {
-			/* a plain int64 column: copied as is */
-			std::memcpy(out + (size_t)c * R, q.result_host + (size_t)parts[0].first * R, (size_t)R * 8);
+			/* a plain int64 column: copied as is (large columns by several threads) */
+			char* dst = (char*)(out + (size_t)c * R);
+			const char* src = (const char*)(q.result_host + (size_t)parts[0].first * R);
+			const size_t bytes = (size_t)R * 8;
+			const size_t nt = std::min<size_t>(8, std::max<size_t>(1, bytes >> 22));
+			if (nt == 1) {
+				std::memcpy(dst, src, bytes);
+				continue;
+			}
+			std::vector<std::thread> th;
+			const size_t chunk = (bytes / nt + 63) & ~(size_t)63;
+			for (size_t t = 0; t < nt; t++) {
+				const size_t b = t * chunk;
+				if (b < bytes) {
+					th.emplace_back([=] { std::memcpy(dst + b, src + b, std::min(chunk, bytes - b)); });
+				}
+			}
+			for (auto& x : th) {
+				x.join();
+			}
 			continue;
 		}
 		for (int64_t r = 0; r < R; r++) {

@@ -231,7 +231,7 @@ struct Pipeline {
 struct Flavor {
 	int threads = 256;        /* threads per CTA */
 	int rows = 4;             /* consecutive rows per thread and tile step */
-	std::string aggr = "auto";/* auto | dense | global | cache */
+	std::string aggr = "auto";/* auto | dense | global | cache | part */
 	int cache_slots = 1024;   /* shared-memory group cache (aggr=cache) */
 	int bucket = 32;          /* join bucket bytes: 32 (sector) or the slot size */
 	int grid = 0;             /* CTAs per SM (0 = occupancy) */
@@ -251,6 +251,9 @@ struct Flavor {
 	int sink_smem = 96 * 1024; /* most shared memory a dense aggregation keeps its slots in (else global) */
 	int64_t group_slots = 0;  /* hash group table slots (0 = sized from the groups bound and fill) */
 	int probe_lanes = 1;      /* lanes that probe one join key together (1 = each lane its own key) */
+	int private_groups = 8;   /* lowcard=private: groups per CTA with per-thread accumulators */
+	int parts = 0;            /* aggr=part: partitions (0 = from the groups bound) */
+	int stage = 0;            /* aggr=part: records a CTA stages before a flush (0 = 8192) */
 	int64_t out_rows = 0;     /* result row capacity of an emitting pipeline (0 = from its bound, at
 	                           * most 4 rows per input row + 2^20 when joinN probes multiply rows) */
 
@@ -317,6 +320,35 @@ struct GeneratedCode {
 };
 
 /* device state of one pipeline's sink, allocated before code generation */
+/* Partitioned hash aggregation of one pipeline (flavor aggr=part; voila_device.cuh describes
+ * the two passes).  P == 0: the pipeline aggregates into a global group table instead. */
+struct PartPlan {
+	int P = 0;                 /* partitions (power of two) */
+	int log2P = 0;
+	int S = 0;                 /* slots of a partition's shared-memory table (power of two) */
+	int C = 0;                 /* records staged per CTA */
+	int rec_words = 1;         /* 64-bit words per record */
+	std::vector<int> rec_word, rec_off; /* per aggregate: its record field (count: -1) */
+	int agg_threads = 512;     /* threads of the aggregation kernel */
+	int64_t cap = 0;           /* record capacity */
+	int64_t fmax = 0;          /* flush capacity (rows of the segment table) */
+	int64_t R = 0;             /* records above which a partition is split over several items */
+	int64_t max_items = 0;
+	int64_t scratch = 0;       /* capacity of the split partitions' partial groups */
+	size_t smem1 = 0, smem2 = 0; /* dynamic shared memory of the two passes */
+	void* buf = nullptr;       /* records */
+	void* seg = nullptr;       /* fmax x P segment words */
+	void* skeys = nullptr;     /* partial groups: stored keys */
+	void* sacc = nullptr;      /* partial groups: accumulator words */
+	void* items = nullptr;     /* per split item: (scratch position << 16) | groups */
+	unsigned long long* ctl = nullptr; /* per run: record cursor, flush count, item counter,
+	                                    * partial cursor, P record totals, P done counters (u32) */
+};
+
+/* the partitioned aggregation of pipeline p under flavor f, or P == 0 when it does not apply
+ * (not a hash group-by, keys wider than 31 bits, records wider than 128 bits, ...) */
+PartPlan part_plan(const Pipeline& p, const LoweredPlan& plan, const Flavor& f, int sms);
+
 struct PipeDeviceState {
 	void* sink_dev = nullptr;            /* aggregation state (global sums, dense slots, group table) */
 	int64_t sink_cap = 0;
@@ -325,6 +357,7 @@ struct PipeDeviceState {
 	bool self_cleaning = false;          /* the pipeline's last kernel leaves sink_dev zeroed */
 	void* stage_hash = nullptr;          /* staged join build: materialised hashes */
 	unsigned long long* done = nullptr;  /* last-block counter */
+	PartPlan part;                       /* partitioned aggregation (aggr=part) */
 };
 
 /* query-wide device state the generated kernels write to */

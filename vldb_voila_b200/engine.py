@@ -427,11 +427,11 @@ class Query:
         return r.value, c.value
 
     def result(self):
-        """int64 array of shape (rows, cols)."""
+        """int64 array of shape (rows, cols), column-major (the C ABI's layout; no transpose)."""
         r, c = self.shape()
         out = np.empty(max(r * c, 1), dtype=np.int64)
         check(lib().vc_query_result_copy(self._h, out.ctypes.data, out.size))
-        return out[: r * c].reshape(c, r).T.copy()
+        return out[: r * c].reshape(c, r).T
 
     def result_text(self):
         return _text_call(lib().vc_query_result_text, self._h)

@@ -253,6 +253,8 @@ struct PipeGen {
 	}
 
 	int A() const { return (int)p.sink.aggs.size(); }
+	/* survivors each thread takes per pass of a compaction flush (gathers in flight) */
+	int FV() const { return fl.flush_rows; }
 	/* partitioned aggregation (aggr=part) of a standalone pipeline */
 	bool part() const { return st.part.P > 0 && !item; }
 	std::string rec_type() const { return st.part.rec_words == 2 ? "ulonglong2" : "unsigned long long"; }
@@ -700,8 +702,8 @@ struct PipeGen {
 		}
 		for (size_t c = 0; c < p.cols.size(); c++) {
 			if (lazy_first_use[c] == at) {
-				o << "      if (act[0]) { x" << c << "[0] = vd::load_one<" << ctype(p.cols[c].type) << (p.cols[c].host ? ", true" : "")
-				  << ">(c" << c << ", row); }\n";
+				o << "#pragma unroll\n      for (int v = 0; v < " << V << "; v++) { if (act[v]) { x" << c << "[v] = vd::load_one<"
+				  << ctype(p.cols[c].type) << (p.cols[c].host ? ", true" : "") << ">(c" << c << ", row[v]); } }\n";
 			}
 		}
 	}
@@ -830,7 +832,7 @@ struct PipeGen {
 		}
 		o << "    cpend += nsel;\n";
 		o << "    vd::block_sync();\n";
-		o << "    if (cpend >= " << T << ") { cflush(); }\n";
+		o << "    if (cpend >= " << T * FV() << ") { cflush(); }\n";
 		o << "    }\n";
 	}
 
@@ -841,7 +843,7 @@ struct PipeGen {
 		if (compact_at < 0) {
 			return;
 		}
-		const int cap = T + T * V;
+		const int cap = T * FV() + T * V;
 		/* row indices as 32 bits when every row of the table fits */
 		o << "  __shared__ " << (p.rows <= (int64_t)UINT32_MAX ? "uint32_t" : "int64_t") << " csel[" << cap << "];\n";
 		o << "  __shared__ int cscan[33];\n";
@@ -850,14 +852,17 @@ struct PipeGen {
 		for (size_t k = 0; k < carried.size(); k++) {
 			o << "  __shared__ int64_t ccar" << k << "[" << cap << "];\n";
 		}
+		const int F = FV();
 		o << "  auto cflush = [&]() {\n";
-		o << "    for (int base = 0; base < cpend; base += " << T << ") {\n";
-		o << "      const int ci = base + (int)threadIdx.x;\n";
-		o << "      const bool live = ci < cpend;\n";
-		o << "      const int64_t row = live ? (int64_t)csel[ci] : 0;\n";
+		o << "    for (int base = 0; base < cpend; base += " << T * F << ") {\n";
+		o << "      bool act[" << F << "];\n      int64_t row[" << F << "];\n";
+		o << "#pragma unroll\n      for (int v = 0; v < " << F << "; v++) {\n";
+		o << "        const int ci = base + v * " << T << " + (int)threadIdx.x;\n";
+		o << "        act[v] = ci < cpend;\n";
+		o << "        row[v] = act[v] ? (int64_t)csel[ci] : 0;\n";
+		o << "      }\n";
 		const int saveV = V;
-		V = 1;
-		o << "      bool act[1] = {live};\n";
+		V = F;
 		/* every column is gathered just before the first op (or the sink) that reads it, and
 		 * only for rows still alive there: a row that fails a probe never touches the columns
 		 * of the later ones */
@@ -883,12 +888,14 @@ struct PipeGen {
 		}
 		for (size_t c = 0; c < p.cols.size(); c++) {
 			if (lazy_first_use[c] != INT32_MAX) {
-				o << "      " << ctype(p.cols[c].type) << " x" << c << "[1] = {0};\n";
+				o << "      " << ctype(p.cols[c].type) << " x" << c << "[" << F << "] = {0};\n";
 			}
 		}
 		for (size_t k = 0; k < carried.size(); k++) {
-			o << "      int64_t pay" << carried[k].first << "_" << carried[k].second << "[1] = {live ? ccar" << k
-			  << "[ci] : 0};\n";
+			const std::string pv = "pay" + std::to_string(carried[k].first) + "_" + std::to_string(carried[k].second);
+			o << "      int64_t " << pv << "[" << F << "];\n";
+			o << "#pragma unroll\n      for (int v = 0; v < " << F << "; v++) { " << pv << "[v] = act[v] ? ccar" << k << "[base + v * "
+			  << T << " + (int)threadIdx.x] : 0; }\n";
 		}
 		lazy_rows = true;
 		emit_rest(compact_at + 1);
@@ -1422,8 +1429,13 @@ struct PipeGen {
 		o << "        shist[q] = 0u;\n";
 		o << "      }\n";
 		o << "    } else {\n";
+		/* records beyond the capacity are dropped (the run fails with the error bit); the
+		 * flush's segment row, if it has one, still says so: no records */
 		o << "      if (threadIdx.x == 0) { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
-		o << "      for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) { shist[q] = 0u; }\n";
+		o << "      for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) {\n";
+		o << "        if (pf < pfmax) { pseg[pf * " << NP << "ull + q] = 0ull; }\n";
+		o << "        shist[q] = 0u;\n";
+		o << "      }\n";
 		o << "    }\n";
 		o << "    if (threadIdx.x == 0) { pcount = 0u; }\n";
 		o << "    vd::block_sync();\n";
@@ -1476,7 +1488,8 @@ struct PipeGen {
 		const PartPlan& pp = st.part;
 		const Sink& s = p.sink;
 		const int NP = pp.P, S = pp.S, W = s.nwords, AT = pp.agg_threads;
-		const int U = 4; /* record loads in flight per thread */
+		const int U = 4; /* record loads in flight per thread; a window's marks fill the count array */
+		static_assert(kPartSegs * 4 >= 512 * 4 * 2, "window marks must fit the segment count array");
 		const std::string RT = rec_type();
 		std::ostringstream k;
 		k << "extern \"C\" __global__ void __launch_bounds__(" << AT << ") " << name << "_extract(const VcParams p) {\n";
@@ -1542,13 +1555,32 @@ struct PipeGen {
 		k << "      }\n";
 		k << "      vd::block_sync();\n";
 		k << "      const uint32_t tot = vd::block_excl_scan(scnt, spre, nseg, xscan);\n";
-		k << "      for (uint32_t base = 0; base < tot; base += blockDim.x * " << U << "u) {\n";
+		/* windows of blockDim.x * U records: each non-empty segment marks its first position
+		 * in the window (the one straddling the window start marks position 0), a running
+		 * maximum gives every position its segment; record j of the window goes to thread
+		 * j % blockDim.x, so a warp reads consecutive records */
+		k << "      uint16_t* const smark = (uint16_t*)scnt;\n";
+		k << "      const uint32_t wn = blockDim.x * " << U << "u;\n";
+		k << "      for (uint32_t base = 0; base < tot; base += wn) {\n";
+		k << "        for (uint32_t i = threadIdx.x; i < wn; i += blockDim.x) { smark[i] = 0; }\n";
+		k << "        vd::block_sync();\n";
+		/* the window's segments: from the one holding its first record to the one holding its
+		 * last (empty segments share the next one's prefix; the search takes the last) */
+		k << "        const int slo = vd::seg_of(spre, nseg, base);\n";
+		k << "        const int shi = vd::seg_of(spre, nseg, min(base + wn, tot) - 1u);\n";
+		k << "        for (int sg = slo + (int)threadIdx.x; sg <= shi; sg += blockDim.x) {\n";
+		k << "          const uint32_t b = spre[sg];\n";
+		k << "          if ((sseg[sg] & 0xffffull) != 0ull) { smark[b > base ? b - base : 0u] = (uint16_t)(sg + 1); }\n";
+		k << "        }\n";
+		k << "        vd::block_sync();\n";
+		k << "        vd::block_incl_max_scan_u16(smark, (int)wn, xscan);\n";
 		k << "        " << RT << " r[" << U << "];\n        bool live[" << U << "];\n";
 		k << "#pragma unroll\n        for (int u = 0; u < " << U << "; u++) {\n";
-		k << "          const uint32_t jj = base + (uint32_t)u * blockDim.x + threadIdx.x;\n";
+		k << "          const uint32_t i = (uint32_t)u * blockDim.x + threadIdx.x;\n";
+		k << "          const uint32_t jj = base + i;\n";
 		k << "          live[u] = jj < tot;\n";
 		k << "          if (live[u]) {\n";
-		k << "            const int sg = vd::seg_of(spre, nseg, jj);\n";
+		k << "            const int sg = (int)smark[i] - 1;\n";
 		k << "            r[u] = __ldcs(&pbuf[(sseg[sg] >> 16) + (jj - spre[sg])]);\n";
 		k << "          }\n";
 		k << "        }\n";
@@ -1584,18 +1616,15 @@ struct PipeGen {
 		k << "            } else { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
 		k << "          }\n";
 		k << "        }\n";
+		k << "        vd::block_sync();\n";
 		k << "      }\n";
-		k << "      vd::block_sync();\n";
 		k << "    }\n";
 		/* a split partition's item: leave the groups in a scratch run; the last item merges */
 		k << "    bool emit = kq == 1u;\n";
 		k << "    if (kq > 1u) {\n";
-		k << "      uint32_t ng = 0u;\n";
-		k << "      for (int s0 = 0; s0 < " << S << "; s0 += blockDim.x) {\n";
-		k << "        uint32_t n1;\n";
-		k << "        vd::block_rank(skeys[s0 + threadIdx.x] != 0u, xscan, &n1);\n";
-		k << "        ng += n1;\n";
-		k << "      }\n";
+		k << "      uint32_t mine = 0u, ng;\n";
+		k << "      for (int sl = threadIdx.x; sl < " << S << "; sl += blockDim.x) { mine += skeys[sl] != 0u ? 1u : 0u; }\n";
+		k << "      const uint32_t pre = vd::block_excl_sum(mine, xscan, &ng);\n";
 		k << "      if (threadIdx.x == 0) {\n";
 		k << "        const unsigned long long x0 = atomicAdd(&pctl[3], (unsigned long long)ng);\n";
 		k << "        if (x0 + ng > xcap) { atomicOr(err, VD_ERR_TABLE_FULL); ng = 0u; }\n";
@@ -1605,18 +1634,16 @@ struct PipeGen {
 		k << "      vd::block_sync();\n";
 		k << "      const unsigned long long x0 = xrun >> 16;\n";
 		k << "      const uint32_t nrun = (uint32_t)(xrun & 0xffffull);\n";
-		k << "      uint32_t wpos = 0u;\n";
-		k << "      for (int s0 = 0; s0 < " << S << "; s0 += blockDim.x) {\n";
-		k << "        const int sl = s0 + (int)threadIdx.x;\n";
+		k << "      uint32_t wpos = pre;\n";
+		k << "      for (int sl = threadIdx.x; sl < " << S << "; sl += blockDim.x) {\n";
 		k << "        const uint32_t key = skeys[sl];\n";
-		k << "        uint32_t n1;\n";
-		k << "        const uint32_t rk = vd::block_rank(key != 0u, xscan, &n1);\n";
-		k << "        if (key != 0u && wpos + rk < nrun) {\n";
-		k << "          xkeys[x0 + wpos + rk] = key;\n";
-		k << "#pragma unroll\n          for (int a = 0; a < " << W << "; a++) { xacc[(x0 + wpos + rk) * " << W << "ull + a] = sacc[sl * "
+		k << "        if (key == 0u) { continue; }\n";
+		k << "        if (wpos < nrun) {\n";
+		k << "          xkeys[x0 + wpos] = key;\n";
+		k << "#pragma unroll\n          for (int a = 0; a < " << W << "; a++) { xacc[(x0 + wpos) * " << W << "ull + a] = sacc[sl * "
 		  << W << " + a]; }\n";
 		k << "        }\n";
-		k << "        wpos += n1;\n";
+		k << "        wpos++;\n";
 		k << "      }\n";
 		k << "      __threadfence();\n";
 		k << "      vd::block_sync();\n";
@@ -1659,23 +1686,15 @@ struct PipeGen {
 		};
 		/* one reservation of result rows per item: count the groups, then write them */
 		k << "    if (emit) {\n";
-		k << "      uint32_t ng = 0u;\n";
-		k << "      for (int s0 = 0; s0 < " << S << "; s0 += blockDim.x) {\n";
-		k << "        uint32_t n1;\n";
-		k << "        vd::block_rank(skeys[s0 + threadIdx.x] != 0u, xscan, &n1);\n";
-		k << "        ng += n1;\n";
-		k << "      }\n";
+		k << "      uint32_t mine = 0u, ng;\n";
+		k << "      for (int sl = threadIdx.x; sl < " << S << "; sl += blockDim.x) { mine += skeys[sl] != 0u ? 1u : 0u; }\n";
+		k << "      const uint32_t pre = vd::block_excl_sum(mine, xscan, &ng);\n";
 		k << "      if (threadIdx.x == 0) { xres[0] = ng ? atomicAdd(ocount, (unsigned long long)ng) : 0ull; }\n";
 		k << "      vd::block_sync();\n";
-		k << "      const int64_t obase = (int64_t)xres[0];\n";
-		k << "      uint32_t wpos = 0u;\n";
-		k << "      for (int s0 = 0; s0 < " << S << "; s0 += blockDim.x) {\n";
-		k << "        const int sl = s0 + (int)threadIdx.x;\n";
+		k << "      int64_t pos = (int64_t)xres[0] + (int64_t)pre;\n";
+		k << "      for (int sl = threadIdx.x; sl < " << S << "; sl += blockDim.x) {\n";
 		k << "        const uint32_t key = skeys[sl];\n";
-		k << "        uint32_t n1;\n";
-		k << "        const uint32_t rk = vd::block_rank(key != 0u, xscan, &n1);\n";
-		k << "        const int64_t pos = obase + (int64_t)(wpos + rk);\n";
-		k << "        wpos += n1;\n";
+		k << "        if (key == 0u) { continue; }\n";
 		k << "        uint64_t w[" << W << "];\n";
 		k << "#pragma unroll\n        for (int a = 0; a < " << W << "; a++) { w[a] = key != 0u ? sacc[sl * " << W << " + a] : 0ull; }\n";
 		k << "        const bool take = key != 0u && (int64_t)" << field(s.count_idx) << " > 0;\n";
@@ -1703,9 +1722,9 @@ struct PipeGen {
 			col++;
 		}
 		k << "        }\n";
-		k << "        if (key != 0u) {\n          skeys[sl] = 0u;\n";
-		k << "#pragma unroll\n          for (int a = 0; a < " << W << "; a++) { sacc[sl * " << W << " + a] = 0ull; }\n";
-		k << "        }\n";
+		k << "        pos++;\n";
+		k << "        skeys[sl] = 0u;\n";
+		k << "#pragma unroll\n        for (int a = 0; a < " << W << "; a++) { sacc[sl * " << W << " + a] = 0ull; }\n";
 		k << "      }\n";
 		k << "      vd::block_sync();\n";
 		k << "    }\n";

@@ -1066,6 +1066,81 @@ __device__ __forceinline__ uint32_t block_rank(bool take, uint32_t* scratch, uin
 	return r;
 }
 
+/* Exclusive prefix of x over the block's threads, and the block's sum in *total.  All threads
+ * call it; `scratch` holds 33 words of shared memory. */
+__device__ __forceinline__ uint32_t block_excl_sum(uint32_t x, uint32_t* scratch, uint32_t* total)
+{
+	const unsigned lane = lane_id(), warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+	uint32_t v = x;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+		if ((int)lane >= o) {
+			v += y;
+		}
+	}
+	if (lane == 31) {
+		scratch[warp] = v;
+	}
+	block_sync();
+	if (threadIdx.x == 0) {
+		uint32_t run = 0;
+		for (unsigned w = 0; w < nw; w++) {
+			const uint32_t c = scratch[w];
+			scratch[w] = run;
+			run += c;
+		}
+		scratch[32] = run;
+	}
+	block_sync();
+	const uint32_t r = scratch[warp] + v - x;
+	*total = scratch[32];
+	block_sync();
+	return r;
+}
+
+/* In-place inclusive running maximum over n 16-bit values in shared memory (n a multiple of
+ * the block size; each thread takes n / blockDim.x consecutive ones).  All threads call it;
+ * `scratch` holds 33 words of shared memory. */
+__device__ __forceinline__ void block_incl_max_scan_u16(uint16_t* a, int n, uint32_t* scratch)
+{
+	const int per = n / (int)blockDim.x;
+	const int b = (int)threadIdx.x * per;
+	const unsigned lane = lane_id(), warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+	uint32_t m = 0;
+	for (int i = 0; i < per; i++) {
+		m = max(m, (uint32_t)a[b + i]);
+	}
+	uint32_t x = m;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+		if ((int)lane >= o) {
+			x = max(x, y);
+		}
+	}
+	const uint32_t before = __shfl_up_sync(0xffffffffu, x, 1);
+	if (lane == 31) {
+		scratch[warp] = x;
+	}
+	block_sync();
+	if (threadIdx.x == 0) {
+		uint32_t run = 0;
+		for (unsigned w = 0; w < nw; w++) {
+			const uint32_t c = scratch[w];
+			scratch[w] = run;
+			run = max(run, c);
+		}
+	}
+	block_sync();
+	uint32_t run = max(scratch[warp], lane ? before : 0u);
+	for (int i = 0; i < per; i++) {
+		run = max(run, (uint32_t)a[b + i]);
+		a[b + i] = (uint16_t)run;
+	}
+	block_sync();
+}
+
 /* Slot of stored key `key` (packed key + 1) in a shared-memory table of S (power of two)
  * slots, inserting it at the first free slot of its linear probe sequence from h; -1 when
  * every slot holds another key. */

@@ -64,6 +64,9 @@ std::string Flavor::str() const
 	if (probe_lanes != 1) {
 		o << ",probe=" << probe_lanes;
 	}
+	if (flush_rows != 1) {
+		o << ",frows=" << flush_rows;
+	}
 	if (private_groups != 8) {
 		o << ",pgroups=" << private_groups;
 	}
@@ -194,6 +197,11 @@ void Flavor::apply(Flavor& f, const std::string& s0)
 			f.probe_lanes = num(1, 32);
 			if (f.probe_lanes & (f.probe_lanes - 1)) {
 				throw Error(1, "probe lanes must be a power of two");
+			}
+		} else if (k == "frows") {
+			f.flush_rows = num(1, 8);
+			if (f.flush_rows & (f.flush_rows - 1)) {
+				throw Error(1, "frows must be 1, 2, 4 or 8");
 			}
 		} else if (k == "pgroups") {
 			f.private_groups = num(1, 16);

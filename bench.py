@@ -574,9 +574,8 @@ def run_config5(args):
 
     # (b) one persistent kernel over all pipelines, learned flavors
     # batched pipelines build their join tables in place (dense or direct hash; one work
-    # phase per table): a staged build becomes the automatic choice, and a partitioned
-    # group-by (two passes with a data-dependent item count) the global group table
-    batch_flavors = [f.replace("build=staged", "build=auto").replace("aggr=part", "aggr=global") for f in learned]
+    # phase per table): a staged build becomes the automatic choice
+    batch_flavors = [f.replace("build=staged", "build=auto") for f in learned]
     queries_learned = [e.query(workload(s).plan, f) for e, s, f in zip(engines, specs, batch_flavors)]
     batch = Batch(queries_learned, threads=256, tiles_per_item=16)
     for _ in range(2):

@@ -308,10 +308,12 @@ def test_bad_partition_knobs_are_rejected(flavor):
     assert ex.value.code == 1
 
 
-def test_partitioned_aggregation_is_not_batched():
+def test_batched_partitioned_aggregation_uses_a_group_table():
+    """A batch runs a query prepared with aggr=part through the global group table."""
     from vldb_voila_b200.engine import Batch
     w, e = offline("groupby:rows=100000,keys=100000")
     q = e.query(w.plan, "cuda(aggr=part)")
-    with pytest.raises(VoilaError) as ex:
-        Batch([q])
-    assert ex.value.code == 6 and "aggr=part" in str(ex.value)
+    assert "pflush" in q.source()
+    b = Batch([q])
+    src = b.source()
+    assert "gt_find_or_insert" in src and "pflush" not in src

@@ -54,3 +54,23 @@ def test_partitioned_sub_aggregation():
     q = e.query(m["plan"], "cuda(aggr=part)")
     q.run()
     assert q.result_lines() == expect
+
+
+def test_batched_partitioned_query_matches_standalone():
+    """A batch takes a query prepared with aggr=part through the global group table; the
+    query still runs standalone with its partitioned kernels afterwards."""
+    from vldb_voila_b200.engine import Batch
+    spec = "groupby:rows=300000,keys=20000,zipf=1.0,seed=14"
+    w = workload(spec)
+    data = generate_workload_host(w)
+    expect = result_lines(run_plan(w.plan, data))
+    e = Engine(0)
+    e.load_workload(w, data=data)
+    q = e.query(w.plan, "cuda(aggr=part)")
+    b = Batch([q])
+    for _ in range(2):
+        b.run()
+        b.wait()
+        assert q.result_lines() == expect
+    q.run()
+    assert q.result_lines() == expect

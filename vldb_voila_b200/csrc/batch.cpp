@@ -120,6 +120,15 @@ static void add_clears_in_order(Batch& b, BatchCode& bc)
 
 static void batch_prepare(Batch& b, const std::vector<Flavor>& flavors, int64_t tiles_per_item)
 {
+	/* a query prepared with a partitioned group-by runs it through a global group table here */
+	for (Query* q : b.queries) {
+		QueryState& st = state_of(*q);
+		for (auto& p : q->plan.pipes) {
+			if (p.sink.kind == Sink::AggHash && !st.pipes[p.id].sink_dev) {
+				alloc_group_table(*q, p, st.pipes[p.id]);
+			}
+		}
+	}
 	if (b.eng->offline) {
 		/* compile-only engines: generate and compile the batch module and build its work
 		 * queue (on the host only, for inspection) */

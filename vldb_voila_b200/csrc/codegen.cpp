@@ -2082,6 +2082,10 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 				f.lowcard = "combine";
 			}
 			f.cache_slots = std::min(f.cache_slots, 256);
+			if (f.aggr == "part") {
+				/* two passes with a data-dependent item count: the global group table instead */
+				f.aggr = "global";
+			}
 			f.sink_smem = std::min(f.sink_smem, 16 * 1024);
 			return f;
 		};
@@ -2139,9 +2143,8 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 			/* the query keeps its own parameter layout for standalone runs */
 			const int saved_err = p.err_slot;
 			const std::vector<int> saved_cols = p.col_slots;
-			if (st.pipes[p.id].part.P > 0) {
-				throw Error(6, "batched queries cannot hold a partitioned aggregation (aggr=part): create the query "
-					"with another aggr");
+			if (p.sink.kind == Sink::AggHash && !st.pipes[p.id].sink_dev) {
+				throw Error(6, "batch: a partitioned group-by has no group table");
 			}
 			const Flavor pfl = batch_flavor(p.id);
 			PipeGen g(p, q.plan, pfl, st.pipes[p.id], qs, prm);

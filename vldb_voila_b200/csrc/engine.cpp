@@ -312,6 +312,27 @@ Query::~Query()
 }
 
 static std::map<Query*, QueryState> g_state;
+QueryState& state_of(Query& q);
+
+/* A batch runs a partitioned group-by (aggr=part) through the global split group table
+ * instead: allocated here on first use (keys in 32-byte buckets, then the packed accumulator
+ * words) and cleared once; the batch clears it before every run. */
+void alloc_group_table(Query& q, const Pipeline& p, PipeDeviceState& ps)
+{
+	const Flavor pf = q.flavor.for_pipe(p.id);
+	const int fill = pf.fill;
+	ps.sink_cap = pf.group_slots > 0 ? pow2_at_least(pf.group_slots)
+		: std::max<int64_t>(pow2_at_least((std::max<int64_t>(p.sink.groups_bound, 1) * 100 + fill - 1) / fill), 1024);
+	const size_t kb = (((size_t)ps.sink_cap * (p.sink.key_bits <= 31 ? 4 : 8)) + 255) & ~(size_t)255;
+	ps.sink_bytes = kb + (size_t)ps.sink_cap * p.sink.nwords * 8;
+	ps.sink_dev = dev_alloc(q, ps.sink_bytes);
+	ps.sink_acc = (char*)ps.sink_dev + kb;
+	if (!q.eng->offline) {
+		ps.self_cleaning = true;
+		VC_CHECK_CUDA(cudaMemset(ps.sink_dev, 0, ps.sink_bytes));
+		state_of(q).clean_memsets.push_back({ps.sink_dev, ps.sink_bytes});
+	}
+}
 static std::mutex g_state_mu;
 
 QueryState& state_of(Query& q)

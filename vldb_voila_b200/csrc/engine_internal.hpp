@@ -436,6 +436,7 @@ struct QueryState {
 
 QueryState& state_of(Query& q);
 void* column_dev(Query& q, const PipeColumn& pc);
+void alloc_group_table(Query& q, const Pipeline& p, PipeDeviceState& ps);
 
 /* ------------------------------------------------------------------ batches ------------ */
 

@@ -280,22 +280,28 @@ def test_per_pipeline_flavor_overrides():
 
 
 def test_partitioned_aggregation_plan():
-    """aggr=part: pass 1 stages records and flushes partition-ordered runs, pass 2 is a
-    persistent kernel over partitions that writes the result rows itself (no group table, no
-    extraction scan)."""
+    """aggr=part: a histogram pass counts each partition's rows, the pipeline's kernel stages
+    records and scatters them so each partition's records are contiguous, and a persistent
+    kernel aggregates each partition in shared memory and writes its result rows itself (no
+    group table, no extraction scan)."""
     w, e = offline("groupby:rows=6000000,keys=1500000,zipf=0,seed=3")
     q = e.query(w.plan, "cuda(aggr=part)")
     src = q.source()
     info = q.info()
-    assert "pflush()" in src and "vd::block_excl_scan(shist, soff, 1024" in src  # 2 x 1.5M / 4096 slots
+    # 2 x 1.5M groups / 4096 slots per partition table -> 1024 partitions
+    assert "pflush()" in src and "vd::block_excl_scan(stot, shist, 1024" in src
     assert "vd::st_find_or_insert(skeys, 4096" in src and "gt_find_or_insert" not in src
     k = {x["name"]: x for x in info["kernels"]}
-    assert k["vc_p0_extract"]["threads"] == 512
+    assert [x["name"] for x in info["kernels"]] == ["vc_p0_hist", "vc_p0_main", "vc_p0_extract"]
+    assert k["vc_p0_extract"]["threads"] == 512 and k["vc_p0_hist"]["smem"] == 1024 * 8
     # records of key + two value fields fit one word; 8192 staged records + 1024 x 2 counters
     assert k["vc_p0_main"]["smem"] == 8192 * 8 + 8192 * 4 + 1024 * 8
+    # the histogram pass reads the key column only
+    hist = src[src.index("vc_p0_hist"):src.index("vc_p0_main")]
+    assert "load_rows<int32_t, 4>(c0" in hist and "(c1" not in hist and "(c2" not in hist
     # an explicit partition count and stage size
     src2 = e.query(w.plan, "cuda(aggr=part,parts=2048,stage=4096,threads=512)").source()
-    assert "vd::block_excl_scan(shist, soff, 2048" in src2 and "+ 2048u > 4096u" in src2
+    assert "vd::block_excl_scan(stot, shist, 2048" in src2 and "+ 2048u > 4096u" in src2
     # too few partitions for the groups bound: falls back to the global table
     assert "gt_find_or_insert" in e.query(w.plan, "cuda(aggr=part,parts=16)").source()
 

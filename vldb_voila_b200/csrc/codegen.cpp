@@ -71,11 +71,9 @@ static int span_bits(const Bounds& b)
 	return std::max(bits, 1);
 }
 
-/* segments an aggregation item loads into shared memory at a time */
-static constexpr int kPartSegs = 1024;
-
 PartPlan part_plan(const Pipeline& p, const LoweredPlan& plan, const Flavor& f, int sms)
 {
+	(void)sms;
 	PartPlan pp;
 	const Sink& s = p.sink;
 	if (f.aggr != "part" || s.kind != Sink::AggHash || s.key_bits > 31 || s.count_idx < 0) {
@@ -145,16 +143,15 @@ PartPlan part_plan(const Pipeline& p, const LoweredPlan& plan, const Flavor& f, 
 	}
 	const int64_t rows = std::max<int64_t>(p.rows, 1);
 	pp.cap = joinn ? 4 * rows + (1 << 20) : rows;
-	/* every flush but a CTA's last holds more than C - TV records */
-	const int64_t grid_max = (int64_t)sms * std::max(1, 2048 / f.threads);
-	pp.fmax = (pp.cap + (C - TV) - 1) / (C - TV) + grid_max + 1;
+	if (pp.cap >= (int64_t)UINT32_MAX) {
+		return PartPlan(); /* record positions are 32-bit */
+	}
 	pp.R = std::max<int64_t>(4 * (int64_t)S, (pp.cap + 2047) / 2048);
 	pp.max_items = P + pp.cap / pp.R + 1;
 	/* a split item leaves at most min(S, its records) groups; split items hold at least R / 2
 	 * records each */
 	pp.scratch = std::min<int64_t>(pp.cap, (2 * pp.cap / pp.R + 1) * S) + S;
-	pp.smem2 = (size_t)S * 4 + (size_t)S * W * 8 + (size_t)kPartSegs * 8 + (size_t)kPartSegs * 4 +
-		(size_t)(kPartSegs + 1) * 4 + (size_t)P * 12;
+	pp.smem2 = (size_t)S * 4 + (size_t)S * W * 8 + (size_t)P * 12 + (size_t)P * 8;
 	pp.smem2 = (pp.smem2 + 15) & ~(size_t)15;
 	return pp;
 }
@@ -253,6 +250,7 @@ struct PipeGen {
 	}
 
 	int A() const { return (int)p.sink.aggs.size(); }
+	bool part_hist = false;    /* generating the histogram pass of a partitioned group-by */
 	/* survivors each thread takes per pass of a compaction flush (gathers in flight) */
 	int FV() const { return fl.flush_rows; }
 	/* partitioned aggregation (aggr=part) of a standalone pipeline */
@@ -401,7 +399,7 @@ struct PipeGen {
 	}
 
 	std::string gen_main() {
-		fn_header("_main");
+		fn_header(part_hist ? "_hist" : "_main");
 		if (p.source_inter >= 0) {
 			/* the rows come from an earlier pipeline of the query: wait for it before reading
 			 * the row count (or any column) */
@@ -412,15 +410,24 @@ struct PipeGen {
 		} else {
 			o << "  const int64_t n = " << P((unsigned long long)p.rows) << ";\n";
 		}
-		p.err_slot = (int)params.size();
-		o << "  unsigned* const err = (unsigned*)p.v[" << params.size() << "];\n";
-		params.push_back(0); /* error word, filled by the runtime */
-		p.col_slots.clear();
-		for (size_t c = 0; c < p.cols.size(); c++) {
-			p.col_slots.push_back((int)params.size());
-			o << "  const " << ctype(p.cols[c].type) << "* __restrict__ c" << c << " = (const "
-			  << ctype(p.cols[c].type) << "*)p.v[" << params.size() << "];\n";
-			params.push_back(0); /* column pointer, filled by the runtime */
+		if (part_hist) {
+			/* the histogram pass reads the same error word and column pointers as the main kernel */
+			o << "  unsigned* const err = (unsigned*)p.v[" << p.err_slot << "];\n";
+			for (size_t c = 0; c < p.cols.size(); c++) {
+				o << "  const " << ctype(p.cols[c].type) << "* __restrict__ c" << c << " = (const "
+				  << ctype(p.cols[c].type) << "*)p.v[" << p.col_slots[c] << "];\n";
+			}
+		} else {
+			p.err_slot = (int)params.size();
+			o << "  unsigned* const err = (unsigned*)p.v[" << params.size() << "];\n";
+			params.push_back(0); /* error word, filled by the runtime */
+			p.col_slots.clear();
+			for (size_t c = 0; c < p.cols.size(); c++) {
+				p.col_slots.push_back((int)params.size());
+				o << "  const " << ctype(p.cols[c].type) << "* __restrict__ c" << c << " = (const "
+				  << ctype(p.cols[c].type) << "*)p.v[" << params.size() << "];\n";
+				params.push_back(0); /* column pointer, filled by the runtime */
+			}
 		}
 		o << "  (void)err;\n";
 		o << "  extern __shared__ __align__(128) unsigned char vd_smem[];\n";
@@ -599,6 +606,9 @@ struct PipeGen {
 	std::vector<BExprP> sink_exprs() {
 		std::vector<BExprP> r;
 		for (auto& k : p.sink.keys) r.push_back(k);
+		if (part_hist) {
+			return r;
+		}
 		for (auto& k : p.sink.pay) r.push_back(k);
 		for (auto& a : p.sink.aggs) if (a.arg) r.push_back(a.arg);
 		for (auto& k : p.sink.outs) r.push_back(k);
@@ -636,6 +646,15 @@ struct PipeGen {
 		eager.assign(p.cols.size(), compact_at < 0);
 		carried.clear();
 		if (compact_at < 0) {
+			if (part_hist) {
+				/* the histogram pass reads only what the ops and the group keys need */
+				eager.assign(p.cols.size(), false);
+				for (auto& op : p.ops) {
+					if (op.pred) cols_of(op.pred, eager);
+					for (auto& k : op.keys) cols_of(k, eager);
+				}
+				for (auto& k : p.sink.keys) cols_of(k, eager);
+			}
 			return;
 		}
 		for (int i = 0; i <= compact_at; i++) {
@@ -1384,69 +1403,93 @@ struct PipeGen {
 
 	/* ------------------------------------------------------- partitioned aggregation ---- */
 
-	/* pass 1 state: the CTA's staged records (shared memory: records, then per record its
-	 * partition << 16 | rank, then per partition its staged count and its offset in the
-	 * flush) and the flush that writes them out as one partition-ordered run */
+	/* per-run words of a partitioned group-by (PartPlan::ctl): item counter, partial-run
+	 * cursor, histogram done counter, then P record totals, P partition starts, P scatter
+	 * cursors (64-bit) and P split-item done counters (32-bit) */
+	std::string part_ctl_decl() {
+		const PartPlan& pp = st.part;
+		const int NP = pp.P;
+		std::ostringstream d;
+		d << "  unsigned long long* const pctl = " << Pptr(pp.ctl, "unsigned long long*") << ";\n";
+		d << "  unsigned long long* const ptot = pctl + 4;\n";
+		d << "  unsigned long long* const pstart = pctl + 4 + " << NP << ";\n";
+		d << "  unsigned long long* const pcur = pctl + 4 + " << 2 * NP << ";\n";
+		d << "  unsigned* const pdone = (unsigned*)(pctl + 4 + " << 3 * NP << ");\n";
+		d << "  (void)ptot; (void)pstart; (void)pcur; (void)pdone;\n";
+		return d.str();
+	}
+
+	/* partition of packed key pk: the top log2 P bits of its hash (the slot in a partition's
+	 * table takes the low bits) */
+	std::string part_of(const std::string& pk) {
+		return "((uint32_t)vd::mix_hash32((uint32_t)(" + pk + ")) >> " + std::to_string(32 - st.part.log2P) + ")";
+	}
+
+	/* pass 0 (histogram) and pass 1 (scatter) state.  Pass 0 counts each partition's records
+	 * per CTA in shared memory; the last CTA turns the totals into partition starts.  Pass 1
+	 * stages the CTA's records in shared memory (records, then per record its partition << 16
+	 * | rank, then per partition its staged count and its reserved position); a flush reserves
+	 * each partition's run with one atomic on that partition's cursor and scatters the records,
+	 * so every partition's records end up contiguous. */
 	void part_prologue() {
 		const PartPlan& pp = st.part;
 		const int NP = pp.P;
+		o << part_ctl_decl();
+		if (part_hist) {
+			smem_sink = (size_t)NP * 8;
+			o << "  uint32_t* const shist = (uint32_t*)vd_smem;\n";
+			o << "  for (int i = threadIdx.x; i < " << NP << "; i += blockDim.x) { shist[i] = 0u; }\n";
+			o << "  vd::block_sync();\n";
+			return;
+		}
 		const std::string RT = rec_type();
 		smem_sink = pp.smem1;
-		o << "  unsigned long long* const pctl = " << Pptr(pp.ctl, "unsigned long long*") << ";\n";
-		o << "  unsigned long long* const ptot = pctl + 4;\n";
 		o << "  " << RT << "* const pbuf = " << Pptr(pp.buf, RT + "*") << ";\n";
-		o << "  unsigned long long* const pseg = " << Pptr(pp.seg, "unsigned long long*") << ";\n";
 		o << "  const unsigned long long pcap = " << Pu((unsigned long long)pp.cap) << ";\n";
-		o << "  const unsigned long long pfmax = " << Pu((unsigned long long)pp.fmax) << ";\n";
 		o << "  " << RT << "* const srec = (" << RT << "*)vd_smem;\n";
 		o << "  uint32_t* const smeta = (uint32_t*)(vd_smem + " << (size_t)pp.C * 8 * pp.rec_words << ");\n";
 		o << "  uint32_t* const shist = smeta + " << pp.C << ";\n";
-		o << "  uint32_t* const soff = shist + " << NP << ";\n";
-		o << "  __shared__ uint32_t pscan[33];\n";
-		o << "  __shared__ unsigned long long pfl[2];\n";
+		o << "  uint32_t* const sbase = shist + " << NP << ";\n";
 		o << "  __shared__ uint32_t pcount;\n";
 		o << "  for (int i = threadIdx.x; i < " << NP << "; i += blockDim.x) { shist[i] = 0u; }\n";
 		o << "  if (threadIdx.x == 0) { pcount = 0u; }\n";
 		o << "  vd::block_sync();\n";
 		o << "  auto pflush = [&]() {\n";
 		o << "    const uint32_t pn = *(volatile uint32_t*)&pcount;\n";
-		o << "    vd::block_excl_scan(shist, soff, " << NP << ", pscan);\n";
-		o << "    if (threadIdx.x == 0) {\n";
-		o << "      pfl[0] = atomicAdd(&pctl[0], (unsigned long long)pn);\n";
-		o << "      pfl[1] = atomicAdd(&pctl[1], 1ull);\n";
+		o << "    for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) {\n";
+		o << "      const uint32_t c = shist[q];\n";
+		o << "      shist[q] = 0u;\n";
+		o << "      uint32_t b = 0xffffffffu;\n";
+		o << "      if (c != 0u) {\n";
+		o << "        const unsigned long long at = __ldcg(&pstart[q]) + atomicAdd(&pcur[q], (unsigned long long)c);\n";
+		o << "        if (at + c <= pcap) { b = (uint32_t)at; } else { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
+		o << "      }\n";
+		o << "      sbase[q] = b;\n";
 		o << "    }\n";
 		o << "    vd::block_sync();\n";
-		o << "    const unsigned long long pb = pfl[0], pf = pfl[1];\n";
-		o << "    if (pb + pn <= pcap && pf < pfmax) {\n";
-		o << "      for (uint32_t i = threadIdx.x; i < pn; i += blockDim.x) {\n";
-		o << "        const uint32_t m = smeta[i];\n";
-		o << "        pbuf[pb + soff[m >> 16] + (m & 0xffffu)] = srec[i];\n";
-		o << "      }\n";
-		o << "      for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) {\n";
-		o << "        const uint32_t c = shist[q];\n";
-		o << "        pseg[pf * " << NP << "ull + q] = ((pb + soff[q]) << 16) | c;\n";
-		o << "        if (c) { atomicAdd(&ptot[q], (unsigned long long)c); }\n";
-		o << "        shist[q] = 0u;\n";
-		o << "      }\n";
-		o << "    } else {\n";
-		/* records beyond the capacity are dropped (the run fails with the error bit); the
-		 * flush's segment row, if it has one, still says so: no records */
-		o << "      if (threadIdx.x == 0) { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
-		o << "      for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) {\n";
-		o << "        if (pf < pfmax) { pseg[pf * " << NP << "ull + q] = 0ull; }\n";
-		o << "        shist[q] = 0u;\n";
-		o << "      }\n";
+		o << "    for (uint32_t i = threadIdx.x; i < pn; i += blockDim.x) {\n";
+		o << "      const uint32_t m = smeta[i];\n";
+		o << "      const uint32_t b = sbase[m >> 16];\n";
+		o << "      if (b != 0xffffffffu) { pbuf[b + (m & 0xffffu)] = srec[i]; }\n";
 		o << "    }\n";
 		o << "    if (threadIdx.x == 0) { pcount = 0u; }\n";
 		o << "    vd::block_sync();\n";
 		o << "  };\n";
 	}
 
-	/* pass 1 per row: the record, its partition (the top log2 P bits of the key's hash) and
-	 * its staging position; a stage without room for another round of rows is flushed first */
+	/* pass 0: count the row into its partition.  Pass 1: the record, its partition and its
+	 * staging position; a stage without room for another round of rows is flushed first. */
 	void part_row(const std::vector<Bounds>& kb) {
 		const PartPlan& pp = st.part;
 		const Sink& s = p.sink;
+		if (part_hist) {
+			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
+			o << "      if (act[v]) {\n";
+			o << "        const uint64_t pk = " << packed_key(s.keys, kb, s.key_shift, "v") << ";\n";
+			o << "        atomicAdd(&shist[" << part_of("pk") << "], 1u);\n";
+			o << "      }\n    }\n";
+			return;
+		}
 		o << "    vd::block_sync();\n";
 		o << "    if (*(volatile uint32_t*)&pcount + " << T * V << "u > " << pp.C << "u) { pflush(); }\n";
 		o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
@@ -1463,7 +1506,7 @@ struct PipeGen {
 			o << "        rw[" << pp.rec_word[a] << "] |= ((uint64_t)(" << expr(s.aggs[a].arg, "v") << ") - (uint64_t)" << lo
 			  << ") << " << pp.rec_off[a] << ";\n";
 		}
-		o << "        pt = (uint32_t)vd::mix_hash32((uint32_t)pk) >> " << 32 - pp.log2P << ";\n";
+		o << "        pt = " << part_of("pk") << ";\n";
 		o << "      }\n";
 		o << "      const unsigned bm = __ballot_sync(0xffffffffu, act[v]);\n";
 		o << "      uint32_t wb = 0u;\n";
@@ -1482,14 +1525,36 @@ struct PipeGen {
 		o << "    }\n";
 	}
 
-	/* pass 2: the persistent aggregation kernel over work items (one partition, or a share of
-	 * the flushes of a partition holding more than R records) */
+	/* end of pass 0: the CTA's counts into the totals; the last CTA writes the partition
+	 * starts (exclusive prefix sums of the totals).  End of pass 1: the last flush. */
+	void part_epilogue() {
+		const int NP = st.part.P;
+		o << "  vd::block_sync();\n";
+		if (!part_hist) {
+			o << "  if (*(volatile uint32_t*)&pcount > 0u) { pflush(); }\n";
+			return;
+		}
+		o << "  for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) {\n";
+		o << "    if (shist[q] != 0u) { atomicAdd(&ptot[q], (unsigned long long)shist[q]); }\n";
+		o << "  }\n";
+		o << "  __shared__ int hist_last;\n";
+		o << "  __shared__ uint32_t hscan[33];\n";
+		o << "  if (vd::last_block_done(&pctl[2], (unsigned long long)gridDim.x, &hist_last)) {\n";
+		o << "    uint32_t* const stot = shist + " << NP << ";\n";
+		o << "    for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) { stot[q] = (uint32_t)__ldcg(&ptot[q]); }\n";
+		o << "    vd::block_sync();\n";
+		o << "    vd::block_excl_scan(stot, shist, " << NP << ", hscan);\n";
+		o << "    for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) { pstart[q] = shist[q]; }\n";
+		o << "  }\n";
+	}
+
+	/* pass 2: the persistent aggregation kernel over work items (a partition's contiguous
+	 * records, or an equal share of them for a partition holding more than R records) */
 	std::string gen_part_aggregate() {
 		const PartPlan& pp = st.part;
 		const Sink& s = p.sink;
 		const int NP = pp.P, S = pp.S, W = s.nwords, AT = pp.agg_threads;
-		const int U = 4; /* record loads in flight per thread; a window's marks fill the count array */
-		static_assert(kPartSegs * 4 >= 512 * 4 * 2, "window marks must fit the segment count array");
+		const int U = 4; /* record loads in flight per thread */
 		const std::string RT = rec_type();
 		std::ostringstream k;
 		k << "extern \"C\" __global__ void __launch_bounds__(" << AT << ") " << name << "_extract(const VcParams p) {\n";
@@ -1498,36 +1563,29 @@ struct PipeGen {
 		k << "  int64_t* const out = " << Pptr(qs.out, "int64_t*") << ";\n";
 		k << "  const int64_t ocap = " << P((unsigned long long)qs.out_cap) << ";\n";
 		k << "  unsigned long long* const ocount = " << Pptr(qs.out_count, "unsigned long long*") << ";\n";
-		k << "  unsigned long long* const pctl = " << Pptr(pp.ctl, "unsigned long long*") << ";\n";
-		k << "  const unsigned long long* const ptot = pctl + 4;\n";
-		k << "  unsigned* const pdone = (unsigned*)(pctl + 4 + " << NP << ");\n";
+		k << part_ctl_decl();
 		k << "  const " << RT << "* __restrict__ pbuf = " << Pptr(pp.buf, "const " + RT + "*") << ";\n";
-		k << "  const unsigned long long* __restrict__ pseg = " << Pptr(pp.seg, "const unsigned long long*") << ";\n";
 		k << "  uint32_t* const xkeys = " << Pptr(pp.skeys, "uint32_t*") << ";\n";
 		k << "  unsigned long long* const xacc = " << Pptr(pp.sacc, "unsigned long long*") << ";\n";
 		k << "  unsigned long long* const xitems = " << Pptr(pp.items, "unsigned long long*") << ";\n";
 		k << "  const unsigned long long R = " << Pu((unsigned long long)pp.R) << ";\n";
-		k << "  const unsigned long long fmax = " << Pu((unsigned long long)pp.fmax) << ";\n";
 		k << "  const unsigned long long xcap = " << Pu((unsigned long long)pp.scratch) << ";\n";
 		k << "  extern __shared__ __align__(128) unsigned char vd_smem[];\n";
 		k << "  uint32_t* const skeys = (uint32_t*)vd_smem;\n";
 		k << "  unsigned long long* const sacc = (unsigned long long*)(vd_smem + " << (size_t)S * 4 << ");\n";
-		k << "  unsigned long long* const sseg = sacc + " << (size_t)S * W << ";\n";
-		k << "  uint32_t* const scnt = (uint32_t*)(sseg + " << kPartSegs << ");\n";
-		k << "  uint32_t* const spre = scnt + " << kPartSegs << ";\n";
-		k << "  uint32_t* const sk = spre + " << kPartSegs + 1 << ";\n";
+		k << "  uint32_t* const sk = (uint32_t*)(sacc + " << (size_t)S * W << ");\n";
 		k << "  uint32_t* const sa = sk + " << NP << ";\n";
 		k << "  uint32_t* const sb = sa + " << NP << ";\n";
+		k << "  uint32_t* const ka = sb + " << NP << ";\n";
+		k << "  uint32_t* const kb1 = ka + " << NP << ";\n";
 		k << "  __shared__ uint32_t xscan[33];\n";
-		k << "  __shared__ unsigned long long xres[33];\n";
+		k << "  __shared__ unsigned long long xres[1];\n";
 		k << "  __shared__ uint32_t xitem, xlast;\n";
 		k << "  __shared__ unsigned long long xrun;\n";
 		k << "  for (int i = threadIdx.x; i < " << S << "; i += blockDim.x) { skeys[i] = 0u; }\n";
 		k << "  for (int i = threadIdx.x; i < " << S * W << "; i += blockDim.x) { sacc[i] = 0ull; }\n";
-		/* items: every split partition's items first (by partition), then the partitions
-		 * that fit one item; the two counts' inputs borrow the segment arrays */
-		k << "  uint32_t* const ka = (uint32_t*)sseg;\n";
-		k << "  uint32_t* const kb1 = ka + " << NP << ";\n";
+		/* items: every split partition's items first (by partition), then the partitions that
+		 * fit one item */
 		k << "  for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) {\n";
 		k << "    const unsigned long long t = __ldcg(&ptot[q]);\n";
 		k << "    const uint32_t kq = (uint32_t)((t + R - 1ull) / R);\n";
@@ -1536,62 +1594,31 @@ struct PipeGen {
 		k << "  vd::block_sync();\n";
 		k << "  const uint32_t nA = vd::block_excl_scan(ka, sa, " << NP << ", xscan);\n";
 		k << "  const uint32_t nB = vd::block_excl_scan(kb1, sb, " << NP << ", xscan);\n";
-		k << "  const unsigned long long nf = __ldcg(&pctl[1]);\n";
-		k << "  const uint32_t F = (uint32_t)(nf < fmax ? nf : fmax);\n";
 		k << "  for (;;) {\n";
-		k << "    if (threadIdx.x == 0) { xitem = (uint32_t)atomicAdd(&pctl[2], 1ull); }\n";
+		k << "    if (threadIdx.x == 0) { xitem = (uint32_t)atomicAdd(&pctl[0], 1ull); }\n";
 		k << "    vd::block_sync();\n";
 		k << "    const uint32_t item = xitem;\n";
 		k << "    if (item >= nA + nB) { break; }\n";
 		k << "    int q;\n    uint32_t j, kq;\n";
 		k << "    if (item < nA) { q = vd::last_at_most(sa, " << NP << ", item); j = item - sa[q]; kq = sk[q]; }\n";
 		k << "    else { q = vd::last_at_most(sb, " << NP << ", item - nA); j = 0u; kq = 1u; }\n";
-		k << "    const uint32_t f0 = (uint32_t)((uint64_t)j * F / kq), f1 = (uint32_t)((uint64_t)(j + 1u) * F / kq);\n";
-		k << "    for (uint32_t fb = f0; fb < f1; fb += " << kPartSegs << "u) {\n";
-		k << "      const int nseg = (int)min((uint32_t)" << kPartSegs << ", f1 - fb);\n";
-		k << "      for (int i = threadIdx.x; i < nseg; i += blockDim.x) {\n";
-		k << "        const unsigned long long sw = __ldcg(&pseg[(uint64_t)(fb + (uint32_t)i) * " << NP << "ull + (uint64_t)q]);\n";
-		k << "        sseg[i] = sw;\n        scnt[i] = (uint32_t)(sw & 0xffffull);\n";
+		k << "    const unsigned long long t0 = __ldcg(&pstart[q]), tq = __ldcg(&ptot[q]);\n";
+		k << "    const unsigned long long ra = t0 + tq * j / kq, rb = t0 + tq * (j + 1u) / kq;\n";
+		k << "    for (unsigned long long base = ra; base < rb; base += (unsigned long long)blockDim.x * " << U << "u) {\n";
+		k << "      " << RT << " r[" << U << "];\n      bool live[" << U << "];\n";
+		k << "#pragma unroll\n      for (int u = 0; u < " << U << "; u++) {\n";
+		k << "        const unsigned long long i = base + (unsigned long long)(u * blockDim.x + threadIdx.x);\n";
+		k << "        live[u] = i < rb;\n";
+		k << "        if (live[u]) { r[u] = __ldcs(&pbuf[i]); }\n";
 		k << "      }\n";
-		k << "      vd::block_sync();\n";
-		k << "      const uint32_t tot = vd::block_excl_scan(scnt, spre, nseg, xscan);\n";
-		/* windows of blockDim.x * U records: each non-empty segment marks its first position
-		 * in the window (the one straddling the window start marks position 0), a running
-		 * maximum gives every position its segment; record j of the window goes to thread
-		 * j % blockDim.x, so a warp reads consecutive records */
-		k << "      uint16_t* const smark = (uint16_t*)scnt;\n";
-		k << "      const uint32_t wn = blockDim.x * " << U << "u;\n";
-		k << "      for (uint32_t base = 0; base < tot; base += wn) {\n";
-		k << "        for (uint32_t i = threadIdx.x; i < wn; i += blockDim.x) { smark[i] = 0; }\n";
-		k << "        vd::block_sync();\n";
-		/* the window's segments: from the one holding its first record to the one holding its
-		 * last (empty segments share the next one's prefix; the search takes the last) */
-		k << "        const int slo = vd::seg_of(spre, nseg, base);\n";
-		k << "        const int shi = vd::seg_of(spre, nseg, min(base + wn, tot) - 1u);\n";
-		k << "        for (int sg = slo + (int)threadIdx.x; sg <= shi; sg += blockDim.x) {\n";
-		k << "          const uint32_t b = spre[sg];\n";
-		k << "          if ((sseg[sg] & 0xffffull) != 0ull) { smark[b > base ? b - base : 0u] = (uint16_t)(sg + 1); }\n";
-		k << "        }\n";
-		k << "        vd::block_sync();\n";
-		k << "        vd::block_incl_max_scan_u16(smark, (int)wn, xscan);\n";
-		k << "        " << RT << " r[" << U << "];\n        bool live[" << U << "];\n";
-		k << "#pragma unroll\n        for (int u = 0; u < " << U << "; u++) {\n";
-		k << "          const uint32_t i = (uint32_t)u * blockDim.x + threadIdx.x;\n";
-		k << "          const uint32_t jj = base + i;\n";
-		k << "          live[u] = jj < tot;\n";
-		k << "          if (live[u]) {\n";
-		k << "            const int sg = (int)smark[i] - 1;\n";
-		k << "            r[u] = __ldcs(&pbuf[(sseg[sg] >> 16) + (jj - spre[sg])]);\n";
-		k << "          }\n";
-		k << "        }\n";
 		const std::string w0 = pp.rec_words == 2 ? "r[u].x" : "r[u]";
 		const std::string w1 = pp.rec_words == 2 ? "r[u].y" : "r[u]";
 		const unsigned long long kmask = (1ull << s.key_bits) - 1ull;
-		k << "#pragma unroll\n        for (int u = 0; u < " << U << "; u++) {\n";
-		k << "          const uint32_t pk = live[u] ? (uint32_t)(" << w0 << " & " << kmask << "ull) : 0xffffffffu;\n";
-		k << "          const unsigned gm = __match_any_sync(0xffffffffu, pk);\n";
-		k << "          const bool lead = live[u] && (gm & vd::lanemask_lt()) == 0u;\n";
-		k << "          uint64_t w[" << W << "] = {";
+		k << "#pragma unroll\n      for (int u = 0; u < " << U << "; u++) {\n";
+		k << "        const uint32_t pk = live[u] ? (uint32_t)(" << w0 << " & " << kmask << "ull) : 0xffffffffu;\n";
+		k << "        const unsigned gm = __match_any_sync(0xffffffffu, pk);\n";
+		k << "        const bool lead = live[u] && (gm & vd::lanemask_lt()) == 0u;\n";
+		k << "        uint64_t w[" << W << "] = {";
 		for (int i = 0; i < W; i++) {
 			k << (i ? ", " : "") << "0ull";
 		}
@@ -1599,26 +1626,24 @@ struct PipeGen {
 		for (int a = 0; a < A(); a++) {
 			const std::string sh = std::to_string(s.agg_shift[a]);
 			if (s.aggs[a].count) {
-				k << "          w[" << s.agg_word[a] << "] += (uint64_t)__popc(gm) << " << sh << ";\n";
+				k << "        w[" << s.agg_word[a] << "] += (uint64_t)__popc(gm) << " << sh << ";\n";
 				continue;
 			}
 			const int bits = span_bits(s.aggs[a].arg->b);
 			const unsigned long long fmask = (1ull << bits) - 1ull;
-			k << "          w[" << s.agg_word[a] << "] += vd::group_sum_u<" << bits << ">(gm, live[u] ? (("
-			  << (pp.rec_word[a] == 1 ? w1 : w0) << " >> " << pp.rec_off[a] << ") & " << fmask << "ull) : 0ull) << " << sh
-			  << ";\n";
+			k << "        w[" << s.agg_word[a] << "] += vd::group_sum_u<" << bits << ">(gm, live[u] ? ((" << (pp.rec_word[a] == 1 ? w1 : w0)
+			  << " >> " << pp.rec_off[a] << ") & " << fmask << "ull) : 0ull) << " << sh << ";\n";
 		}
-		k << "          if (lead) {\n";
-		k << "            const int sl = vd::st_find_or_insert(skeys, " << S << ", (uint32_t)vd::mix_hash32(pk), pk + 1u);\n";
-		k << "            if (sl >= 0) {\n";
-		k << "#pragma unroll\n              for (int a = 0; a < " << W << "; a++) { if (w[a]) { atomicAdd(&sacc[sl * " << W
+		k << "        if (lead) {\n";
+		k << "          const int sl = vd::st_find_or_insert(skeys, " << S << ", (uint32_t)vd::mix_hash32(pk), pk + 1u);\n";
+		k << "          if (sl >= 0) {\n";
+		k << "#pragma unroll\n            for (int a = 0; a < " << W << "; a++) { if (w[a]) { atomicAdd(&sacc[sl * " << W
 		  << " + a], (unsigned long long)w[a]); } }\n";
-		k << "            } else { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
-		k << "          }\n";
+		k << "          } else { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
 		k << "        }\n";
-		k << "        vd::block_sync();\n";
 		k << "      }\n";
 		k << "    }\n";
+		k << "    vd::block_sync();\n";
 		/* a split partition's item: leave the groups in a scratch run; the last item merges */
 		k << "    bool emit = kq == 1u;\n";
 		k << "    if (kq > 1u) {\n";
@@ -1626,7 +1651,7 @@ struct PipeGen {
 		k << "      for (int sl = threadIdx.x; sl < " << S << "; sl += blockDim.x) { mine += skeys[sl] != 0u ? 1u : 0u; }\n";
 		k << "      const uint32_t pre = vd::block_excl_sum(mine, xscan, &ng);\n";
 		k << "      if (threadIdx.x == 0) {\n";
-		k << "        const unsigned long long x0 = atomicAdd(&pctl[3], (unsigned long long)ng);\n";
+		k << "        const unsigned long long x0 = atomicAdd(&pctl[1], (unsigned long long)ng);\n";
 		k << "        if (x0 + ng > xcap) { atomicOr(err, VD_ERR_TABLE_FULL); ng = 0u; }\n";
 		k << "        xrun = (x0 << 16) | ng;\n";
 		k << "        xitems[item] = xrun;\n";
@@ -1677,14 +1702,13 @@ struct PipeGen {
 		k << "        vd::block_sync();\n";
 		k << "      }\n";
 		k << "    }\n";
-		/* the partition's result rows; the table is left clear for the next item */
+		/* the partition's result rows, reserved with one atomic; the table is left clear */
 		auto field = [&](int a) {
 			const int bits = s.agg_bits[a];
 			const unsigned long long mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
 			return "((w[" + std::to_string(s.agg_word[a]) + "] >> " + std::to_string(s.agg_shift[a]) + ") & " +
 				std::to_string(mask) + "ull)";
 		};
-		/* one reservation of result rows per item: count the groups, then write them */
 		k << "    if (emit) {\n";
 		k << "      uint32_t mine = 0u, ng;\n";
 		k << "      for (int sl = threadIdx.x; sl < " << S << "; sl += blockDim.x) { mine += skeys[sl] != 0u ? 1u : 0u; }\n";
@@ -1696,8 +1720,8 @@ struct PipeGen {
 		k << "        const uint32_t key = skeys[sl];\n";
 		k << "        if (key == 0u) { continue; }\n";
 		k << "        uint64_t w[" << W << "];\n";
-		k << "#pragma unroll\n        for (int a = 0; a < " << W << "; a++) { w[a] = key != 0u ? sacc[sl * " << W << " + a] : 0ull; }\n";
-		k << "        const bool take = key != 0u && (int64_t)" << field(s.count_idx) << " > 0;\n";
+		k << "#pragma unroll\n        for (int a = 0; a < " << W << "; a++) { w[a] = sacc[sl * " << W << " + a]; }\n";
+		k << "        const bool take = (int64_t)" << field(s.count_idx) << " > 0;\n";
 		k << "        if (take && pos < ocap) {\n";
 		k << "          const int64_t cnt = (int64_t)" << field(s.count_idx) << ";\n";
 		int col = 0;
@@ -1781,8 +1805,7 @@ struct PipeGen {
 			break;
 		case Sink::AggHash:
 			if (part()) {
-				o << "  vd::block_sync();\n";
-				o << "  if (*(volatile uint32_t*)&pcount > 0u) { pflush(); }\n";
+				part_epilogue();
 				break;
 			}
 			if (fl.aggr == "cache") {
@@ -1963,6 +1986,22 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 		const Flavor pfl = fl.for_pipe(p.id);
 		PipeGen g(p, plan, pfl, st[p.id], target, prm);
 		std::string main = g.gen_main();
+		const size_t main_smem = g.smem_total;
+		std::string hist;
+		size_t hist_smem = 0;
+		if (g.part()) {
+			/* the partitioned group-by's histogram pass: the same pipeline, counting rows per
+			 * partition */
+			g.o.str("");
+			g.o.clear();
+			g.smem_total = 0;
+			g.smem_sink = 0;
+			g.part_hist = true;
+			hist = g.gen_main();
+			hist_smem = g.smem_total;
+			g.part_hist = false;
+			g.smem_total = main_smem;
+		}
 		std::string extra;
 		if (p.sink.kind == Sink::JoinBuild && !plan.joins[p.sink.join].direct) {
 			extra = g.gen_join_build();
@@ -1971,9 +2010,20 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 		}
 		src << "#define VcParams VcParams" << p.id << "\n";
 		src << "struct VcParams" << p.id << " { unsigned long long v[" << std::max<size_t>(prm.size(), 1) << "]; };\n";
-		src << main << extra;
+		src << hist << main << extra;
 		src << "#undef VcParams\n\n";
 
+		if (!hist.empty()) {
+			Launch h;
+			h.kernel = g.name + "_hist";
+			h.pipe = p.id;
+			h.stage = 0;
+			h.smem = hist_smem;
+			h.threads = pfl.threads;
+			const int64_t htile = (int64_t)pfl.threads * pfl.rows;
+			h.grid_items = std::max<int64_t>((p.rows + htile - 1) / htile, 1);
+			gc.launches.push_back(h);
+		}
 		Launch m;
 		m.kernel = g.name + "_main";
 		m.pipe = p.id;

@@ -978,20 +978,21 @@ __device__ __forceinline__ bool cache_add(unsigned long long* cache, int S, uint
 /* ------------------------------------------------------------------------------------------
  * Partitioned hash aggregation (flavor aggr=part).
  *
+ * Pass 0 runs the pipeline counting each partition's rows (partition: the high bits of the
+ * packed group key's hash); its last CTA turns the totals into partition starts.
+ *
  * Pass 1 (the pipeline's main kernel) turns every surviving row into a record -- the packed
  * group key and each aggregate's value minus its lower bound, bit fields of one or two
  * 64-bit words -- and stages the records of its CTA in shared memory, each with its
- * partition (high bits of the key's hash) and its rank within that partition.  A full stage
- * is flushed as one run ordered by partition: the CTA reserves the run and a flush index
- * with one atomic each, scatters the records to run start + partition offset + rank, and
- * writes the flush's row of the segment table, seg[f * P + p] = (run position << 16) |
- * records of partition p.
+ * partition and its rank within that partition.  A full stage is flushed: one atomic per
+ * partition on that partition's cursor reserves its run, and the records are scattered to
+ * partition start + run + rank, so every partition's records end up contiguous.
  *
  * Pass 2 (a persistent kernel) takes work items, each one partition or, for a partition
- * holding more than R records, a share of its flushes.  An item aggregates its records into
- * a shared-memory table (keys, then packed accumulator words) and writes the partition's
- * result rows; the items of a split partition leave their groups in a scratch run, and the
- * last of them to finish merges the others' runs before writing the rows.
+ * holding more than R records, an equal share of its records.  An item aggregates its
+ * records into a shared-memory table (keys, then packed accumulator words) and writes the
+ * partition's result rows; the items of a split partition leave their groups in a scratch
+ * run, and the last of them to finish merges the others' runs before writing the rows.
  * ------------------------------------------------------------------------------------------ */
 
 /* Exclusive prefix sums out[i] = in[0] + ... + in[i-1] over n values held in shared memory
@@ -1040,32 +1041,6 @@ __device__ __forceinline__ uint32_t block_excl_scan(const uint32_t* in, uint32_t
 	return total;
 }
 
-/* Rank of each thread's `take` among the block's takers (exclusive), and their number in
- * *total.  All threads call it; `scratch` holds 33 words of shared memory. */
-__device__ __forceinline__ uint32_t block_rank(bool take, uint32_t* scratch, uint32_t* total)
-{
-	const unsigned lane = lane_id(), warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-	const unsigned m = __ballot_sync(0xffffffffu, take);
-	if (lane == 0) {
-		scratch[warp] = (uint32_t)__popc(m);
-	}
-	block_sync();
-	if (threadIdx.x == 0) {
-		uint32_t run = 0;
-		for (unsigned w = 0; w < nw; w++) {
-			const uint32_t c = scratch[w];
-			scratch[w] = run;
-			run += c;
-		}
-		scratch[32] = run;
-	}
-	block_sync();
-	const uint32_t r = scratch[warp] + (uint32_t)__popc(m & lanemask_lt());
-	*total = scratch[32];
-	block_sync();
-	return r;
-}
-
 /* Exclusive prefix of x over the block's threads, and the block's sum in *total.  All threads
  * call it; `scratch` holds 33 words of shared memory. */
 __device__ __forceinline__ uint32_t block_excl_sum(uint32_t x, uint32_t* scratch, uint32_t* total)
@@ -1099,48 +1074,6 @@ __device__ __forceinline__ uint32_t block_excl_sum(uint32_t x, uint32_t* scratch
 	return r;
 }
 
-/* In-place inclusive running maximum over n 16-bit values in shared memory (n a multiple of
- * the block size; each thread takes n / blockDim.x consecutive ones).  All threads call it;
- * `scratch` holds 33 words of shared memory. */
-__device__ __forceinline__ void block_incl_max_scan_u16(uint16_t* a, int n, uint32_t* scratch)
-{
-	const int per = n / (int)blockDim.x;
-	const int b = (int)threadIdx.x * per;
-	const unsigned lane = lane_id(), warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-	uint32_t m = 0;
-	for (int i = 0; i < per; i++) {
-		m = max(m, (uint32_t)a[b + i]);
-	}
-	uint32_t x = m;
-#pragma unroll
-	for (int o = 1; o < 32; o <<= 1) {
-		const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-		if ((int)lane >= o) {
-			x = max(x, y);
-		}
-	}
-	const uint32_t before = __shfl_up_sync(0xffffffffu, x, 1);
-	if (lane == 31) {
-		scratch[warp] = x;
-	}
-	block_sync();
-	if (threadIdx.x == 0) {
-		uint32_t run = 0;
-		for (unsigned w = 0; w < nw; w++) {
-			const uint32_t c = scratch[w];
-			scratch[w] = run;
-			run = max(run, c);
-		}
-	}
-	block_sync();
-	uint32_t run = max(scratch[warp], lane ? before : 0u);
-	for (int i = 0; i < per; i++) {
-		run = max(run, (uint32_t)a[b + i]);
-		a[b + i] = (uint16_t)run;
-	}
-	block_sync();
-}
-
 /* Slot of stored key `key` (packed key + 1) in a shared-memory table of S (power of two)
  * slots, inserting it at the first free slot of its linear probe sequence from h; -1 when
  * every slot holds another key. */
@@ -1161,22 +1094,6 @@ __device__ __forceinline__ int st_find_or_insert(uint32_t* skeys, int S, uint32_
 		i = (i + 1) & (uint32_t)(S - 1);
 	}
 	return -1;
-}
-
-/* index of the segment holding virtual record j: the largest s < nseg with pre[s] <= j
- * (pre: exclusive prefix of the segments' record counts, pre[0] = 0) */
-__device__ __forceinline__ int seg_of(const uint32_t* pre, int nseg, uint32_t j)
-{
-	int lo = 0, hi = nseg - 1;
-	while (lo < hi) {
-		const int mid = (lo + hi + 1) >> 1;
-		if (pre[mid] <= j) {
-			lo = mid;
-		} else {
-			hi = mid - 1;
-		}
-	}
-	return lo;
 }
 
 /* the largest p < n with pre[p] <= x (pre non-decreasing, pre[0] = 0 <= x) */

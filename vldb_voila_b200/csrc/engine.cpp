@@ -472,15 +472,14 @@ void query_prepare(Query& q)
 		case Sink::AggHash:
 			ps.part = part_plan(p, plan, q.flavor.for_pipe(p.id), e.sms);
 			if (ps.part.P > 0) {
-				/* partitioned aggregation: records, segment table, partial groups of split
-				 * partitions and per-item runs; its per-run counters live in the arena */
+				/* partitioned aggregation: records, partial groups of split partitions and
+				 * per-item runs; its per-run counters live in the arena */
 				PartPlan& pp = ps.part;
 				pp.buf = dev_alloc(q, (size_t)pp.cap * 8 * pp.rec_words);
-				pp.seg = dev_alloc(q, (size_t)pp.fmax * pp.P * 8);
 				pp.skeys = dev_alloc(q, (size_t)pp.scratch * 4);
 				pp.sacc = dev_alloc(q, (size_t)pp.scratch * p.sink.nwords * 8);
 				pp.items = dev_alloc(q, (size_t)pp.max_items * 8);
-				pp.ctl = (unsigned long long*)arena_take(32 + (size_t)pp.P * 12);
+				pp.ctl = (unsigned long long*)arena_take(32 + (size_t)pp.P * 28);
 				if (!pp.ctl) {
 					throw Error(VC_ERR_UNSUPPORTED, "aggr=part: too many partitions for the per-run state");
 				}

@@ -331,19 +331,18 @@ struct PartPlan {
 	int rec_words = 1;         /* 64-bit words per record */
 	std::vector<int> rec_word, rec_off; /* per aggregate: its record field (count: -1) */
 	int agg_threads = 512;     /* threads of the aggregation kernel */
-	int64_t cap = 0;           /* record capacity */
-	int64_t fmax = 0;          /* flush capacity (rows of the segment table) */
+	int64_t cap = 0;           /* record capacity (below 2^32) */
 	int64_t R = 0;             /* records above which a partition is split over several items */
 	int64_t max_items = 0;
 	int64_t scratch = 0;       /* capacity of the split partitions' partial groups */
 	size_t smem1 = 0, smem2 = 0; /* dynamic shared memory of the two passes */
-	void* buf = nullptr;       /* records */
-	void* seg = nullptr;       /* fmax x P segment words */
+	void* buf = nullptr;       /* records, partition after partition */
 	void* skeys = nullptr;     /* partial groups: stored keys */
 	void* sacc = nullptr;      /* partial groups: accumulator words */
 	void* items = nullptr;     /* per split item: (scratch position << 16) | groups */
-	unsigned long long* ctl = nullptr; /* per run: record cursor, flush count, item counter,
-	                                    * partial cursor, P record totals, P done counters (u32) */
+	unsigned long long* ctl = nullptr; /* per run: item counter, partial cursor, histogram done
+	                                    * counter, P record totals, P starts, P scatter cursors,
+	                                    * P split-item done counters (u32) */
 };
 
 /* the partitioned aggregation of pipeline p under flavor f, or P == 0 when it does not apply

@@ -11,7 +11,7 @@ FLAVORS = ["", "cuda(load=tma,stages=2)", "cuda(lowcard=private,prefetch=0)", "c
            "cuda(compact=0,rows=8,threads=128)", "cuda(hash=voila,compact=-1)", "cuda(build=direct,prefetch=0)",
            "cuda(lowcard=redux,aggr=cache,cache=64)", "cuda(lowcard=atomic,sinksmem=4096)",
            "cuda(build=direct,probe=8)", "cuda(aggr=part)", "cuda(aggr=part,parts=16,stage=2048,threads=128,rows=8)",
-           "cuda(aggr=part,load=tma,stages=2,compact=0)", "cuda(frows=4)", "cuda(frows=8,compact=0,aggr=part)"]
+           "cuda(aggr=part,load=tma,stages=2,compact=0)", "cuda(frows=1)", "cuda(frows=8,compact=0,aggr=part)"]
 
 
 def offline(spec):

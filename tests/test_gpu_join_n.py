@@ -31,7 +31,7 @@ PLANS = {
              "  ((col part.p_partkey)) ((col part.p_category)) (scan part (p_partkey p_category))))",
 }
 FLAVORS = ["", "cuda(build=staged)", "cuda(rows=1,threads=64,graph=0)", "cuda(load=tma,stages=3,aggr=cache,cache=64)",
-           "cuda(hash=voila,rows=8)", "cuda(frows=4,compact=0)", "cuda(aggr=part,frows=2,compact=0)"]
+           "cuda(hash=voila,rows=8)", "cuda(frows=1,compact=0)", "cuda(aggr=part,frows=2,compact=0)"]
 
 
 @pytest.fixture(scope="module")

@@ -274,59 +274,126 @@ struct PipeGen {
 		return std::max(bits, 1);
 	}
 
-	/* Warp pre-aggregation into packed accumulator words: lanes with the same group key
-	 * (__match_any_sync) sum each aggregate's biased value with redux.sync; the sums are
-	 * shifted into their word's bit field.  `lead` marks each group's lowest active lane. */
-	void emit_packed_words(const std::string& key, const std::string& v) {
-		const Sink& s = p.sink;
-		o << "      const unsigned gm = __match_any_sync(0xffffffffu, " << key << ");\n";
-		o << "      const bool lead = act[" << v << "] && (gm & vd::lanemask_lt()) == 0u;\n";
-		o << "      uint64_t w[" << s.nwords << "] = {";
-		for (int i = 0; i < s.nwords; i++) {
-			o << (i ? ", " : "") << "0ull";
+	/* One field of a warp pre-sum: a lane's biased (non-negative) value of `bits` bits, summed
+	 * into bit `shift` of accumulator word `word`; a count field sums one per lane. */
+	struct PresumField {
+		std::string val;
+		int word, shift, bits;
+		bool count;
+	};
+
+	/*
+	 * Warp pre-aggregation into packed accumulator words w[W].  Lanes with the same group key
+	 * (__match_any_sync of `key`, a sentinel on dead lanes) form a group; `lead` marks each
+	 * group's lowest live lane, which updates the table for the group.  A single-lane group
+	 * keeps its own values.  Groups of several lanes are summed one after another with
+	 * full-warp redux.sync (lanes outside the group add zero): redux.sync with each group's
+	 * own member mask would be executed once per distinct mask, so a warp of distinct keys
+	 * would pay for 32 serialised reductions; this way it pays for none.
+	 */
+	void emit_presum(std::ostream& k, const std::string& ind, const std::string& key, const std::string& live,
+		const std::vector<PresumField>& f, int W) {
+		k << ind << "const unsigned gm = __match_any_sync(0xffffffffu, " << key << ");\n";
+		k << ind << "const bool lead = (" << live << ") && (gm & vd::lanemask_lt()) == 0u;\n";
+		for (size_t i = 0; i < f.size(); i++) {
+			if (!f[i].count) {
+				k << ind << "const uint64_t fv" << i << " = (" << live << ") ? (uint64_t)(" << f[i].val << ") : 0ull;\n";
+			}
 		}
-		o << "};\n";
+		k << ind << "uint64_t w[" << W << "] = {";
+		for (int i = 0; i < W; i++) {
+			k << (i ? ", " : "") << "0ull";
+		}
+		k << "};\n";
+		for (size_t i = 0; i < f.size(); i++) {
+			if (f[i].count) {
+				k << ind << "w[" << f[i].word << "] += (uint64_t)((" << live << ") ? 1u : 0u) << " << f[i].shift << ";\n";
+			} else {
+				k << ind << "w[" << f[i].word << "] += fv" << i << " << " << f[i].shift << ";\n";
+			}
+		}
+		k << ind << "unsigned multi = __ballot_sync(0xffffffffu, lead && (gm & (gm - 1u)) != 0u);\n";
+		k << ind << "while (multi) {\n";
+		k << ind << "  const int gl = __ffs(multi) - 1;\n";
+		k << ind << "  multi &= multi - 1u;\n";
+		k << ind << "  const unsigned gg = __shfl_sync(0xffffffffu, gm, gl);\n";
+		k << ind << "  const bool gin = ((gg >> vd::lane_id()) & 1u) != 0u;\n";
+		k << ind << "  uint64_t g[" << W << "] = {";
+		for (int i = 0; i < W; i++) {
+			k << (i ? ", " : "") << "0ull";
+		}
+		k << "};\n";
+		for (size_t i = 0; i < f.size(); i++) {
+			if (f[i].count) {
+				k << ind << "  g[" << f[i].word << "] += (uint64_t)__popc(gg) << " << f[i].shift << ";\n";
+			} else {
+				k << ind << "  g[" << f[i].word << "] += vd::group_sum_u<" << f[i].bits << ">(0xffffffffu, gin ? fv" << i
+				  << " : 0ull) << " << f[i].shift << ";\n";
+			}
+		}
+		k << ind << "  if ((int)vd::lane_id() == gl) {\n";
+		k << ind << "#pragma unroll\n" << ind << "    for (int a = 0; a < " << W << "; a++) { w[a] = g[a]; }\n";
+		k << ind << "  }\n";
+		k << ind << "}\n";
+	}
+
+	/* the sink's aggregates as pre-sum fields of the packed accumulator words, values at row v */
+	std::vector<PresumField> sink_fields(const std::string& v) {
+		const Sink& s = p.sink;
+		std::vector<PresumField> f;
 		for (int a = 0; a < A(); a++) {
 			const auto& ag = s.aggs[a];
-			const std::string sh = std::to_string(s.agg_shift[a]);
 			if (ag.count) {
-				o << "      w[" << s.agg_word[a] << "] += (uint64_t)__popc(gm) << " << sh << ";\n";
+				f.push_back({"", s.agg_word[a], s.agg_shift[a], 0, true});
 				continue;
 			}
 			const std::string lo = P((unsigned long long)(int64_t)ag.arg->b.lo);
-			o << "      w[" << s.agg_word[a] << "] += vd::group_sum_u<" << row_bits(a) << ">(gm, (uint64_t)(" << expr(ag.arg, v)
-			  << ") - (uint64_t)" << lo << ") << " << sh << ";\n";
+			f.push_back({"(uint64_t)(" + expr(ag.arg, v) + ") - (uint64_t)" + lo, s.agg_word[a], s.agg_shift[a], row_bits(a), false});
 		}
+		return f;
 	}
 
-	/* Warp pre-aggregation of one row per lane: the lanes holding the same group key (`key`,
-	 * a 32- or 64-bit expression that is `sentinel` on inactive lanes) form a group; each
-	 * aggregate is summed over the group with redux.sync on the value biased by its lower
-	 * bound (so it is non-negative and has a known bit width), and `lead` marks the lowest
-	 * active lane of each group, which then holds the group's sums in vals[]. */
+	/* Warp pre-aggregation into packed accumulator words for row v (see emit_presum). */
+	void emit_packed_words(const std::string& key, const std::string& v) {
+		emit_presum(o, "      ", key, "act[" + v + "]", sink_fields(v), p.sink.nwords);
+	}
+
+	/* Warp pre-aggregation of one row per lane into vals[] (dense slots): lanes holding the
+	 * same slot (`key`, a sentinel on inactive lanes) form a group whose lowest active lane
+	 * (`lead`) ends up with the group's sums; a single-lane group keeps its own values, and
+	 * groups of several lanes are summed one after another with full-warp redux.sync on the
+	 * values biased by their lower bounds (non-negative, of known bit width). */
 	void emit_group_reduce(const std::string& key) {
 		o << "      const unsigned gm = __match_any_sync(0xffffffffu, " << key << ");\n";
 		o << "      const bool lead = act[v] && (gm & vd::lanemask_lt()) == 0u;\n";
-		o << "      const uint64_t gn = (uint64_t)__popc(gm);\n";
+		std::vector<std::string> lo(A());
+		for (int a = 0; a < A(); a++) {
+			const auto& ag = p.sink.aggs[a];
+			if (!ag.count) {
+				lo[a] = P((unsigned long long)(int64_t)ag.arg->b.lo);
+				o << "      const uint64_t fv" << a << " = act[v] ? (uint64_t)vals[" << a << "] - (uint64_t)" << lo[a]
+				  << " : 0ull;\n";
+			}
+		}
+		o << "      unsigned multi = __ballot_sync(0xffffffffu, lead && (gm & (gm - 1u)) != 0u);\n";
+		o << "      while (multi) {\n";
+		o << "        const int gl = __ffs(multi) - 1;\n";
+		o << "        multi &= multi - 1u;\n";
+		o << "        const unsigned gg = __shfl_sync(0xffffffffu, gm, gl);\n";
+		o << "        const bool gin = ((gg >> vd::lane_id()) & 1u) != 0u;\n";
+		o << "        const uint64_t gn = (uint64_t)__popc(gg);\n";
 		for (int a = 0; a < A(); a++) {
 			const auto& ag = p.sink.aggs[a];
 			if (ag.count) {
-				o << "      vals[" << a << "] = (int64_t)gn;\n";
+				o << "        if ((int)vd::lane_id() == gl) { vals[" << a << "] = (int64_t)gn; }\n";
 				continue;
 			}
-			const __int128 span = ag.arg->b.hi - ag.arg->b.lo;
-			int bits = 64;
-			if (span >= 0 && span < ((__int128)1 << 64)) {
-				bits = 0;
-				for (unsigned __int128 x = (unsigned __int128)span; x; x >>= 1) {
-					bits++;
-				}
-				bits = std::max(bits, 1);
-			}
-			const std::string lo = P((unsigned long long)(int64_t)ag.arg->b.lo);
-			o << "      vals[" << a << "] = (int64_t)(vd::group_sum_u<" << bits << ">(gm, (uint64_t)vals[" << a
-			  << "] - (uint64_t)" << lo << ") + (uint64_t)" << lo << " * gn);\n";
+			o << "        const uint64_t gs" << a << " = vd::group_sum_u<" << row_bits(a) << ">(0xffffffffu, gin ? fv" << a
+			  << " : 0ull);\n";
+			o << "        if ((int)vd::lane_id() == gl) { vals[" << a << "] = (int64_t)(gs" << a << " + (uint64_t)" << lo[a]
+			  << " * gn); }\n";
 		}
+		o << "      }\n";
 	}
 
 	std::string agg_vals(const std::string& v) {
@@ -1284,7 +1351,7 @@ struct PipeGen {
 				  << "][" << W << "];\n";
 				o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
 				o << "      const uint64_t pk = act[v] ? (" << packed_key(s.keys, kb, s.key_shift, "v") << ") : 0ull;\n";
-				emit_packed_words("act[v] ? (unsigned long long)pk : ~0ull", "v");
+				emit_packed_words(p.sink.key_bits <= 31 ? "act[v] ? (unsigned)pk : 0xffffffffu" : "act[v] ? (unsigned long long)pk : ~0ull", "v");
 				o << "      ldr[v] = lead;\n      kk[v] = (" << K << ")(pk + 1ull);\n";
 				o << "      hk[v] = " << table_hash(s.keys, "pk", s.key_bits, "v") << ";\n";
 				o << "#pragma unroll\n      for (int a = 0; a < " << W << "; a++) { ww[v][a] = w[a]; }\n";
@@ -1304,7 +1371,7 @@ struct PipeGen {
 			}
 			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
 			o << "      const uint64_t pk = act[v] ? (" << packed_key(s.keys, kb, s.key_shift, "v") << ") : 0ull;\n";
-			emit_packed_words("act[v] ? (unsigned long long)pk : ~0ull", "v");
+			emit_packed_words(p.sink.key_bits <= 31 ? "act[v] ? (unsigned)pk : 0xffffffffu" : "act[v] ? (unsigned long long)pk : ~0ull", "v");
 			o << "      if (lead) {\n";
 			o << "        const uint64_t h = " << table_hash(s.keys, "pk", s.key_bits, "v") << ";\n";
 			o << "        const " << K << " key = (" << K << ")(pk + 1ull);\n";
@@ -1616,23 +1683,19 @@ struct PipeGen {
 		const unsigned long long kmask = (1ull << s.key_bits) - 1ull;
 		k << "#pragma unroll\n      for (int u = 0; u < " << U << "; u++) {\n";
 		k << "        const uint32_t pk = live[u] ? (uint32_t)(" << w0 << " & " << kmask << "ull) : 0xffffffffu;\n";
-		k << "        const unsigned gm = __match_any_sync(0xffffffffu, pk);\n";
-		k << "        const bool lead = live[u] && (gm & vd::lanemask_lt()) == 0u;\n";
-		k << "        uint64_t w[" << W << "] = {";
-		for (int i = 0; i < W; i++) {
-			k << (i ? ", " : "") << "0ull";
-		}
-		k << "};\n";
-		for (int a = 0; a < A(); a++) {
-			const std::string sh = std::to_string(s.agg_shift[a]);
-			if (s.aggs[a].count) {
-				k << "        w[" << s.agg_word[a] << "] += (uint64_t)__popc(gm) << " << sh << ";\n";
-				continue;
+		{
+			std::vector<PresumField> f;
+			for (int a = 0; a < A(); a++) {
+				if (s.aggs[a].count) {
+					f.push_back({"", s.agg_word[a], s.agg_shift[a], 0, true});
+					continue;
+				}
+				const int bits = span_bits(s.aggs[a].arg->b);
+				const unsigned long long fmask = (1ull << bits) - 1ull;
+				f.push_back({"(" + (pp.rec_word[a] == 1 ? w1 : w0) + " >> " + std::to_string(pp.rec_off[a]) + ") & " +
+					std::to_string(fmask) + "ull", s.agg_word[a], s.agg_shift[a], bits, false});
 			}
-			const int bits = span_bits(s.aggs[a].arg->b);
-			const unsigned long long fmask = (1ull << bits) - 1ull;
-			k << "        w[" << s.agg_word[a] << "] += vd::group_sum_u<" << bits << ">(gm, live[u] ? ((" << (pp.rec_word[a] == 1 ? w1 : w0)
-			  << " >> " << pp.rec_off[a] << ") & " << fmask << "ull) : 0ull) << " << sh << ";\n";
+			emit_presum(k, "        ", "pk", "live[u]", f, W);
 		}
 		k << "        if (lead) {\n";
 		k << "          const int sl = vd::st_find_or_insert(skeys, " << S << ", (uint32_t)vd::mix_hash32(pk), pk + 1u);\n";

@@ -64,7 +64,7 @@ std::string Flavor::str() const
 	if (probe_lanes != 1) {
 		o << ",probe=" << probe_lanes;
 	}
-	if (flush_rows != 1) {
+	if (flush_rows != 4) {
 		o << ",frows=" << flush_rows;
 	}
 	if (private_groups != 8) {

@@ -10,7 +10,7 @@ SPECS = ["sel_aggr:rows=1000", "join_aggr:build=100,probe=1000", "groupby:rows=1
 FLAVORS = ["", "cuda(load=tma,stages=2)", "cuda(lowcard=private,prefetch=0)", "cuda(aggr=cache,build=staged)",
            "cuda(compact=0,rows=8,threads=128)", "cuda(hash=voila,compact=-1)", "cuda(build=direct,prefetch=0)",
            "cuda(lowcard=redux,aggr=cache,cache=64)", "cuda(lowcard=atomic,sinksmem=4096)",
-           "cuda(build=direct,probe=8)", "cuda(aggr=part)", "cuda(aggr=part,parts=16,stage=2048,threads=128,rows=8)",
+           "cuda(build=direct,probe=8)", "cuda(aggr=part)", "cuda(aggr=part,parts=16,threads=128,rows=8)",
            "cuda(aggr=part,load=tma,stages=2,compact=0)", "cuda(frows=1)", "cuda(frows=8,compact=0,aggr=part)"]
 
 
@@ -200,9 +200,7 @@ def test_join_n_plans_compile(flavor):
     w, e = offline("star:rows=1000,custs=50")
     q = e.query(JOIN_N_PLAN, flavor)
     src = q.source()
-    # the match loop may walk the whole table; it is block-uniform when the sink stages rows
-    loop = "vd::block_any(anyp)" if "aggr=part" in flavor else "__any_sync"
-    assert loop in src and "1ull) * SPB" in src
+    assert "__any_sync" in src and "1ull) * SPB" in src  # the match loop may walk the whole table
     assert "vd::dense_test" not in src
 
 
@@ -280,33 +278,34 @@ def test_per_pipeline_flavor_overrides():
 
 
 def test_partitioned_aggregation_plan():
-    """aggr=part: a histogram pass counts each partition's rows, the pipeline's kernel stages
-    records and scatters them so each partition's records are contiguous, and a persistent
-    kernel aggregates each partition in shared memory and writes its result rows itself (no
-    group table, no extraction scan)."""
+    """aggr=part: a histogram pass counts each partition's rows per CTA, the pipeline's kernel
+    (same grid, same tiles per CTA) writes each record at its partition's next position, so
+    every partition's records are contiguous, and a persistent kernel aggregates each
+    partition in shared memory and writes its result rows itself (no group table, no
+    extraction scan)."""
     w, e = offline("groupby:rows=6000000,keys=1500000,zipf=0,seed=3")
     q = e.query(w.plan, "cuda(aggr=part)")
     src = q.source()
     info = q.info()
     # 2 x 1.5M groups / 4096 slots per partition table -> 1024 partitions
-    assert "pflush()" in src and "vd::block_excl_scan(stot, shist, 1024" in src
+    assert "vd::block_excl_scan(stot, shist, 1024" in src and "atomicAdd(&scur[" in src
     assert "vd::st_find_or_insert(skeys, 4096" in src and "gt_find_or_insert" not in src
     k = {x["name"]: x for x in info["kernels"]}
     assert [x["name"] for x in info["kernels"]] == ["vc_p0_hist", "vc_p0_main", "vc_p0_extract"]
     assert k["vc_p0_extract"]["threads"] == 512 and k["vc_p0_hist"]["smem"] == 1024 * 8
-    # records of key + two value fields fit one word; 8192 staged records + 1024 x 2 counters
-    assert k["vc_p0_main"]["smem"] == 8192 * 8 + 8192 * 4 + 1024 * 8
+    # the scatter pass keeps one cursor per partition in shared memory
+    assert k["vc_p0_main"]["smem"] == 1024 * 4
     # the histogram pass reads the key column only
     hist = src[src.index("vc_p0_hist"):src.index("vc_p0_main")]
     assert "load_rows<int32_t, 4>(c0" in hist and "(c1" not in hist and "(c2" not in hist
-    # an explicit partition count and stage size
-    src2 = e.query(w.plan, "cuda(aggr=part,parts=2048,stage=4096,threads=512)").source()
-    assert "vd::block_excl_scan(stot, shist, 2048" in src2 and "+ 2048u > 4096u" in src2
+    # an explicit partition count
+    src2 = e.query(w.plan, "cuda(aggr=part,parts=2048,threads=512)").source()
+    assert "vd::block_excl_scan(stot, shist, 2048" in src2
     # too few partitions for the groups bound: falls back to the global table
     assert "gt_find_or_insert" in e.query(w.plan, "cuda(aggr=part,parts=16)").source()
 
 
-@pytest.mark.parametrize("flavor", ["cuda(parts=24)", "cuda(parts=8)", "cuda(stage=1000)", "cuda(stage=32768)"])
+@pytest.mark.parametrize("flavor", ["cuda(parts=24)", "cuda(parts=8)", "cuda(parts=4096)", "cuda(frows=3)"])
 def test_bad_partition_knobs_are_rejected(flavor):
     w, e = offline("groupby:rows=1000,keys=100000")
     with pytest.raises(VoilaError) as ex:
@@ -319,7 +318,7 @@ def test_batched_partitioned_aggregation_uses_a_group_table():
     from vldb_voila_b200.engine import Batch
     w, e = offline("groupby:rows=100000,keys=100000")
     q = e.query(w.plan, "cuda(aggr=part)")
-    assert "pflush" in q.source()
+    assert "_hist" in q.source()
     b = Batch([q])
     src = b.source()
-    assert "gt_find_or_insert" in src and "pflush" not in src
+    assert "gt_find_or_insert" in src and "scur" not in src

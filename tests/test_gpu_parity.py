@@ -18,7 +18,7 @@ FLAVORS = ["", "cuda(rows=8,threads=128,load=tma,stages=3)", "cuda(aggr=cache,ca
            "cuda(hash=voila,lowcard=private,threads=128,fill=75)", "cuda(build=direct,prefetch=0)",
            "cuda(lowcard=redux,aggr=cache,cache=64)", "cuda(build=direct,probe=4,rows=2)",
            "cuda(build=staged,probe=32,compact=-1)", "cuda(aggr=part)",
-           "cuda(aggr=part,parts=16,stage=2048,threads=128,rows=8,load=tma,stages=2)", "cuda(frows=1)",
+           "cuda(aggr=part,parts=16,threads=128,rows=8,load=tma,stages=2)", "cuda(frows=1)",
            "cuda(frows=8,compact=0,threads=128,rows=2)"]
 
 

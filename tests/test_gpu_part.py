@@ -33,7 +33,7 @@ def check(spec, flavor, runs=2):
     "groupby:rows=5,keys=1000000,seed=13",
 ])
 @pytest.mark.parametrize("flavor", ["cuda(aggr=part,parts=16)", "cuda(aggr=part,parts=2048,threads=512,rows=8)",
-                                    "cuda(aggr=part,stage=2048,threads=64,rows=2)"])
+                                    "cuda(aggr=part,threads=64,rows=2)"])
 def test_partitioned_aggregation_vs_oracle(spec, flavor):
     check(spec, flavor)
 

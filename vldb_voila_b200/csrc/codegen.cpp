@@ -73,7 +73,6 @@ static int span_bits(const Bounds& b)
 
 PartPlan part_plan(const Pipeline& p, const LoweredPlan& plan, const Flavor& f, int sms)
 {
-	(void)sms;
 	PartPlan pp;
 	const Sink& s = p.sink;
 	if (f.aggr != "part" || s.kind != Sink::AggHash || s.key_bits > 31 || s.count_idx < 0) {
@@ -124,19 +123,10 @@ PartPlan part_plan(const Pipeline& p, const LoweredPlan& plan, const Flavor& f, 
 		pp.log2P++;
 	}
 	pp.S = S;
-	const int TV = f.threads * f.rows;
-	int C = f.stage ? f.stage : 8192;
-	while (C < 2 * TV) {
-		C <<= 1;
-	}
-	if (C > 16384) {
-		return PartPlan();
-	}
-	pp.C = C;
-	pp.smem1 = (size_t)C * 8 * pp.rec_words + (size_t)C * 4 + (size_t)P * 8;
-	if (pp.smem1 > 200 * 1024) {
-		return PartPlan();
-	}
+	/* the histogram and scatter passes run the same grid: at most the CTAs that the threads
+	 * of a CTA allow per SM */
+	pp.max_ctas = (int64_t)sms * std::max(1, 2048 / f.threads);
+	pp.smem1 = (size_t)P * 4;
 	bool joinn = false;
 	for (auto& op : p.ops) {
 		joinn = joinn || (op.kind == Op::Probe && !plan.joins[op.join].join01);
@@ -813,7 +803,7 @@ struct PipeGen {
 	/* sinks whose rows use block-wide collectives (appends): loops around them must be
 	 * uniform over the block, not just the warp */
 	bool sink_block_collective() const {
-		return p.sink.kind == Sink::Emit || (p.sink.kind == Sink::AggHash && part()) ||
+		return p.sink.kind == Sink::Emit ||
 			(p.sink.kind == Sink::JoinBuild && !plan.joins[p.sink.join].direct && !plan.joins[p.sink.join].dense);
 	}
 
@@ -1492,16 +1482,17 @@ struct PipeGen {
 		return "((uint32_t)vd::mix_hash32((uint32_t)(" + pk + ")) >> " + std::to_string(32 - st.part.log2P) + ")";
 	}
 
-	/* pass 0 (histogram) and pass 1 (scatter) state.  Pass 0 counts each partition's records
-	 * per CTA in shared memory; the last CTA turns the totals into partition starts.  Pass 1
-	 * stages the CTA's records in shared memory (records, then per record its partition << 16
-	 * | rank, then per partition its staged count and its reserved position); a flush reserves
-	 * each partition's run with one atomic on that partition's cursor and scatters the records,
-	 * so every partition's records end up contiguous. */
+	/* pass 0 (histogram) and pass 1 (scatter) state.  Both passes run the same grid over the
+	 * same tiles, so CTA b of pass 1 emits exactly the records CTA b of pass 0 counted.  Pass 0
+	 * counts each partition's rows in shared memory and writes its row of the count matrix;
+	 * the last CTA turns the totals into partition starts.  Pass 1 reserves, for each
+	 * partition, its CTA's run with one atomic on the partition's cursor, then writes each
+	 * record at its partition's next position: every partition's records end up contiguous. */
 	void part_prologue() {
 		const PartPlan& pp = st.part;
 		const int NP = pp.P;
 		o << part_ctl_decl();
+		o << "  uint32_t* const pcnt = " << Pptr(pp.cnt, "uint32_t*") << ";\n";
 		if (part_hist) {
 			smem_sink = (size_t)NP * 8;
 			o << "  uint32_t* const shist = (uint32_t*)vd_smem;\n";
@@ -1512,59 +1503,30 @@ struct PipeGen {
 		const std::string RT = rec_type();
 		smem_sink = pp.smem1;
 		o << "  " << RT << "* const pbuf = " << Pptr(pp.buf, RT + "*") << ";\n";
-		o << "  const unsigned long long pcap = " << Pu((unsigned long long)pp.cap) << ";\n";
-		o << "  " << RT << "* const srec = (" << RT << "*)vd_smem;\n";
-		o << "  uint32_t* const smeta = (uint32_t*)(vd_smem + " << (size_t)pp.C * 8 * pp.rec_words << ");\n";
-		o << "  uint32_t* const shist = smeta + " << pp.C << ";\n";
-		o << "  uint32_t* const sbase = shist + " << NP << ";\n";
-		o << "  __shared__ uint32_t pcount;\n";
-		o << "  for (int i = threadIdx.x; i < " << NP << "; i += blockDim.x) { shist[i] = 0u; }\n";
-		o << "  if (threadIdx.x == 0) { pcount = 0u; }\n";
+		o << "  const uint32_t pcap = (uint32_t)" << Pu((unsigned long long)pp.cap) << ";\n";
+		o << "  uint32_t* const scur = (uint32_t*)vd_smem;\n";
+		emit_pdl_wait();
+		o << "  for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) {\n";
+		o << "    const uint32_t c = __ldcg(&pcnt[(uint64_t)blockIdx.x * " << NP << "u + q]);\n";
+		o << "    scur[q] = c != 0u ? (uint32_t)(__ldcg(&pstart[q]) + atomicAdd(&pcur[q], (unsigned long long)c)) : 0u;\n";
+		o << "  }\n";
 		o << "  vd::block_sync();\n";
-		o << "  auto pflush = [&]() {\n";
-		o << "    const uint32_t pn = *(volatile uint32_t*)&pcount;\n";
-		o << "    for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) {\n";
-		o << "      const uint32_t c = shist[q];\n";
-		o << "      shist[q] = 0u;\n";
-		o << "      uint32_t b = 0xffffffffu;\n";
-		o << "      if (c != 0u) {\n";
-		o << "        const unsigned long long at = __ldcg(&pstart[q]) + atomicAdd(&pcur[q], (unsigned long long)c);\n";
-		o << "        if (at + c <= pcap) { b = (uint32_t)at; } else { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
-		o << "      }\n";
-		o << "      sbase[q] = b;\n";
-		o << "    }\n";
-		o << "    vd::block_sync();\n";
-		o << "    for (uint32_t i = threadIdx.x; i < pn; i += blockDim.x) {\n";
-		o << "      const uint32_t m = smeta[i];\n";
-		o << "      const uint32_t b = sbase[m >> 16];\n";
-		o << "      if (b != 0xffffffffu) { pbuf[b + (m & 0xffffu)] = srec[i]; }\n";
-		o << "    }\n";
-		o << "    if (threadIdx.x == 0) { pcount = 0u; }\n";
-		o << "    vd::block_sync();\n";
-		o << "  };\n";
 	}
 
-	/* pass 0: count the row into its partition.  Pass 1: the record, its partition and its
-	 * staging position; a stage without room for another round of rows is flushed first. */
+	/* pass 0: count the row into its partition.  Pass 1: write the row's record (the packed
+	 * key, then each summed value minus its lower bound) at its partition's next position. */
 	void part_row(const std::vector<Bounds>& kb) {
 		const PartPlan& pp = st.part;
 		const Sink& s = p.sink;
+		o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
+		o << "      if (act[v]) {\n";
+		o << "        const uint64_t pk = " << packed_key(s.keys, kb, s.key_shift, "v") << ";\n";
 		if (part_hist) {
-			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
-			o << "      if (act[v]) {\n";
-			o << "        const uint64_t pk = " << packed_key(s.keys, kb, s.key_shift, "v") << ";\n";
 			o << "        atomicAdd(&shist[" << part_of("pk") << "], 1u);\n";
 			o << "      }\n    }\n";
 			return;
 		}
-		o << "    vd::block_sync();\n";
-		o << "    if (*(volatile uint32_t*)&pcount + " << T * V << "u > " << pp.C << "u) { pflush(); }\n";
-		o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
-		o << "      uint64_t rw[2] = {0ull, 0ull};\n";
-		o << "      uint32_t pt = 0u;\n";
-		o << "      if (act[v]) {\n";
-		o << "        const uint64_t pk = " << packed_key(s.keys, kb, s.key_shift, "v") << ";\n";
-		o << "        rw[0] = pk;\n";
+		o << "        uint64_t rw[2] = {pk, 0ull};\n";
 		for (int a = 0; a < A(); a++) {
 			if (s.aggs[a].count) {
 				continue;
@@ -1573,36 +1535,29 @@ struct PipeGen {
 			o << "        rw[" << pp.rec_word[a] << "] |= ((uint64_t)(" << expr(s.aggs[a].arg, "v") << ") - (uint64_t)" << lo
 			  << ") << " << pp.rec_off[a] << ";\n";
 		}
-		o << "        pt = " << part_of("pk") << ";\n";
-		o << "      }\n";
-		o << "      const unsigned bm = __ballot_sync(0xffffffffu, act[v]);\n";
-		o << "      uint32_t wb = 0u;\n";
-		o << "      if (vd::lane_id() == 0u && bm) { wb = atomicAdd(&pcount, (uint32_t)__popc(bm)); }\n";
-		o << "      wb = __shfl_sync(0xffffffffu, wb, 0);\n";
-		o << "      if (act[v]) {\n";
-		o << "        const uint32_t pos = wb + (uint32_t)__popc(bm & vd::lanemask_lt());\n";
-		o << "        const uint32_t rank = atomicAdd(&shist[pt], 1u);\n";
+		o << "        const uint32_t at = atomicAdd(&scur[" << part_of("pk") << "], 1u);\n";
+		o << "        if (at < pcap) {\n";
 		if (pp.rec_words == 2) {
-			o << "        srec[pos] = make_ulonglong2(rw[0], rw[1]);\n";
+			o << "          pbuf[at] = make_ulonglong2(rw[0], rw[1]);\n";
 		} else {
-			o << "        srec[pos] = rw[0];\n";
+			o << "          pbuf[at] = rw[0];\n";
 		}
-		o << "        smeta[pos] = (pt << 16) | rank;\n";
-		o << "      }\n";
-		o << "    }\n";
+		o << "        } else { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
+		o << "      }\n    }\n";
 	}
 
-	/* end of pass 0: the CTA's counts into the totals; the last CTA writes the partition
-	 * starts (exclusive prefix sums of the totals).  End of pass 1: the last flush. */
+	/* end of pass 0: the CTA's counts into its row of the count matrix and the totals; the
+	 * last CTA writes the partition starts (exclusive prefix sums of the totals) */
 	void part_epilogue() {
 		const int NP = st.part.P;
-		o << "  vd::block_sync();\n";
 		if (!part_hist) {
-			o << "  if (*(volatile uint32_t*)&pcount > 0u) { pflush(); }\n";
 			return;
 		}
+		o << "  vd::block_sync();\n";
 		o << "  for (int q = threadIdx.x; q < " << NP << "; q += blockDim.x) {\n";
-		o << "    if (shist[q] != 0u) { atomicAdd(&ptot[q], (unsigned long long)shist[q]); }\n";
+		o << "    const uint32_t c = shist[q];\n";
+		o << "    pcnt[(uint64_t)blockIdx.x * " << NP << "u + q] = c;\n";
+		o << "    if (c != 0u) { atomicAdd(&ptot[q], (unsigned long long)c); }\n";
 		o << "  }\n";
 		o << "  __shared__ int hist_last;\n";
 		o << "  __shared__ uint32_t hscan[33];\n";
@@ -2076,6 +2031,7 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 		src << hist << main << extra;
 		src << "#undef VcParams\n\n";
 
+		int hist_launch = -1;
 		if (!hist.empty()) {
 			Launch h;
 			h.kernel = g.name + "_hist";
@@ -2085,6 +2041,8 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 			h.threads = pfl.threads;
 			const int64_t htile = (int64_t)pfl.threads * pfl.rows;
 			h.grid_items = std::max<int64_t>((p.rows + htile - 1) / htile, 1);
+			h.grid_cap = st[p.id].part.max_ctas;
+			hist_launch = (int)gc.launches.size();
 			gc.launches.push_back(h);
 		}
 		Launch m;
@@ -2096,6 +2054,10 @@ GeneratedCode generate_cuda(LoweredPlan& plan, const Flavor& fl, std::vector<Pip
 		const int64_t tile = (int64_t)pfl.threads * pfl.rows;
 		m.grid_items = std::max<int64_t>((p.rows + tile - 1) / tile, 1);
 		m.dominant = p.id == plan.result_pipe;
+		if (hist_launch >= 0) {
+			m.grid_with = hist_launch;
+			m.grid_cap = st[p.id].part.max_ctas;
+		}
 		if (p.sink.kind == Sink::AggGlobal || p.sink.kind == Sink::AggDense) {
 			/* the last-block publication needs every launched block to count itself */
 			m.grid_items = std::max<int64_t>(m.grid_items, 1);

@@ -978,15 +978,16 @@ __device__ __forceinline__ bool cache_add(unsigned long long* cache, int S, uint
 /* ------------------------------------------------------------------------------------------
  * Partitioned hash aggregation (flavor aggr=part).
  *
- * Pass 0 runs the pipeline counting each partition's rows (partition: the high bits of the
- * packed group key's hash); its last CTA turns the totals into partition starts.
+ * Pass 0 runs the pipeline counting each partition's rows per CTA (partition: the high bits
+ * of the packed group key's hash) into a CTAs x partitions count matrix; its last CTA turns
+ * the totals into partition starts.
  *
- * Pass 1 (the pipeline's main kernel) turns every surviving row into a record -- the packed
- * group key and each aggregate's value minus its lower bound, bit fields of one or two
- * 64-bit words -- and stages the records of its CTA in shared memory, each with its
- * partition and its rank within that partition.  A full stage is flushed: one atomic per
- * partition on that partition's cursor reserves its run, and the records are scattered to
- * partition start + run + rank, so every partition's records end up contiguous.
+ * Pass 1 (the pipeline's main kernel) runs the same grid over the same tiles, so each CTA
+ * emits exactly the rows it counted.  It reserves its run in every partition with one atomic
+ * on that partition's cursor, then writes each surviving row's record -- the packed group key
+ * and each aggregate's value minus its lower bound, bit fields of one or two 64-bit words --
+ * at its partition's next position (a shared-memory cursor): every partition's records end
+ * up contiguous.
  *
  * Pass 2 (a persistent kernel) takes work items, each one partition or, for a partition
  * holding more than R records, an equal share of its records.  An item aggregates its

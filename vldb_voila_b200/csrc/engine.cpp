@@ -73,9 +73,6 @@ std::string Flavor::str() const
 	if (parts) {
 		o << ",parts=" << parts;
 	}
-	if (stage) {
-		o << ",stage=" << stage;
-	}
 	o << ")";
 	for (auto& ov : overrides) {
 		o << ";p" << ov.first << "=" << ov.second;
@@ -209,11 +206,6 @@ void Flavor::apply(Flavor& f, const std::string& s0)
 			f.parts = num(0, 2048);
 			if (f.parts && (f.parts < 16 || (f.parts & (f.parts - 1)))) {
 				throw Error(1, "parts must be 0 or a power of two from 16 to 2048");
-			}
-		} else if (k == "stage") {
-			f.stage = num(0, 16384);
-			if (f.stage && (f.stage < 2048 || (f.stage & (f.stage - 1)))) {
-				throw Error(1, "stage must be 0 or a power of two from 2048 to 16384");
 			}
 		} else if (k == "ocap") {
 			f.out_rows = num(0, 1 << 30);
@@ -476,6 +468,7 @@ void query_prepare(Query& q)
 				 * per-item runs; its per-run counters live in the arena */
 				PartPlan& pp = ps.part;
 				pp.buf = dev_alloc(q, (size_t)pp.cap * 8 * pp.rec_words);
+				pp.cnt = dev_alloc(q, (size_t)pp.max_ctas * pp.P * 4);
 				pp.skeys = dev_alloc(q, (size_t)pp.scratch * 4);
 				pp.sacc = dev_alloc(q, (size_t)pp.scratch * p.sink.nwords * 8);
 				pp.items = dev_alloc(q, (size_t)pp.max_items * 8);
@@ -627,16 +620,33 @@ static void launch_all(Query& q, cudaStream_t stream, bool capturing = false)
 			VC_CHECK_CUDA(cudaEventCreate(&e));
 		}
 	}
+	std::vector<int64_t> grids(n, 1);
 	for (size_t i = 0; i < n; i++) {
 		const Launch& l = q.code.launches[i];
-		const int occ = st.occupancy[i];
 		const int g = q.flavor.for_pipe(l.pipe).grid;
+		int occ = st.occupancy[i];
+		if (l.grid_with >= 0) {
+			/* the same tiles per CTA as the launch it repeats: the smaller occupancy of both */
+			occ = std::min(occ, st.occupancy[(size_t)l.grid_with]);
+		}
+		for (size_t j = 0; j < n; j++) {
+			if (q.code.launches[j].grid_with == (int)i) {
+				occ = std::min(occ, st.occupancy[j]);
+			}
+		}
 		int64_t per_sm = g > 0 ? std::min(g, occ) : occ;
 		int64_t grid = (int64_t)q.eng->sms * per_sm;
 		if (l.grid_items > 0) {
 			grid = std::min<int64_t>(grid, l.grid_items);
 		}
-		grid = std::max<int64_t>(grid, 1);
+		if (l.grid_cap > 0) {
+			grid = std::min<int64_t>(grid, l.grid_cap);
+		}
+		grids[i] = std::max<int64_t>(grid, 1);
+	}
+	for (size_t i = 0; i < n; i++) {
+		const Launch& l = q.code.launches[i];
+		const int64_t grid = l.grid_with >= 0 ? grids[(size_t)l.grid_with] : grids[i];
 		void* args[] = {q.params[l.pipe].data()};
 		if (q.profile) {
 			VC_CHECK_CUDA(cudaEventRecordWithFlags(q.ev[2 * i], stream, capturing ? cudaEventRecordExternal : 0));

@@ -254,7 +254,6 @@ struct Flavor {
 	int private_groups = 8;   /* lowcard=private: groups per CTA with per-thread accumulators */
 	int flush_rows = 4;       /* compaction: survivors per thread and pass of a flush */
 	int parts = 0;            /* aggr=part: partitions (0 = from the groups bound) */
-	int stage = 0;            /* aggr=part: records a CTA stages before a flush (0 = 8192) */
 	int64_t out_rows = 0;     /* result row capacity of an emitting pipeline (0 = from its bound, at
 	                           * most 4 rows per input row + 2^20 when joinN probes multiply rows) */
 
@@ -310,6 +309,8 @@ struct Launch {
 	size_t smem = 0;
 	int threads = 256;
 	int64_t grid_items = 0;      /* work items that bound the grid (0 = persistent over SMs) */
+	int64_t grid_cap = 0;        /* most CTAs (0 = no limit) */
+	int grid_with = -1;          /* launch whose grid this one repeats (same tiles per CTA) */
 	bool dominant = false;       /* the fact pipeline's main kernel */
 	void** memset_ptr = nullptr; /* MemsetZero */
 	size_t memset_bytes = 0;
@@ -327,7 +328,6 @@ struct PartPlan {
 	int P = 0;                 /* partitions (power of two) */
 	int log2P = 0;
 	int S = 0;                 /* slots of a partition's shared-memory table (power of two) */
-	int C = 0;                 /* records staged per CTA */
 	int rec_words = 1;         /* 64-bit words per record */
 	std::vector<int> rec_word, rec_off; /* per aggregate: its record field (count: -1) */
 	int agg_threads = 512;     /* threads of the aggregation kernel */
@@ -336,7 +336,9 @@ struct PartPlan {
 	int64_t max_items = 0;
 	int64_t scratch = 0;       /* capacity of the split partitions' partial groups */
 	size_t smem1 = 0, smem2 = 0; /* dynamic shared memory of the two passes */
+	int64_t max_ctas = 0;      /* most CTAs of the histogram and scatter passes */
 	void* buf = nullptr;       /* records, partition after partition */
+	void* cnt = nullptr;       /* max_ctas x P: the histogram pass's count per CTA and partition */
 	void* skeys = nullptr;     /* partial groups: stored keys */
 	void* sacc = nullptr;      /* partial groups: accumulator words */
 	void* items = nullptr;     /* per split item: (scratch position << 16) | groups */

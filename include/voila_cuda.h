@@ -170,7 +170,10 @@ int vc_workload_batch(int count, uint64_t seed, int64_t min_rows, int64_t max_ro
  * state.  Replaces Compiler::_generate + call_cxx_compiler + voila_query_new
  * (compiler.cpp:19-57, :343-385; codegen.cpp:371-376).
  * flavor: "" or "cuda(key=value,...)" with keys threads, rows, load=ldg|tma, stages,
- * prefetch, compact, aggr=auto|dense|global|cache, cache, lowcard=combine|atomic|private|redux,
+ * prefetch, compact, frows (survivors per thread in a compaction flush, 1..8),
+ * aggr=auto|dense|global|cache|part (part: partitioned group-by, histogram + scatter + one
+ * shared-memory table per partition), parts (partitions of aggr=part, 16..2048), cache,
+ * lowcard=combine|atomic|private|redux, pgroups (groups per CTA of lowcard=private),
  * build=auto|direct|staged|dense, hash=mix|voila, fill, dense, sinksmem, gcap (group table
  * slots), ocap (result rows of an emitting plan), probe (1..32 lanes that probe one join key
  * together), grid, graph.
@@ -263,7 +266,9 @@ int vc_join_aggr_noalloc(const int32_t* build_key, const int32_t* build_attr, in
  * outlive the batch.  flavors may be NULL (each query's own) or hold one flavor per query
  * (NULL entries = the query's own).  tiles_per_item: tiles of a pipeline per work item.
  * Inside a batch, loads are plain (load=ldg), lowcard=private runs as lowcard=combine and
- * cache= is capped at 256 slots, since every CTA reserves the largest shape's shared memory. */
+ * cache= is capped at 256 slots, since every CTA reserves the largest shape's shared memory;
+ * a partitioned group-by (aggr=part) runs through a global group table, allocated on first
+ * use. */
 typedef struct vc_batch vc_batch;
 int vc_batch_new(vc_query** queries, int n, const char** flavors, int threads, int64_t tiles_per_item, vc_batch** out);
 int vc_batch_run(vc_batch* b, void* stream);

@@ -64,7 +64,7 @@ def test_hash_group_aggregates_share_accumulator_words():
     """sum(v1) (20-bit values), sum(v2) (6-bit) and count over 6M rows need 43, 29 and 23 bits:
     two 64-bit words, so each group update is two atomics instead of three."""
     w, e = offline("groupby:rows=6000000,keys=1500000,zipf=0.0,seed=3")
-    src = e.query(w.plan).source()
+    src = e.query(w.plan, "cuda(aggr=global)").source()
     assert "uint64_t w[2]" in src and "gt_add<2>" in src
     assert "gt_find_or_insert_pre<uint32_t>" in src  # first buckets of all rows loaded ahead
 
@@ -303,6 +303,10 @@ def test_partitioned_aggregation_plan():
     assert "vd::block_excl_scan(stot, shist, 2048" in src2
     # too few partitions for the groups bound: falls back to the global table
     assert "gt_find_or_insert" in e.query(w.plan, "cuda(aggr=part,parts=16)").source()
+    # aggr=auto partitions group-bys of more than 2^18 groups, not smaller ones
+    assert "_hist" in e.query(w.plan).source()
+    w2, e2 = offline("groupby:rows=6000000,keys=200000,zipf=0,seed=3")
+    assert "_hist" not in e2.query(w2.plan).source()
 
 
 @pytest.mark.parametrize("flavor", ["cuda(parts=24)", "cuda(parts=8)", "cuda(parts=4096)", "cuda(frows=3)"])

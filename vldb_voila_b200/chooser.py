@@ -58,6 +58,9 @@ def _hash_grid():
     for threads, rows, pf, aggr, fill in itertools.product(
             (256, 512), (2, 4), (0, 1), ("global", "cache,cache=256", "cache,cache=2048"), (50, 75)):
         out.append(f"cuda(threads={threads},rows={rows},prefetch={pf},aggr={aggr},fill={fill})")
+    # the partitioned group-by (histogram + scatter + shared-memory tables per partition)
+    for threads, rows in itertools.product((256, 512), (4, 8)):
+        out.append(f"cuda(threads={threads},rows={rows},aggr=part)")
     return out
 
 

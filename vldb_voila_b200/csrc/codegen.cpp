@@ -75,7 +75,10 @@ PartPlan part_plan(const Pipeline& p, const LoweredPlan& plan, const Flavor& f, 
 {
 	PartPlan pp;
 	const Sink& s = p.sink;
-	if (f.aggr != "part" || s.kind != Sink::AggHash || s.key_bits > 31 || s.count_idx < 0) {
+	/* aggr=auto partitions group-bys whose groups bound passes 2^18 (a global table of
+	 * several MiB and more, where random atomics into it dominate) */
+	const bool wanted = f.aggr == "part" || (f.aggr == "auto" && s.groups_bound >= (int64_t)1 << 18);
+	if (!wanted || s.kind != Sink::AggHash || s.key_bits > 31 || s.count_idx < 0) {
 		return PartPlan();
 	}
 	/* record: the packed key in the low bits of word 0, then each summed value (minus its
@@ -241,12 +244,6 @@ struct PipeGen {
 
 	int A() const { return (int)p.sink.aggs.size(); }
 	bool part_hist = false;    /* generating the histogram pass of a partitioned group-by */
-	/* an atomic add of int64 `v` into the dense slot array: shared-memory slots take the
-	 * 32-bit split add, global ones a 64-bit atomic */
-	std::string smem_or_global_add(const std::string& ptr, const std::string& v) const {
-		return dense_in_smem ? "vd::smem_add_u64(" + ptr + ", (uint64_t)" + v + ");"
-			: "atomicAdd(" + ptr + ", (unsigned long long)" + v + ");";
-	}
 	/* survivors each thread takes per pass of a compaction flush (gathers in flight) */
 	int FV() const { return fl.flush_rows; }
 	/* partitioned aggregation (aggr=part) of a standalone pipeline */
@@ -1305,7 +1302,7 @@ struct PipeGen {
 				o << "#pragma unroll\n          for (int a = 0; a < " << A() << "; a++) { priv[(code * " << A() << " + a) * "
 				  << T << " + threadIdx.x] += vals[a]; }\n";
 				o << "        } else {\n";
-				o << "#pragma unroll\n          for (int a = 0; a < " << A() << "; a++) { " << smem_or_global_add("&sacc[slot * " + std::to_string(A()) + " + a]", "vals[a]") << " }\n";
+				o << "#pragma unroll\n          for (int a = 0; a < " << A() << "; a++) { atomicAdd(&sacc[slot * " << A() << " + a], (unsigned long long)vals[a]); }\n";
 				o << "        }\n      }\n    }\n";
 				break;
 			}
@@ -1321,7 +1318,7 @@ struct PipeGen {
 				o << "#pragma unroll\n        for (int a = 0; a < " << A() << "; a++) { sacc[slot * " << A()
 				  << " + a] += (unsigned long long)vals[a]; }\n";
 			} else {
-				o << "#pragma unroll\n        for (int a = 0; a < " << A() << "; a++) { " << smem_or_global_add("&sacc[slot * " + std::to_string(A()) + " + a]", "vals[a]") << " }\n";
+				o << "#pragma unroll\n        for (int a = 0; a < " << A() << "; a++) { atomicAdd(&sacc[slot * " << A() << " + a], (unsigned long long)vals[a]); }\n";
 			}
 			o << "      }\n    }\n";
 			break;
@@ -1659,8 +1656,8 @@ struct PipeGen {
 		k << "        if (lead) {\n";
 		k << "          const int sl = vd::st_find_or_insert(skeys, " << S << ", (uint32_t)vd::mix_hash32(pk), pk + 1u);\n";
 		k << "          if (sl >= 0) {\n";
-		k << "#pragma unroll\n            for (int a = 0; a < " << W << "; a++) { if (w[a]) { vd::smem_add_u64(&sacc[sl * " << W
-		  << " + a], w[a]); } }\n";
+		k << "#pragma unroll\n            for (int a = 0; a < " << W << "; a++) { if (w[a]) { atomicAdd(&sacc[sl * " << W
+		  << " + a], (unsigned long long)w[a]); } }\n";
 		k << "          } else { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
 		k << "        }\n";
 		k << "      }\n";
@@ -1709,7 +1706,7 @@ struct PipeGen {
 		k << "            if (sl >= 0) {\n";
 		k << "#pragma unroll\n              for (int a = 0; a < " << W << "; a++) {\n";
 		k << "                const unsigned long long wv = __ldcg(&xacc[(b2 + e) * " << W << "ull + a]);\n";
-		k << "                if (wv) { vd::smem_add_u64(&sacc[sl * " << W << " + a], wv); }\n";
+		k << "                if (wv) { atomicAdd(&sacc[sl * " << W << " + a], wv); }\n";
 		k << "              }\n";
 		k << "            } else { atomicOr(err, VD_ERR_TABLE_FULL); }\n";
 		k << "          }\n";

@@ -715,25 +715,6 @@ __device__ __forceinline__ bool join_insert(JoinSlot<KeyT, PayT>* __restrict__ s
 	return false;
 }
 
-/* 64-bit add into a shared-memory word as 32-bit atomics: the low half, then the high half
- * with the low half's carry (each add's carry is decided by the value it saw, so the carries
- * sum to the true overflow).  Measured on B200: 32-bit shared-memory atomics run about four
- * times the rate of 64-bit ones.  The word is exact once every add has finished; it is never
- * read while adds are in flight. */
-__device__ __forceinline__ void smem_add_u64(unsigned long long* a, uint64_t v)
-{
-	unsigned* w = reinterpret_cast<unsigned*>(a);
-	const unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
-	unsigned c = 0u;
-	if (lo != 0u) {
-		const unsigned old = atomicAdd(w, lo);
-		c = old + lo < old ? 1u : 0u;
-	}
-	if (hi + c != 0u) {
-		atomicAdd(w + 1, hi + c);
-	}
-}
-
 /* ---------------------------------------------------------------- group tables --- */
 
 /*
@@ -861,7 +842,7 @@ __device__ __forceinline__ bool gt_cache_add(K* ckeys, unsigned long long* cacc,
 #pragma unroll
 			for (int a = 0; a < W; a++) {
 				if (w[a]) {
-					smem_add_u64(cacc + i * W + a, w[a]);
+					atomicAdd(cacc + i * W + a, (unsigned long long)w[a]);
 				}
 			}
 			return true;

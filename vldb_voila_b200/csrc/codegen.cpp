@@ -244,6 +244,9 @@ struct PipeGen {
 
 	int A() const { return (int)p.sink.aggs.size(); }
 	bool part_hist = false;    /* generating the histogram pass of a partitioned group-by */
+	/* compaction within each warp (no block barriers): when the rest of the pipeline needs no
+	 * block-wide collectives (appending sinks, JoinN loops over an appending sink) */
+	bool warp_compact() const { return !sink_block_collective(); }
 	/* survivors each thread takes per pass of a compaction flush (gathers in flight) */
 	int FV() const { return fl.flush_rows; }
 	/* partitioned aggregation (aggr=part) of a standalone pipeline */
@@ -904,6 +907,24 @@ struct PipeGen {
 		/* selection vector: the survivors' rows (and carried payloads) are appended to the
 		 * block's pending buffer; the rest of the pipeline runs once at least a full pass of
 		 * threads is pending, so every lane of the dependent gather/probe chain has a row */
+		if (warp_compact()) {
+			/* each warp appends its own survivors (ballot + rank) and flushes on its own */
+			o << "    {\n      int wcnt = 0;\n";
+			o << "#pragma unroll\n      for (int v = 0; v < " << V << "; v++) {\n";
+			o << "        const unsigned m = __ballot_sync(0xffffffffu, act[v]);\n";
+			o << "        if (act[v]) {\n";
+			o << "          const int pos = cpend + wcnt + __popc(m & vd::lanemask_lt());\n";
+			o << "          csel[pos] = r0 + v;\n";
+			for (size_t k = 0; k < carried.size(); k++) {
+				o << "          ccar" << k << "[pos] = pay" << carried[k].first << "_" << carried[k].second << "[v];\n";
+			}
+			o << "        }\n        wcnt += __popc(m);\n      }\n";
+			o << "      cpend += wcnt;\n    }\n";
+			o << "    __syncwarp();\n";
+			o << "    if (cpend >= " << 32 * FV() << ") { cflush(); }\n";
+			o << "    }\n";
+			return;
+		}
 		o << "    const int nsel = vd::block_compact_rows<" << V << ">(act, r0, csel + cpend, cscan, csel_pos);\n";
 		for (size_t k = 0; k < carried.size(); k++) {
 			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) { if (act[v]) { ccar" << k
@@ -922,21 +943,35 @@ struct PipeGen {
 		if (compact_at < 0) {
 			return;
 		}
-		const int cap = T * FV() + T * V;
+		const bool wc = warp_compact();
+		/* per warp (warp compaction) or per block: a flush's worth of rows plus one more tile */
+		const int lanes = wc ? 32 : T;
+		const int cap = lanes * FV() + lanes * V;
+		const std::string sel_t = p.rows <= (int64_t)UINT32_MAX ? "uint32_t" : "int64_t";
 		/* row indices as 32 bits when every row of the table fits */
-		o << "  __shared__ " << (p.rows <= (int64_t)UINT32_MAX ? "uint32_t" : "int64_t") << " csel[" << cap << "];\n";
-		o << "  __shared__ int cscan[33];\n";
-		o << "  int csel_pos[" << V << "];\n";
-		o << "  int cpend = 0;\n";
-		for (size_t k = 0; k < carried.size(); k++) {
-			o << "  __shared__ int64_t ccar" << k << "[" << cap << "];\n";
+		if (wc) {
+			o << "  __shared__ " << sel_t << " csel_all[" << (T / 32) * cap << "];\n";
+			o << "  " << sel_t << "* const csel = csel_all + (threadIdx.x >> 5) * " << cap << ";\n";
+			for (size_t k = 0; k < carried.size(); k++) {
+				o << "  __shared__ int64_t ccar" << k << "_all[" << (T / 32) * cap << "];\n";
+				o << "  int64_t* const ccar" << k << " = ccar" << k << "_all + (threadIdx.x >> 5) * " << cap << ";\n";
+			}
+		} else {
+			o << "  __shared__ " << sel_t << " csel[" << cap << "];\n";
+			o << "  __shared__ int cscan[33];\n";
+			o << "  int csel_pos[" << V << "];\n";
+			for (size_t k = 0; k < carried.size(); k++) {
+				o << "  __shared__ int64_t ccar" << k << "[" << cap << "];\n";
+			}
 		}
+		o << "  int cpend = 0;\n";
 		const int F = FV();
+		const std::string lane_ix = wc ? "(int)vd::lane_id()" : "(int)threadIdx.x";
 		o << "  auto cflush = [&]() {\n";
-		o << "    for (int base = 0; base < cpend; base += " << T * F << ") {\n";
+		o << "    for (int base = 0; base < cpend; base += " << lanes * F << ") {\n";
 		o << "      bool act[" << F << "];\n      int64_t row[" << F << "];\n";
 		o << "#pragma unroll\n      for (int v = 0; v < " << F << "; v++) {\n";
-		o << "        const int ci = base + v * " << T << " + (int)threadIdx.x;\n";
+		o << "        const int ci = base + v * " << lanes << " + " << lane_ix << ";\n";
 		o << "        act[v] = ci < cpend;\n";
 		o << "        row[v] = act[v] ? (int64_t)csel[ci] : 0;\n";
 		o << "      }\n";
@@ -974,14 +1009,14 @@ struct PipeGen {
 			const std::string pv = "pay" + std::to_string(carried[k].first) + "_" + std::to_string(carried[k].second);
 			o << "      int64_t " << pv << "[" << F << "];\n";
 			o << "#pragma unroll\n      for (int v = 0; v < " << F << "; v++) { " << pv << "[v] = act[v] ? ccar" << k << "[base + v * "
-			  << T << " + (int)threadIdx.x] : 0; }\n";
+			  << lanes << " + " << lane_ix << "] : 0; }\n";
 		}
 		lazy_rows = true;
 		emit_rest(compact_at + 1);
 		lazy_rows = false;
 		V = saveV;
 		o << "    }\n";
-		o << "    vd::block_sync();\n";
+		o << (wc ? "    __syncwarp();\n" : "    vd::block_sync();\n");
 		o << "    cpend = 0;\n";
 		o << "  };\n";
 	}

@@ -426,12 +426,15 @@ class Query:
         check(lib().vc_query_result_shape(self._h, ctypes.byref(r), ctypes.byref(c)))
         return r.value, c.value
 
-    def result(self):
-        """int64 array of shape (rows, cols), column-major (the C ABI's layout; no transpose)."""
+    def result(self, out=None):
+        """int64 array of shape (rows, cols), column-major (the C ABI's layout; no transpose).
+        out: an int64 buffer of at least rows * cols elements to fill (reused across runs it
+        saves the page faults of a fresh allocation); the result is then a view of it."""
         r, c = self.shape()
-        out = np.empty(max(r * c, 1), dtype=np.int64)
+        if out is None or out.size < max(r * c, 1):
+            out = np.empty(max(r * c, 1), dtype=np.int64)
         check(lib().vc_query_result_copy(self._h, out.ctypes.data, out.size))
-        return out[: r * c].reshape(c, r).T
+        return out.reshape(-1)[: r * c].reshape(c, r).T
 
     def result_text(self):
         return _text_call(lib().vc_query_result_text, self._h)

@@ -170,7 +170,7 @@ int vc_workload_batch(int count, uint64_t seed, int64_t min_rows, int64_t max_ro
  * state.  Replaces Compiler::_generate + call_cxx_compiler + voila_query_new
  * (compiler.cpp:19-57, :343-385; codegen.cpp:371-376).
  * flavor: "" or "cuda(key=value,...)" with keys threads, rows, load=ldg|tma, stages,
- * prefetch, compact, frows (survivors per thread in a compaction flush, 1..8),
+ * prefetch, compact, frows (survivors per thread in a compaction flush, 1..16),
  * aggr=auto|dense|global|cache|part (part: partitioned group-by, histogram + scatter + one
  * shared-memory table per partition), parts (partitions of aggr=part, 16..2048), cache,
  * lowcard=combine|atomic|private|redux, pgroups (groups per CTA of lowcard=private),

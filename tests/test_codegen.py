@@ -309,7 +309,7 @@ def test_partitioned_aggregation_plan():
     assert "_hist" not in e2.query(w2.plan).source()
 
 
-@pytest.mark.parametrize("flavor", ["cuda(parts=24)", "cuda(parts=8)", "cuda(parts=4096)", "cuda(frows=3)"])
+@pytest.mark.parametrize("flavor", ["cuda(parts=24)", "cuda(parts=8)", "cuda(parts=4096)", "cuda(frows=3)", "cuda(frows=32)"])
 def test_bad_partition_knobs_are_rejected(flavor):
     w, e = offline("groupby:rows=1000,keys=100000")
     with pytest.raises(VoilaError) as ex:

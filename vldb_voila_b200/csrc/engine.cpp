@@ -64,7 +64,7 @@ std::string Flavor::str() const
 	if (probe_lanes != 1) {
 		o << ",probe=" << probe_lanes;
 	}
-	if (flush_rows != 4) {
+	if (flush_rows != 8) {
 		o << ",frows=" << flush_rows;
 	}
 	if (private_groups != 8) {
@@ -196,9 +196,9 @@ void Flavor::apply(Flavor& f, const std::string& s0)
 				throw Error(1, "probe lanes must be a power of two");
 			}
 		} else if (k == "frows") {
-			f.flush_rows = num(1, 8);
+			f.flush_rows = num(1, 16);
 			if (f.flush_rows & (f.flush_rows - 1)) {
-				throw Error(1, "frows must be 1, 2, 4 or 8");
+				throw Error(1, "frows must be 1, 2, 4, 8 or 16");
 			}
 		} else if (k == "pgroups") {
 			f.private_groups = num(1, 16);

@@ -252,7 +252,7 @@ struct Flavor {
 	int64_t group_slots = 0;  /* hash group table slots (0 = sized from the groups bound and fill) */
 	int probe_lanes = 1;      /* lanes that probe one join key together (1 = each lane its own key) */
 	int private_groups = 8;   /* lowcard=private: groups per CTA with per-thread accumulators */
-	int flush_rows = 4;       /* compaction: survivors per thread and pass of a flush */
+	int flush_rows = 8;       /* compaction: survivors per thread and pass of a flush */
 	int parts = 0;            /* aggr=part: partitions (0 = from the groups bound) */
 	int64_t out_rows = 0;     /* result row capacity of an emitting pipeline (0 = from its bound, at
 	                           * most 4 rows per input row + 2^20 when joinN probes multiply rows) */

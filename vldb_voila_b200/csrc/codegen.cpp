@@ -245,8 +245,17 @@ struct PipeGen {
 	int A() const { return (int)p.sink.aggs.size(); }
 	bool part_hist = false;    /* generating the histogram pass of a partitioned group-by */
 	/* compaction within each warp (no block barriers): when the rest of the pipeline needs no
-	 * block-wide collectives (appending sinks, JoinN loops over an appending sink) */
-	bool warp_compact() const { return !sink_block_collective(); }
+	 * block-wide collectives (appending sinks, JoinN loops over an appending sink), and no
+	 * column is read in place from host memory -- there a block's flush, whose warps each take
+	 * consecutive survivors of one stretch of rows, makes fewer PCIe requests per gather */
+	bool warp_compact() const {
+		for (auto& c : p.cols) {
+			if (c.host) {
+				return false;
+			}
+		}
+		return !sink_block_collective();
+	}
 	/* survivors each thread takes per pass of a compaction flush (gathers in flight) */
 	int FV() const { return fl.flush_rows; }
 	/* partitioned aggregation (aggr=part) of a standalone pipeline */
@@ -947,22 +956,25 @@ struct PipeGen {
 		/* per warp (warp compaction) or per block: a flush's worth of rows plus one more tile */
 		const int lanes = wc ? 32 : T;
 		const int cap = lanes * FV() + lanes * V;
-		const std::string sel_t = p.rows <= (int64_t)UINT32_MAX ? "uint32_t" : "int64_t";
 		/* row indices as 32 bits when every row of the table fits */
-		if (wc) {
-			o << "  __shared__ " << sel_t << " csel_all[" << (T / 32) * cap << "];\n";
-			o << "  " << sel_t << "* const csel = csel_all + (threadIdx.x >> 5) * " << cap << ";\n";
-			for (size_t k = 0; k < carried.size(); k++) {
-				o << "  __shared__ int64_t ccar" << k << "_all[" << (T / 32) * cap << "];\n";
-				o << "  int64_t* const ccar" << k << " = ccar" << k << "_all + (threadIdx.x >> 5) * " << cap << ";\n";
-			}
-		} else {
-			o << "  __shared__ " << sel_t << " csel[" << cap << "];\n";
+		const bool sel32 = p.rows <= (int64_t)UINT32_MAX;
+		const std::string sel_t = sel32 ? "uint32_t" : "int64_t";
+		/* the buffers live in dynamic shared memory after the sink's (before any tile ring) */
+		const size_t copies = wc ? (size_t)(T / 32) : 1;
+		size_t off = (smem_sink + 15) & ~(size_t)15;
+		o << "  " << sel_t << "* const csel = (" << sel_t << "*)(vd_smem + " << off << ")"
+		  << (wc ? " + (threadIdx.x >> 5) * " + std::to_string(cap) : std::string()) << ";\n";
+		off += copies * cap * (sel32 ? 4 : 8);
+		for (size_t k = 0; k < carried.size(); k++) {
+			off = (off + 15) & ~(size_t)15;
+			o << "  int64_t* const ccar" << k << " = (int64_t*)(vd_smem + " << off << ")"
+			  << (wc ? " + (threadIdx.x >> 5) * " + std::to_string(cap) : std::string()) << ";\n";
+			off += copies * cap * 8;
+		}
+		smem_sink = off;
+		if (!wc) {
 			o << "  __shared__ int cscan[33];\n";
 			o << "  int csel_pos[" << V << "];\n";
-			for (size_t k = 0; k < carried.size(); k++) {
-				o << "  __shared__ int64_t ccar" << k << "[" << cap << "];\n";
-			}
 		}
 		o << "  int cpend = 0;\n";
 		const int F = FV();

@@ -497,6 +497,7 @@ def main():
                          "algorithmic_bytes": w.probe_bytes,
                          "logical_gbs": w.probe_bytes / (dom_avg / 1e3) / 1e9,
                          "kernel_ms": dom_avg,
+                         "kernel_share_of_step": dom_avg / ms,
                          "kernel_rows_per_s": w.fact_rows / (dom_avg / 1e3),
                          "stream_read_floor": {"gbs": floor_gbs, "frac_of_peak": floor_gbs / peak,
                                                "kernel_over_floor": statistics.mean(floor_ms) / dom_avg,

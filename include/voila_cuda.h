@@ -173,10 +173,10 @@ int vc_workload_batch(int count, uint64_t seed, int64_t min_rows, int64_t max_ro
  * prefetch, compact, frows (survivors per thread in a compaction flush, 1..16),
  * aggr=auto|dense|global|cache|part (part: partitioned group-by, histogram + scatter + one
  * shared-memory table per partition), parts (partitions of aggr=part, 16..2048), cache,
- * lowcard=combine|atomic|private|redux, pgroups (groups per CTA of lowcard=private),
+ * lowcard=combine|atomic|private|redux|regs|packed, pgroups (groups per CTA of lowcard=private|regs|packed),
  * build=auto|direct|staged|dense, hash=mix|voila, fill, dense, sinksmem, gcap (group table
  * slots), ocap (result rows of an emitting plan), probe (1..32 lanes that probe one join key
- * together), grid, graph.
+ * together), grid, minctas (CTAs per SM the main kernel's registers must allow), graph.
  * VC_ERR_INVALID for an unknown or out-of-range knob; VC_ERR_UNSUPPORTED when the flavor's
  * shared memory exceeds the device's per-CTA limit or build=dense meets a large key space. */
 int vc_query_new(vc_engine* eng, const char* plan, const char* flavor, vc_query** out);
@@ -265,7 +265,7 @@ int vc_join_aggr_noalloc(const int32_t* build_key, const int32_t* build_attr, in
  * vc_batch_run + vc_batch_wait, vc_query_result_* read each query's rows.  The queries must
  * outlive the batch.  flavors may be NULL (each query's own) or hold one flavor per query
  * (NULL entries = the query's own).  tiles_per_item: tiles of a pipeline per work item.
- * Inside a batch, loads are plain (load=ldg), lowcard=private runs as lowcard=combine and
+ * Inside a batch, loads are plain (load=ldg), lowcard=private|regs|packed run as lowcard=combine and
  * cache= is capped at 256 slots, since every CTA reserves the largest shape's shared memory;
  * a partitioned group-by (aggr=part) runs through a global group table, allocated on first
  * use. */

@@ -11,7 +11,9 @@ FLAVORS = ["", "cuda(load=tma,stages=2)", "cuda(lowcard=private,prefetch=0)", "c
            "cuda(compact=0,rows=8,threads=128)", "cuda(hash=voila,compact=-1)", "cuda(build=direct,prefetch=0)",
            "cuda(lowcard=redux,aggr=cache,cache=64)", "cuda(lowcard=atomic,sinksmem=4096)",
            "cuda(build=direct,probe=8)", "cuda(aggr=part)", "cuda(aggr=part,parts=16,threads=128,rows=8)",
-           "cuda(aggr=part,load=tma,stages=2,compact=0)", "cuda(frows=1)", "cuda(frows=8,compact=0,aggr=part)"]
+           "cuda(aggr=part,load=tma,stages=2,compact=0)", "cuda(frows=1)", "cuda(frows=8,compact=0,aggr=part)",
+           "cuda(lowcard=regs)", "cuda(lowcard=regs,load=tma,stages=2,rows=8,pgroups=4)",
+           "cuda(aggr=direct)", "cuda(aggr=dcache,cache=256)"]
 
 
 def offline(spec):
@@ -303,10 +305,18 @@ def test_partitioned_aggregation_plan():
     assert "vd::block_excl_scan(stot, shist, 2048" in src2
     # too few partitions for the groups bound: falls back to the global table
     assert "gt_find_or_insert" in e.query(w.plan, "cuda(aggr=part,parts=16)").source()
-    # aggr=auto partitions group-bys of more than 2^18 groups, not smaller ones
-    assert "_hist" in e.query(w.plan).source()
-    w2, e2 = offline("groupby:rows=6000000,keys=200000,zipf=0,seed=3")
-    assert "_hist" not in e2.query(w2.plan).source()
+    # aggr=auto: a key space no larger than the hash table would be takes the direct table
+    # (slot = packed key); a wider one with more than 2^18 groups is partitioned, fewer
+    # groups take the hash table
+    auto = e.query(w.plan).source()
+    assert "_hist" not in auto and "gt_find_or_insert" not in auto and "gt_cache_add" in auto
+    wide = ("(aggr hash ((col k)) ((fun sum (col lineitem.l_extendedprice)) (fun count)) (project ((assign k "
+            "(fun * (col lineitem.l_orderkey) (const 1000))) (col lineitem.l_extendedprice)) "
+            "(scan lineitem (l_orderkey l_extendedprice))))")
+    assert "_hist" in e.query(wide).source()
+    w2, e2 = offline("groupby:rows=100000,keys=200000,zipf=0,seed=3")
+    src3 = e2.query(wide).source()
+    assert "_hist" not in src3 and "gt_find_or_insert" in src3
 
 
 @pytest.mark.parametrize("flavor", ["cuda(parts=24)", "cuda(parts=8)", "cuda(parts=4096)", "cuda(frows=3)", "cuda(frows=32)"])

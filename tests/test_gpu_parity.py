@@ -19,7 +19,9 @@ FLAVORS = ["", "cuda(rows=8,threads=128,load=tma,stages=3)", "cuda(aggr=cache,ca
            "cuda(lowcard=redux,aggr=cache,cache=64)", "cuda(build=direct,probe=4,rows=2)",
            "cuda(build=staged,probe=32,compact=-1)", "cuda(aggr=part)",
            "cuda(aggr=part,parts=16,threads=128,rows=8,load=tma,stages=2)", "cuda(frows=1)",
-           "cuda(frows=8,compact=0,threads=128,rows=2)"]
+           "cuda(frows=8,compact=0,threads=128,rows=2)", "cuda(lowcard=regs)",
+           "cuda(lowcard=regs,load=tma,stages=2,rows=8,pgroups=2,threads=128)", "cuda(lowcard=regs,rows=1,prefetch=0)",
+           "cuda(aggr=direct)", "cuda(aggr=dcache,cache=64,rows=8,threads=128)"]
 
 
 def run_gpu(w, plan, flavor="", on_device=False, data=None):
@@ -61,7 +63,9 @@ def test_full_size_vs_oracle(spec):
     e = Engine(0)
     e.load_workload(w, on_device=True)
     for flavor in ["", "cuda(load=tma)", "cuda(build=staged,aggr=cache)", "cuda(build=direct)", "cuda(aggr=part)",
-                   "cuda(aggr=part,threads=512,parts=256)", "cuda(frows=1)"]:
+                   "cuda(aggr=part,threads=512,parts=256)", "cuda(frows=1)",
+                   "cuda(lowcard=regs)", "cuda(lowcard=regs,load=tma,rows=8)", "cuda(aggr=direct)",
+                   "cuda(aggr=dcache)", "cuda(aggr=dcache,cache=256,threads=512,rows=2)"]:
         q = e.query(w.plan, flavor)
         q.run()
         assert q.result_lines() == expect, flavor

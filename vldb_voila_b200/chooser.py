@@ -46,7 +46,7 @@ def _load_modes():
 def _scan_grid():
     out = []
     for threads, rows, (load, pf, stages), lowcard in itertools.product(
-            (128, 256), (4, 8), _load_modes(), ("combine", "private", "redux")):
+            (128, 256), (4, 8), _load_modes(), ("combine", "private", "redux", "regs")):
         items = [f"threads={threads}", f"rows={rows}", f"load={load}", f"lowcard={lowcard}"]
         items += [f"prefetch={pf}"] if pf is not None else [f"stages={stages}"]
         out.append("cuda(" + ",".join(items) + ")")
@@ -61,6 +61,9 @@ def _hash_grid():
     # the partitioned group-by (histogram + scatter + shared-memory tables per partition)
     for threads, rows in itertools.product((256, 512), (4, 8)):
         out.append(f"cuda(threads={threads},rows={rows},aggr=part)")
+    # the direct table (slot = packed key), alone or behind the shared-memory cache
+    for threads, rows, aggr in itertools.product((256, 512), (2, 4), ("direct", "dcache,cache=256", "dcache,cache=2048")):
+        out.append(f"cuda(threads={threads},rows={rows},prefetch=1,aggr={aggr})")
     return out
 
 

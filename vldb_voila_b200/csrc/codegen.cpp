@@ -171,6 +171,12 @@ struct PipeGen {
 	std::map<const BExpr*, int> const_slot; /* parameter slot of each constant node */
 	bool private_acc = false;  /* per-thread private accumulators (lowcard=private) */
 	int kGmax = 8;             /* distinct groups per block held in private accumulators (pgroups) */
+	bool regs_acc = false;     /* per-thread packed accumulators (lowcard=regs|packed) */
+	bool regs_smem = false;    /* lowcard=packed: the packed words live in shared memory, one
+	                            * column per thread, indexed by the row's code */
+	int regs_tiles = 1;        /* tiles a thread sums into its registers between two flushes */
+	int regs_words = 0;        /* packed 64-bit words per group */
+	std::vector<int> rg_word, rg_shift, rg_bits; /* aggregate a's field, wide enough for a flush's rows */
 	static constexpr int kExtractK = 4; /* slot groups per warp step of the group extraction */
 
 	PipeGen(Pipeline& pp, LoweredPlan& pl, const Flavor& f, const PipeDeviceState& s, const QueryDeviceState& q,
@@ -262,10 +268,75 @@ struct PipeGen {
 	bool part() const { return st.part.P > 0 && !item; }
 	std::string rec_type() const { return st.part.rec_words == 2 ? "ulonglong2" : "unsigned long long"; }
 	/* stored key width of the split hash group table */
+	/* hash group-by with a per-CTA shared-memory cache (aggr=cache, or aggr=dcache and
+	 * aggr=auto over a direct table) */
+	bool gcache() const { return fl.aggr == "cache" || fl.aggr == "dcache" || (fl.aggr == "auto" && gdirect()); }
+	/* the group table is indexed by the packed key (aggr=direct|dcache): no keys, no probes */
+	bool gdirect() const { return st.sink_direct; }
 	int gkey_bytes() const { return p.sink.key_bits <= 31 ? 4 : 8; }
 	std::string gkey_type() const { return p.sink.key_bits <= 31 ? "uint32_t" : "uint64_t"; }
 
 	/* bits of value - lo for one row of aggregate a (the per-row span of the warp pre-sum) */
+	/* Packs every aggregate's sum over R rows of one thread (value minus lower bound; the
+	 * count) into bit fields of 64-bit words, first fit by decreasing width.  Returns the
+	 * number of words, or 0 when a field would not fit a word. */
+	int regs_pack(int64_t R, std::vector<int>& word, std::vector<int>& shift, std::vector<int>& bits) const {
+		int rb = 0;
+		for (int64_t x = R; x; x >>= 1) {
+			rb++;
+		}
+		const int n = A();
+		word.assign(n, 0);
+		shift.assign(n, 0);
+		bits.assign(n, 0);
+		std::vector<int> order(n);
+		for (int a = 0; a < n; a++) {
+			order[a] = a;
+			bits[a] = (p.sink.aggs[a].count ? 0 : row_bits(a)) + rb;
+			if (bits[a] > 64) {
+				return 0;
+			}
+		}
+		std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return bits[x] > bits[y]; });
+		std::vector<int> used;
+		for (int a : order) {
+			size_t w = 0;
+			while (w < used.size() && used[w] + bits[a] > 64) {
+				w++;
+			}
+			if (w == used.size()) {
+				used.push_back(0);
+			}
+			word[a] = (int)w;
+			shift[a] = used[w];
+			used[w] += bits[a];
+		}
+		return (int)used.size();
+	}
+
+	/* lowcard=regs: the flush interval (the most tiles whose packed fields take no more
+	 * words than those of a single tile, at least two) and the field layout */
+	bool plan_regs() {
+		std::vector<int> w, s, b;
+		const int w1 = regs_pack(V, w, s, b);
+		if (w1 == 0) {
+			return false;
+		}
+		const int limit = std::max(w1, 2);
+		for (int F = 16; F >= 1; F >>= 1) {
+			const int wf = regs_pack((int64_t)F * V, w, s, b);
+			if (wf != 0 && wf <= limit) {
+				regs_tiles = F;
+				regs_words = wf;
+				rg_word = w;
+				rg_shift = s;
+				rg_bits = b;
+				return kGmax * regs_words <= 48;
+			}
+		}
+		return false;
+	}
+
 	int row_bits(int a) const {
 		const auto& ag = p.sink.aggs[a];
 		const __int128 span = ag.arg->b.hi - ag.arg->b.lo;
@@ -456,7 +527,8 @@ struct PipeGen {
 			o << "  const struct { const unsigned long long* __restrict__ v; } p = {pv};\n";
 			o << "  (void)nitems;\n";
 		} else {
-			o << "extern \"C\" __global__ void __launch_bounds__(" << T << ") " << name << suffix
+			o << "extern \"C\" __global__ void __launch_bounds__(" << T
+			  << (fl.min_ctas > 0 ? ", " + std::to_string(fl.min_ctas) : std::string()) << ") " << name << suffix
 			  << "(const VcParams p) {\n";
 			o << "  vd::pdl_launch_dependents();\n";
 		}
@@ -561,8 +633,14 @@ struct PipeGen {
 		if (compact_at >= 0) {
 			o << "  if (cpend > 0) { cflush(); }\n";
 		}
+		if (regs_acc) {
+			o << "  rflush();\n";
+		}
 		sink_epilogue();
 		o << "}\n\n";
+		if (regs_acc) {
+			o << "#undef racc\n";
+		}
 		smem_total = std::max(smem_total, smem_sink);
 		return o.str();
 	}
@@ -909,6 +987,10 @@ struct PipeGen {
 		}
 		if (compact_at < 0) {
 			emit_rest(0);
+			if (regs_acc) {
+				/* block-uniform: every thread of the block runs the same tiles */
+				o << "    if (++rtiles == " << regs_tiles << ") { rflush(); rtiles = 0; }\n";
+			}
 			o << "    }\n";
 			return;
 		}
@@ -1260,6 +1342,71 @@ struct PipeGen {
 				  << " + threadIdx.x] = 0; }\n";
 				o << "  vd::block_sync();\n";
 			}
+			/* per-thread register accumulators: packed words for up to kGmax slots (codes of the
+			 * block's dictionary), summed over regs_tiles tiles, then folded per warp by
+			 * redux.sync into the block's slot array */
+			regs_smem = fl.lowcard == "packed";
+			regs_acc = (fl.lowcard == "regs" || regs_smem) && dense_in_smem && replicas == 1 && !item && compact_at < 0 &&
+				A() <= 32 &&
+				!has_join_n() && plan_regs();
+			if (regs_acc) {
+				const size_t dict_bytes = ((size_t)D * 4 + 4 * (kGmax + 1) + 15) & ~(size_t)15;
+				const size_t dict_off = (smem_sink + 15) & ~(size_t)15;
+				smem_sink = dict_off + dict_bytes;
+				const int RW = regs_words;
+				o << "  int* const pdict = (int*)(vd_smem + " << dict_off << ");\n";
+				o << "  int* const pcodes = pdict + " << P((unsigned long long)D) << ";\n";
+				o << "  int* const pncodes = pcodes + " << kGmax << ";\n";
+				o << "  for (int64_t i = threadIdx.x; i < " << P((unsigned long long)D)
+				  << "; i += blockDim.x) { pdict[i] = -1; }\n";
+				o << "  if (threadIdx.x == 0) { *pncodes = 0; }\n";
+				if (regs_smem) {
+					/* word j of code k of this thread at pacc[(k * RW + j) * T + thread] */
+					const size_t pacc_off = (smem_sink + 15) & ~(size_t)15;
+					smem_sink = pacc_off + (size_t)kGmax * RW * T * 8;
+					o << "  uint64_t* const pacc = (uint64_t*)(vd_smem + " << pacc_off << ") + threadIdx.x;\n";
+					o << "#define racc(k, j) pacc[((k) * " << RW << " + (j)) * " << T << "]\n";
+				} else {
+					o << "  uint64_t racc_r[" << kGmax << "][" << RW << "];\n";
+					o << "#define racc(k, j) racc_r[k][j]\n";
+				}
+				o << "#pragma unroll\n  for (int k = 0; k < " << kGmax << "; k++) {\n";
+				o << "#pragma unroll\n    for (int j = 0; j < " << RW << "; j++) { racc(k, j) = 0ull; }\n  }\n";
+				o << "  int rtiles = 0;\n";
+				o << "  vd::block_sync();\n";
+				/* warp-collective: every lane of the warp calls it at the same point */
+				const int cw = rg_word[s.count_idx];
+				o << "  auto rflush = [&]() {\n";
+				o << "    __threadfence_block();\n";
+				o << "#pragma unroll\n    for (int k = 0; k < " << kGmax << "; k++) {\n";
+				o << "      if (__any_sync(0xffffffffu, racc(k, " << cw << ") != 0ull)) {\n";
+				o << "        const int64_t sl = (int64_t)((volatile int*)pcodes)[k];\n";
+				o << "        uint64_t rw[" << RW << "];\n";
+				o << "#pragma unroll\n        for (int j = 0; j < " << RW << "; j++) { rw[j] = racc(k, j); }\n";
+				auto field = [&](int a) {
+					const unsigned long long mask = rg_bits[a] >= 64 ? ~0ull : ((1ull << rg_bits[a]) - 1ull);
+					return "vd::group_sum_u<" + std::to_string(rg_bits[a]) + ">(0xffffffffu, (rw[" +
+						std::to_string(rg_word[a]) + "] >> " + std::to_string(rg_shift[a]) + ") & " +
+						std::to_string(mask) + "ull)";
+				};
+				o << "        const uint64_t cnt = " << field(s.count_idx) << ";\n";
+				o << "        uint64_t mine = 0ull;\n";
+				for (int a = 0; a < A(); a++) {
+					if (a == s.count_idx) {
+						o << "        if (vd::lane_id() == " << a << "u) { mine = cnt; }\n";
+					} else if (s.aggs[a].count) {
+						o << "        if (vd::lane_id() == " << a << "u) { mine = " << field(a) << "; }\n";
+					} else {
+						o << "        { const uint64_t sa = " << field(a) << " + (uint64_t)"
+						  << P((unsigned long long)(int64_t)s.aggs[a].arg->b.lo) << " * cnt;\n";
+						o << "          if (vd::lane_id() == " << a << "u) { mine = sa; } }\n";
+					}
+				}
+				o << "        if (vd::lane_id() < " << A() << "u && mine != 0ull) { atomicAdd(&sacc[sl * " << A()
+				  << " + vd::lane_id()], (unsigned long long)mine); }\n";
+				o << "#pragma unroll\n        for (int j = 0; j < " << RW << "; j++) { racc(k, j) = 0ull; }\n";
+				o << "      }\n    }\n  };\n";
+			}
 			break;
 		}
 		case Sink::AggHash: {
@@ -1269,10 +1416,14 @@ struct PipeGen {
 			}
 			const std::string K = gkey_type();
 			const int W = s.nwords;
-			o << "  " << K << "* const gkeys = " << Pptr(st.sink_dev, K + "*") << ";\n";
-			o << "  unsigned long long* const gacc = " << Pptr(st.sink_acc, "unsigned long long*") << ";\n";
-			o << "  const uint64_t gbmask = " << Pu((unsigned long long)(st.sink_cap / (32 / gkey_bytes()) - 1)) << ";\n";
-			if (fl.aggr == "cache") {
+			if (gdirect()) {
+				o << "  unsigned long long* const gacc = " << Pptr(st.sink_acc, "unsigned long long*") << ";\n";
+			} else {
+				o << "  " << K << "* const gkeys = " << Pptr(st.sink_dev, K + "*") << ";\n";
+				o << "  unsigned long long* const gacc = " << Pptr(st.sink_acc, "unsigned long long*") << ";\n";
+				o << "  const uint64_t gbmask = " << Pu((unsigned long long)(st.sink_cap / (32 / gkey_bytes()) - 1)) << ";\n";
+			}
+			if (gcache()) {
 				const int S = (int)pow2_at_least(std::max(32, fl.cache_slots));
 				const size_t kbytes = ((size_t)S * gkey_bytes() + 15) & ~(size_t)15;
 				smem_sink = kbytes + (size_t)S * W * 8;
@@ -1342,6 +1493,42 @@ struct PipeGen {
 			}
 			o << "      const int64_t slot = act[v] ? (" << slot << ") : 0;\n";
 			o << "      " << agg_vals("v") << "\n";
+			if (regs_acc) {
+				o << "      const int code = act[v] ? vd::dict_code(pdict, pcodes, pncodes, slot, " << kGmax << ") : -2;\n";
+				o << "      if (code == -1) {\n";
+				o << "#pragma unroll\n        for (int a = 0; a < " << A() << "; a++) { "
+				  << "atomicAdd(&sacc[slot * " << A() << " + a], (unsigned long long)vals[a]); }\n";
+				o << "      }\n";
+				for (int j = 0; j < regs_words; j++) {
+					o << "      const uint64_t rw" << j << " = 0ull";
+					for (int a = 0; a < A(); a++) {
+						if (rg_word[a] != j) {
+							continue;
+						}
+						if (s.aggs[a].count) {
+							o << " + (1ull << " << rg_shift[a] << ")";
+						} else {
+							o << " + (((uint64_t)vals[" << a << "] - (uint64_t)" << P((unsigned long long)(int64_t)s.aggs[a].arg->b.lo)
+							  << ") << " << rg_shift[a] << ")";
+						}
+					}
+					o << ";\n";
+				}
+				if (regs_smem) {
+					o << "      if (code >= 0) {\n";
+					for (int j = 0; j < regs_words; j++) {
+						o << "        racc(code, " << j << ") += rw" << j << ";\n";
+					}
+					o << "      }\n    }\n";
+				} else {
+					o << "#pragma unroll\n      for (int k = 0; k < " << kGmax << "; k++) {\n";
+					for (int j = 0; j < regs_words; j++) {
+						o << "        racc(k, " << j << ") += code == k ? rw" << j << " : 0ull;\n";
+					}
+					o << "      }\n    }\n";
+				}
+				break;
+			}
 			if (private_acc) {
 				o << "      if (act[v]) {\n";
 				o << "        const int code = vd::dict_code(pdict, pcodes, pncodes, slot, " << kGmax << ");\n";
@@ -1381,7 +1568,16 @@ struct PipeGen {
 			}
 			const std::string K = gkey_type();
 			const int W = s.nwords;
-			if (fl.aggr != "cache") {
+			if (gdirect() && !gcache()) {
+				/* direct table: each group leader adds its warp's pre-sums at slot = packed key */
+				o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
+				o << "      const uint64_t pk = act[v] ? (" << packed_key(s.keys, kb, s.key_shift, "v") << ") : 0ull;\n";
+				emit_packed_words(p.sink.key_bits <= 31 ? "act[v] ? (unsigned)pk : 0xffffffffu" : "act[v] ? (unsigned long long)pk : ~0ull", "v");
+				o << "      if (lead) { vd::gt_add<" << W << ">(gacc, (int64_t)pk, w); }\n";
+				o << "    }\n";
+				break;
+			}
+			if (!gcache()) {
 				/* three phases so each thread keeps V bucket loads in flight: warp pre-sums of
 				 * every row, then the first bucket of every leader's probe, then the inserts
 				 * and atomics */
@@ -1413,10 +1609,14 @@ struct PipeGen {
 			o << "      if (lead) {\n";
 			o << "        const uint64_t h = " << table_hash(s.keys, "pk", s.key_bits, "v") << ";\n";
 			o << "        const " << K << " key = (" << K << ")(pk + 1ull);\n";
-			if (fl.aggr == "cache") {
+			if (gcache()) {
 				o << "        if (!vd::gt_cache_add<" << K << ", " << W << ">(ckeys, cacc, " << cache_slots << ", h, key, w)) {\n";
-				o << "          const int64_t slot = vd::gt_find_or_insert<" << K << ">(gkeys, gbmask, h, key, err);\n";
-				o << "          if (slot >= 0) { vd::gt_add<" << W << ">(gacc, slot, w); }\n";
+				if (gdirect()) {
+					o << "          vd::gt_add<" << W << ">(gacc, (int64_t)pk, w);\n";
+				} else {
+					o << "          const int64_t slot = vd::gt_find_or_insert<" << K << ">(gkeys, gbmask, h, key, err);\n";
+					o << "          if (slot >= 0) { vd::gt_add<" << W << ">(gacc, slot, w); }\n";
+				}
 				o << "        }\n";
 			} else {
 				o << "        const int64_t slot = vd::gt_find_or_insert<" << K << ">(gkeys, gbmask, h, key, err);\n";
@@ -1874,7 +2074,7 @@ struct PipeGen {
 				part_epilogue();
 				break;
 			}
-			if (fl.aggr == "cache") {
+			if (gcache()) {
 				const std::string K = gkey_type();
 				const int W = s.nwords;
 				o << "  vd::block_sync();\n";
@@ -1884,6 +2084,11 @@ struct PipeGen {
 				o << "      uint64_t w[" << W << "];\n";
 				o << "#pragma unroll\n      for (int a = 0; a < " << W << "; a++) { w[a] = cacc[i * " << W << " + a]; }\n";
 				o << "      const uint64_t pk = (uint64_t)sk - 1ull;\n";
+				if (gdirect()) {
+					o << "      vd::gt_add<" << W << ">(gacc, (int64_t)pk, w);\n";
+					o << "    }\n  }\n";
+					break;
+				}
 				std::string h;
 				for (size_t k = 0; k < s.keys.size(); k++) {
 					const int bits = (k + 1 < s.keys.size() ? s.key_shift[k + 1] : s.key_bits) - s.key_shift[k];
@@ -1961,7 +2166,9 @@ struct PipeGen {
 		k << "  int64_t* const out = " << Pptr(qs.out, "int64_t*") << ";\n";
 		k << "  const int64_t ocap = " << P((unsigned long long)qs.out_cap) << ";\n";
 		k << "  unsigned long long* const ocount = " << Pptr(qs.out_count, "unsigned long long*") << ";\n";
-		k << "  " << K << "* const gkeys = " << Pptr(st.sink_dev, K + "*") << ";\n";
+		if (!gdirect()) {
+			k << "  " << K << "* const gkeys = " << Pptr(st.sink_dev, K + "*") << ";\n";
+		}
 		k << "  unsigned long long* const gacc = " << Pptr(st.sink_acc, "unsigned long long*") << ";\n";
 		k << "  const int64_t nslots = " << P((unsigned long long)st.sink_cap) << ";\n";
 		/* a block takes chunks of blockDim.x * kExtractK slots (slot q * blockDim.x + thread of
@@ -1980,7 +2187,12 @@ struct PipeGen {
 		k << "    " << K << " kw[" << kExtractK << "];\n";
 		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
 		k << "      const int64_t i = cb + (int64_t)q * blockDim.x + threadIdx.x;\n";
-		k << "      kw[q] = i < nslots ? __ldcg(&gkeys[i]) : (" << K << ")0;\n";
+		if (gdirect()) {
+			/* a direct table's slot is its packed key */
+			k << "      kw[q] = i < nslots ? (" << K << ")(i + 1) : (" << K << ")0;\n";
+		} else {
+			k << "      kw[q] = i < nslots ? __ldcg(&gkeys[i]) : (" << K << ")0;\n";
+		}
 		k << "    }\n";
 		k << "    uint64_t w[" << kExtractK << "][" << W << "];\n";
 		k << "    bool take[" << kExtractK << "];\n    int ntake = 0;\n";
@@ -1996,7 +2208,12 @@ struct PipeGen {
 		  << " + a]) : 0ull; }\n";
 		k << "      take[q] = kw[q] != 0 && (int64_t)" << field(s.count_idx) << " > 0;\n";
 		k << "      ntake += take[q] ? 1 : 0;\n";
-		k << "      if (kw[q] != 0) {\n        gkeys[i] = 0;\n";
+		if (gdirect()) {
+			/* a used slot has a non-zero count */
+			k << "      if (take[q]) {\n";
+		} else {
+			k << "      if (kw[q] != 0) {\n        gkeys[i] = 0;\n";
+		}
 		k << "#pragma unroll\n        for (int a = 0; a < " << W << "; a++) { gacc[i * " << W << " + a] = 0ull; }\n      }\n";
 		k << "    }\n";
 		k << "    int64_t pos = vd::block_reserve(ocount, ntake, xres);\n";
@@ -2201,7 +2418,7 @@ BatchCode generate_batch(std::vector<Query*>& queries, const std::vector<Flavor>
 			Flavor f = flavors[qi].for_pipe(pipe);
 			f.threads = threads;
 			f.load = "ldg";
-			if (f.lowcard == "private") {
+			if (f.lowcard == "private" || f.lowcard == "regs" || f.lowcard == "packed") {
 				f.lowcard = "combine";
 			}
 			f.cache_slots = std::min(f.cache_slots, 256);

@@ -67,6 +67,9 @@ std::string Flavor::str() const
 	if (flush_rows != 8) {
 		o << ",frows=" << flush_rows;
 	}
+	if (min_ctas) {
+		o << ",minctas=" << min_ctas;
+	}
 	if (private_groups != 8) {
 		o << ",pgroups=" << private_groups;
 	}
@@ -180,8 +183,9 @@ void Flavor::apply(Flavor& f, const std::string& s0)
 				throw Error(1, "rows must be a power of two");
 			}
 		} else if (k == "aggr") {
-			if (v != "auto" && v != "dense" && v != "global" && v != "cache" && v != "part") {
-				throw Error(1, "aggr must be auto, dense, global, cache or part");
+			if (v != "auto" && v != "dense" && v != "global" && v != "cache" && v != "part" && v != "direct" &&
+				v != "dcache") {
+				throw Error(1, "aggr must be auto, dense, global, cache, part, direct or dcache");
 			}
 			f.aggr = v;
 		} else if (k == "cache") {
@@ -202,6 +206,8 @@ void Flavor::apply(Flavor& f, const std::string& s0)
 			}
 		} else if (k == "pgroups") {
 			f.private_groups = num(1, 16);
+		} else if (k == "minctas") {
+			f.min_ctas = num(0, 32);
 		} else if (k == "parts") {
 			f.parts = num(0, 2048);
 			if (f.parts && (f.parts < 16 || (f.parts & (f.parts - 1)))) {
@@ -227,8 +233,8 @@ void Flavor::apply(Flavor& f, const std::string& s0)
 		} else if (k == "compact") {
 			f.compact = v == "auto" ? -2 : num(-1, 64);
 		} else if (k == "lowcard") {
-			if (v != "combine" && v != "atomic" && v != "private" && v != "redux") {
-				throw Error(1, "lowcard must be combine, atomic, private or redux");
+			if (v != "combine" && v != "atomic" && v != "private" && v != "redux" && v != "regs" && v != "packed") {
+				throw Error(1, "lowcard must be combine, atomic, private, redux, regs or packed");
 			}
 			f.lowcard = v;
 		} else if (k == "hash") {
@@ -462,6 +468,29 @@ void query_prepare(Query& q)
 			ps.sink_bytes = (size_t)p.sink.domain * A * 8;
 			break;
 		case Sink::AggHash:
+			{
+				/* direct group table (aggr=direct|dcache, and aggr=auto where it is no larger
+				 * than the hash table would be): slot = packed key, so it needs no stored keys
+				 * and no probes; every packed key below the largest one has a slot */
+				const Flavor pf = q.flavor.for_pipe(p.id);
+				__int128 pkmax = 0;
+				for (size_t k = 0; k < p.sink.keys.size(); k++) {
+					pkmax += (p.sink.keys[k]->b.hi - p.sink.keys[k]->b.lo) << p.sink.key_shift[k];
+				}
+				const __int128 dbytes = (pkmax + 1) * p.sink.nwords * 8;
+				const __int128 hbytes = (__int128)std::max<int64_t>(pow2_at_least((std::max<int64_t>(p.sink.groups_bound, 1) *
+					100 + pf.fill - 1) / pf.fill), 1024) * ((p.sink.key_bits <= 31 ? 4 : 8) + p.sink.nwords * 8);
+				const bool want = pf.aggr == "direct" || pf.aggr == "dcache" ||
+					(pf.aggr == "auto" && pf.group_slots == 0 && dbytes <= std::max<__int128>(hbytes, (__int128)16 << 20));
+				/* a key space of 2^28 slots and more takes the hash table (aggr=dcache: behind
+				 * the same shared-memory cache) */
+				if (want && pkmax < ((__int128)1 << 28)) {
+					ps.sink_direct = true;
+					ps.sink_cap = (int64_t)pkmax + 1;
+					ps.sink_bytes = (size_t)ps.sink_cap * p.sink.nwords * 8;
+					break;
+				}
+			}
 			ps.part = part_plan(p, plan, q.flavor.for_pipe(p.id), e.sms);
 			if (ps.part.P > 0) {
 				/* partitioned aggregation: records, partial groups of split partitions and
@@ -511,7 +540,9 @@ void query_prepare(Query& q)
 				}
 			}
 		}
-		if (p.sink.kind == Sink::AggHash && ps.part.P == 0) {
+		if (p.sink.kind == Sink::AggHash && ps.sink_direct) {
+			ps.sink_acc = ps.sink_dev;
+		} else if (p.sink.kind == Sink::AggHash && ps.part.P == 0) {
 			const size_t kb = (((size_t)ps.sink_cap * (p.sink.key_bits <= 31 ? 4 : 8)) + 255) & ~(size_t)255;
 			ps.sink_acc = (char*)ps.sink_dev + kb;
 		}

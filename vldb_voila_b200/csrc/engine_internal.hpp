@@ -244,14 +244,18 @@ struct Flavor {
 	int compact = -2;         /* compact survivors after op k (-1 never, -2 auto) */
 	std::string lowcard = "combine"; /* dense aggregation: combine (warp pre-sum by shuffles) | atomic (per-warp
 	                                  * replicas) | private (per-thread accumulators behind a block dictionary)
-	                                  * | redux (warp pre-sum by redux.sync into per-warp replicas) */
+	                                  * | redux (warp pre-sum by redux.sync into per-warp replicas) | regs
+	                                  * (per-thread packed register accumulators behind a block dictionary,
+	                                  * folded per warp every few tiles) | packed (the same packed words in
+	                                  * shared memory, one column per thread) */
 	std::string hash = "mix"; /* table positions: mix (finalizer of the packed key) | voila (runtime.hpp hash) */
 	int fill = 50;            /* largest load factor (percent) of group tables */
 	int64_t direct_limit = 64ll << 20; /* auto: direct when the upper-bound table fits this many bytes */
 	int sink_smem = 96 * 1024; /* most shared memory a dense aggregation keeps its slots in (else global) */
 	int64_t group_slots = 0;  /* hash group table slots (0 = sized from the groups bound and fill) */
 	int probe_lanes = 1;      /* lanes that probe one join key together (1 = each lane its own key) */
-	int private_groups = 8;   /* lowcard=private: groups per CTA with per-thread accumulators */
+	int private_groups = 8;   /* lowcard=private|regs|packed: groups per CTA with per-thread accumulators */
+	int min_ctas = 0;         /* CTAs per SM the main kernel's registers must allow (0 = no bound) */
 	int flush_rows = 8;       /* compaction: survivors per thread and pass of a flush */
 	int parts = 0;            /* aggr=part: partitions (0 = from the groups bound) */
 	int64_t out_rows = 0;     /* result row capacity of an emitting pipeline (0 = from its bound, at
@@ -356,6 +360,8 @@ struct PipeDeviceState {
 	int64_t sink_cap = 0;
 	size_t sink_bytes = 0;
 	void* sink_acc = nullptr;            /* hash group table: accumulator words (sink_dev holds the keys) */
+	bool sink_direct = false;            /* group table indexed by the packed key itself (no keys
+	                                      * stored): sink_cap slots of accumulator words */
 	bool self_cleaning = false;          /* the pipeline's last kernel leaves sink_dev zeroed */
 	void* stage_hash = nullptr;          /* staged join build: materialised hashes */
 	unsigned long long* done = nullptr;  /* last-block counter */

@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--host-resident-only", action="store_true",
                     help="run only the query over host-resident columns, --steps times (for a profiler)")
+    ap.add_argument("--device-only", action="store_true",
+                    help="run only the query over device-resident columns, --steps times (for a profiler)")
     return ap.parse_args()
 
 
@@ -256,12 +258,33 @@ def run_host_resident_only(args):
     return 0
 
 
+def run_device_only(args):
+    """The workload's query over columns generated in HBM, run --steps times with no timing:
+    what a profiler captures for a kernel's counters."""
+    import torch
+
+    from vldb_voila_b200 import Engine, workload
+    w = workload(spec_of(args.workload))
+    eng = Engine(0)
+    eng.load_workload(w, on_device=True)
+    torch.cuda.synchronize()
+    q = eng.query(w.plan, args.flavor)
+    for _ in range(args.steps):
+        q.run()
+    res = q.result()
+    print(json.dumps({"workload": w.spec, "flavor": q.info()["flavor"], "steps": args.steps,
+                      "result_rows": int(len(res))}))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.host_resident_only:
         return run_host_resident_only(args)
+    if args.device_only:
+        return run_device_only(args)
 
     import numpy as np
     import torch
@@ -537,7 +560,8 @@ def run_config5(args):
     t0 = time.time()
     # learned chooser: trained on autotuner timings of separate seeded workloads
     train = ch.training_specs(int(os.environ.get("VC_TRAIN_N", "48")), seed=21, min_rows=100_000, max_rows=20_000_000)
-    records = [{"spec": s, "features": ch.features(s).tolist(), "times_ms": ch.autotune(s, reps=3)} for s in train]
+    reps = int(os.environ.get("VC_TUNE_REPS", "3"))
+    records = [{"spec": s, "features": ch.features(s).tolist(), "times_ms": ch.autotune(s, reps=reps)} for s in train]
     chooser = ch.Chooser()
     loss = chooser.fit(records)
     t_train = time.time() - t0
@@ -547,7 +571,7 @@ def run_config5(args):
         w = workload(s)
         e = Engine(0)
         e.load_workload(w, on_device=True)
-        times = ch.autotune(s, reps=3, engine=e)
+        times = ch.autotune(s, reps=reps, engine=e)
         best = min(times, key=times.get)
         pick = chooser.choose(s)
         records5.append({"spec": s, "best": best, "best_ms": times[best], "chosen": pick, "chosen_ms": times[pick],
@@ -574,6 +598,7 @@ def run_config5(args):
         evs[-1].synchronize()
         plain_ms.append(evs[0].elapsed_time(evs[-1]))
         plain_lat = [evs[0].elapsed_time(e) * 1000.0 for e in evs[1:]]
+        plain_each = [evs[i].elapsed_time(evs[i + 1]) for i in range(len(queries_tuned))]
     expect = [q.result_lines() for q in queries_tuned]
 
     # (b) one persistent kernel over all pipelines, learned flavors
@@ -581,7 +606,10 @@ def run_config5(args):
     # phase per table): a staged build becomes the automatic choice
     batch_flavors = [f.replace("build=staged", "build=auto") for f in learned]
     queries_learned = [e.query(workload(s).plan, f) for e, s, f in zip(engines, specs, batch_flavors)]
-    batch = Batch(queries_learned, threads=256, tiles_per_item=16)
+    # queries whose fact pipeline fills the GPU by itself run as their own launches after the
+    # persistent kernel (vc_batch_new_split), the rest inside it
+    solo_rows = int(float(os.environ.get("VC_BATCH_SOLO_ROWS", str(1 << 22))))
+    batch = Batch(queries_learned, threads=256, tiles_per_item=16, solo_rows=solo_rows)
     for _ in range(2):
         batch.run(stream)
         batch.wait()
@@ -611,6 +639,9 @@ def run_config5(args):
         "latency_us": {"batched_p50": p(batch_lat, 50), "batched_p99": p(batch_lat, 99),
                        "per_pipeline_p50": p(plain_lat, 50), "per_pipeline_p99": p(plain_lat, 99)},
         "results_identical": exact,
+        "solo_rows": solo_rows,
+        "per_pipeline_ms_by_template": {t: round(sum(ms for s, ms in zip(specs, plain_each) if s.startswith(t)), 3)
+                                        for t in sorted({s.split(":")[0] for s in specs})},
         "chooser": {"train_workloads": len(train), "train_loss": loss, "heldout_pipelines": len(records5),
                     "geomean_chosen_over_best": float(np.exp(np.mean(np.log(ratio)))),
                     "max_chosen_over_best": float(np.max(ratio)),

@@ -171,8 +171,10 @@ int vc_workload_batch(int count, uint64_t seed, int64_t min_rows, int64_t max_ro
  * (compiler.cpp:19-57, :343-385; codegen.cpp:371-376).
  * flavor: "" or "cuda(key=value,...)" with keys threads, rows, load=ldg|tma, stages,
  * prefetch, compact, frows (survivors per thread in a compaction flush, 1..16),
- * aggr=auto|dense|global|cache|part (part: partitioned group-by, histogram + scatter + one
- * shared-memory table per partition), parts (partitions of aggr=part, 16..2048), cache,
+ * aggr=auto|dense|global|cache|part|direct|dcache (part: partitioned group-by, histogram +
+ * scatter + one shared-memory table per partition; direct: a group table indexed by the packed
+ * key, no stored keys; dcache: the direct table behind the shared-memory cache), parts
+ * (partitions of aggr=part, 16..2048), cache,
  * lowcard=combine|atomic|private|redux|regs|packed, pgroups (groups per CTA of lowcard=private|regs|packed),
  * build=auto|direct|staged|dense, hash=mix|voila, fill, dense, sinksmem, gcap (group table
  * slots), ocap (result rows of an emitting plan), probe (1..32 lanes that probe one join key
@@ -271,6 +273,14 @@ int vc_join_aggr_noalloc(const int32_t* build_key, const int32_t* build_attr, in
  * use. */
 typedef struct vc_batch vc_batch;
 int vc_batch_new(vc_query** queries, int n, const char** flavors, int threads, int64_t tiles_per_item, vc_batch** out);
+/* vc_batch_new whose queries with a pipeline of at least solo_rows rows (0 = none) run as
+ * their own launches, with their own flavors' kernels, on the same stream right after the
+ * persistent kernel that runs the rest: a pipeline that fills the GPU by itself gains nothing
+ * from the batch's lean shared shapes.  vc_batch_info reports "batched" and "solo" counts;
+ * vc_batch_latencies gives a solo query the time from the batch's start to its end.  No
+ * counterpart in the reference, which runs queries one at a time. */
+int vc_batch_new_split(vc_query** queries, int n, const char** flavors, int threads, int64_t tiles_per_item,
+	int64_t solo_rows, vc_batch** out);
 int vc_batch_run(vc_batch* b, void* stream);
 /* Waits for the run; VC_ERR_TIMEOUT if a bounded dependency wait gave up. */
 int vc_batch_wait(vc_batch* b);

@@ -13,7 +13,8 @@ FLAVORS = ["", "cuda(load=tma,stages=2)", "cuda(lowcard=private,prefetch=0)", "c
            "cuda(build=direct,probe=8)", "cuda(aggr=part)", "cuda(aggr=part,parts=16,threads=128,rows=8)",
            "cuda(aggr=part,load=tma,stages=2,compact=0)", "cuda(frows=1)", "cuda(frows=8,compact=0,aggr=part)",
            "cuda(lowcard=regs)", "cuda(lowcard=regs,load=tma,stages=2,rows=8,pgroups=4)",
-           "cuda(aggr=direct)", "cuda(aggr=dcache,cache=256)"]
+           "cuda(aggr=direct)", "cuda(aggr=dcache,cache=256)", "cuda(lowcard=combine)",
+           "cuda(lowcard=packed,load=tma,stages=2,pgroups=3)"]
 
 
 def offline(spec):
@@ -106,6 +107,22 @@ def test_batch_module_compiles_and_dedups_shapes():
     assert "t += nitems" in src
     # block barriers are the non-aligned form: warps may arrive diverged after probe loops
     assert "__syncthreads" not in src and "vd::block_sync()" in src
+
+
+def test_split_batch_counts():
+    """vc_batch_new_split leaves queries whose largest pipeline reaches solo_rows out of the
+    persistent kernel."""
+    from vldb_voila_b200.engine import Batch
+    specs = ["sel_aggr:rows=1000", "sel_aggr:rows=200000", "groupby:rows=5000,keys=100", "star:rows=300000"]
+    engines, queries = [], []
+    for s in specs:
+        w, e = offline(s)
+        engines.append(e)
+        queries.append(e.query(w.plan))
+    info = Batch(queries, solo_rows=100000).info()
+    assert (info["queries"], info["batched"], info["solo"]) == (4, 2, 2)
+    assert Batch(queries).info()["solo"] == 0
+    assert Batch(queries, solo_rows=1).info()["work_items"] == 0
 
 
 def test_batch_work_queue_only_waits_on_earlier_items():

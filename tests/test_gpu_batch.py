@@ -46,6 +46,34 @@ def test_mixed_batch_matches_oracle_and_is_repeatable():
         assert q.result_lines() == e, s
 
 
+def test_split_batch_runs_large_queries_on_their_own():
+    """vc_batch_new_split: queries with a pipeline of at least solo_rows rows run as their own
+    launches after the persistent kernel; every query still gets the oracle's rows, over
+    repeated runs, and every query has a latency."""
+    specs = batch_specs(16, seed=6, min_rows=1_000, max_rows=300_000)
+    specs += ["groupby:rows=0,keys=10,seed=1"]
+    engines, queries, expect = _setup(specs)
+    rows = [workload(s).fact_rows for s in specs]
+    cut = sorted(rows)[len(rows) // 2]
+    b = Batch(queries, tiles_per_item=2, solo_rows=cut)
+    info = b.info()
+    assert info["solo"] >= 1 and info["batched"] >= 1 and info["solo"] + info["batched"] == len(specs)
+    for _ in range(2):
+        b.run()
+        b.wait()
+        for s, q, e in zip(specs, queries, expect):
+            assert q.result_lines() == e, s
+    lat = b.latencies_us()
+    assert len(lat) == len(specs) and all(x >= 0 for x in lat)
+    # every query on its own: the persistent kernel holds no work items
+    alone = Batch(queries, solo_rows=1)
+    assert alone.info()["batched"] == 0 and alone.info()["work_items"] == 0
+    alone.run()
+    alone.wait()
+    for s, q, e in zip(specs, queries, expect):
+        assert q.result_lines() == e, s
+
+
 def test_batch_with_per_query_flavors():
     specs = batch_specs(12, seed=4, min_rows=10_000, max_rows=200_000)
     choice = ["cuda(lowcard=private)", "cuda(aggr=cache,cache=128)", "cuda(prefetch=0,rows=2)", ""]

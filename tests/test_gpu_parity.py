@@ -21,7 +21,8 @@ FLAVORS = ["", "cuda(rows=8,threads=128,load=tma,stages=3)", "cuda(aggr=cache,ca
            "cuda(aggr=part,parts=16,threads=128,rows=8,load=tma,stages=2)", "cuda(frows=1)",
            "cuda(frows=8,compact=0,threads=128,rows=2)", "cuda(lowcard=regs)",
            "cuda(lowcard=regs,load=tma,stages=2,rows=8,pgroups=2,threads=128)", "cuda(lowcard=regs,rows=1,prefetch=0)",
-           "cuda(aggr=direct)", "cuda(aggr=dcache,cache=64,rows=8,threads=128)"]
+           "cuda(aggr=direct)", "cuda(aggr=dcache,cache=64,rows=8,threads=128)", "cuda(lowcard=combine)",
+           "cuda(lowcard=packed,load=tma,stages=2,pgroups=3,rows=2)"]
 
 
 def run_gpu(w, plan, flavor="", on_device=False, data=None):

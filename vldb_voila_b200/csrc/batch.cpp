@@ -28,6 +28,7 @@ namespace vc {
 
 int abi_guard_mlp(const std::function<void()>& f);
 void query_mark_external_run(Query& q, cudaStream_t s);
+void query_launch(Query& q, cudaStream_t stream);
 Query* vc_query_internal(vc_query* q);
 
 Batch::~Batch()
@@ -224,44 +225,95 @@ static void batch_run(Batch& b, cudaStream_t s)
 
 using namespace vc;
 
+/* A batch: the queries that run in the persistent kernel (b), and those whose largest
+ * pipeline has at least solo_rows rows, which run as their own launches (each with its own
+ * flavor's kernels: the persistent kernel's lean shapes would only slow a pipeline that fills
+ * the GPU by itself) on the same stream after it. */
 struct vc_batch {
 	Batch b;
+	bool has_batch = false;
+	std::vector<Query*> solo;
+	std::vector<int> slot;          /* per query: its index in b.queries, or -(solo index + 1) */
+	cudaEvent_t ev0 = nullptr;      /* before the batch's first launch */
+	std::vector<cudaEvent_t> ev;    /* after each solo query */
+	cudaStream_t stream = nullptr;  /* the stream of the last run */
+	bool offline = false;
+	~vc_batch()
+	{
+		if (offline) {
+			return;
+		}
+		if (ev0) {
+			cudaEventDestroy(ev0);
+		}
+		for (auto e : ev) {
+			cudaEventDestroy(e);
+		}
+	}
 };
 
 extern "C" {
 
-int vc_batch_new(vc_query** queries, int n, const char** flavors, int threads, int64_t tiles_per_item, vc_batch** out)
+static int64_t query_rows(const Query& q)
+{
+	int64_t r = 0;
+	for (const auto& p : q.plan.pipes) {
+		r = std::max(r, p.rows);
+	}
+	return r;
+}
+
+int vc_batch_new_split(vc_query** queries, int n, const char** flavors, int threads, int64_t tiles_per_item,
+	int64_t solo_rows, vc_batch** out)
 {
 	vc_batch* h = nullptr;
 	int rc = abi_guard_mlp([&] {
-		if (!queries || n < 1 || !out || threads < 32 || threads > 1024 || threads % 32 || tiles_per_item < 1) {
+		if (!queries || n < 1 || !out || threads < 32 || threads > 1024 || threads % 32 || tiles_per_item < 1 ||
+			solo_rows < 0) {
 			throw Error(VC_ERR_INVALID, "bad batch arguments");
 		}
 		h = new vc_batch();
 		std::vector<Flavor> fls;
+		Engine* eng = nullptr;
 		for (int i = 0; i < n; i++) {
 			if (!queries[i]) {
 				throw Error(VC_ERR_INVALID, "null query in batch");
 			}
 			Query* q = vc_query_internal(queries[i]);
-			if (h->b.eng && h->b.eng->device != q->eng->device) {
+			if (eng && eng->device != q->eng->device) {
 				throw Error(VC_ERR_INVALID, "batched queries must live on one device");
 			}
-			if (h->b.eng && h->b.eng->offline != q->eng->offline) {
+			if (eng && eng->offline != q->eng->offline) {
 				throw Error(VC_ERR_INVALID, "a batch cannot mix offline and device queries");
 			}
-			h->b.eng = q->eng;
+			eng = q->eng;
+			if (solo_rows > 0 && query_rows(*q) >= solo_rows) {
+				h->slot.push_back(-(int)h->solo.size() - 1);
+				h->solo.push_back(q);
+				continue;
+			}
+			h->slot.push_back((int)h->b.queries.size());
 			h->b.queries.push_back(q);
 			fls.push_back(flavors && flavors[i] ? Flavor::parse(flavors[i]) : q->flavor);
 		}
+		h->b.eng = eng;
+		h->offline = eng->offline;
 		h->b.flavor.threads = threads;
-		batch_prepare(h->b, fls, tiles_per_item);
+		h->has_batch = !h->b.queries.empty();
+		if (h->has_batch) {
+			batch_prepare(h->b, fls, tiles_per_item);
+		}
 		*out = h;
 	});
 	if (rc != VC_OK && h) {
 		delete h; /* the error message of the failed call stays in place */
 	}
 	return rc;
+}
+
+int vc_batch_new(vc_query** queries, int n, const char** flavors, int threads, int64_t tiles_per_item, vc_batch** out)
+{
+	return vc_batch_new_split(queries, n, flavors, threads, tiles_per_item, 0, out);
 }
 
 int vc_batch_run(vc_batch* h, void* stream)
@@ -273,7 +325,25 @@ int vc_batch_run(vc_batch* h, void* stream)
 		if (h->b.eng->offline) {
 			throw Error(VC_ERR_NO_DEVICE, "an offline engine only generates and compiles code");
 		}
-		batch_run(h->b, (cudaStream_t)stream);
+		VC_CHECK_CUDA(cudaSetDevice(h->b.eng->device));
+		h->stream = (cudaStream_t)stream;
+		if (!h->solo.empty()) {
+			if (!h->ev0) {
+				VC_CHECK_CUDA(cudaEventCreate(&h->ev0));
+				h->ev.assign(h->solo.size(), nullptr);
+				for (auto& e : h->ev) {
+					VC_CHECK_CUDA(cudaEventCreate(&e));
+				}
+			}
+			VC_CHECK_CUDA(cudaEventRecord(h->ev0, h->stream));
+		}
+		if (h->has_batch) {
+			batch_run(h->b, h->stream);
+		}
+		for (size_t k = 0; k < h->solo.size(); k++) {
+			query_launch(*h->solo[k], h->stream);
+			VC_CHECK_CUDA(cudaEventRecord(h->ev[k], h->stream));
+		}
 	});
 }
 
@@ -285,7 +355,10 @@ int vc_batch_wait(vc_batch* h)
 		}
 		Batch& b = h->b;
 		VC_CHECK_CUDA(cudaSetDevice(b.eng->device));
-		VC_CHECK_CUDA(cudaStreamSynchronize(b.stream));
+		VC_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+		if (!h->has_batch) {
+			return;
+		}
 		unsigned err = 0;
 		VC_CHECK_CUDA(cudaMemcpy(&err, b.err, sizeof(err), cudaMemcpyDeviceToHost));
 		if (err) {
@@ -306,17 +379,30 @@ int vc_batch_wait(vc_batch* h)
 int vc_batch_latencies(vc_batch* h, double* us, int n)
 {
 	return abi_guard_mlp([&] {
-		if (!h || !us || n < (int)h->b.queries.size()) {
+		if (!h || !us || n < (int)h->slot.size()) {
 			throw Error(VC_ERR_INVALID, "bad arguments");
 		}
 		Batch& b = h->b;
-		std::vector<unsigned long long> f(b.queries.size() + 1);
 		VC_CHECK_CUDA(cudaSetDevice(b.eng->device));
-		VC_CHECK_CUDA(cudaStreamSynchronize(b.stream));
-		VC_CHECK_CUDA(cudaMemcpy(f.data(), b.finish, sizeof(unsigned long long) * f.size(), cudaMemcpyDeviceToHost));
+		VC_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+		std::vector<unsigned long long> f(b.queries.size() + 1, 0ull);
+		if (h->has_batch) {
+			VC_CHECK_CUDA(cudaMemcpy(f.data(), b.finish, sizeof(unsigned long long) * f.size(), cudaMemcpyDeviceToHost));
+		}
 		const unsigned long long start = f.back();
-		for (size_t i = 0; i < b.queries.size(); i++) {
-			us[i] = f[i] >= start ? (double)(f[i] - start) / 1000.0 : -1.0;
+		for (size_t i = 0; i < h->slot.size(); i++) {
+			const int k = h->slot[i];
+			if (k >= 0) {
+				/* the persistent kernel's clock from its start */
+				us[i] = f[(size_t)k] >= start ? (double)(f[(size_t)k] - start) / 1000.0 : -1.0;
+			} else {
+				/* events from the batch's first launch to the solo query's end */
+				float ms = -1.0f;
+				if (h->ev0 && cudaEventElapsedTime(&ms, h->ev0, h->ev[(size_t)(-k - 1)]) != cudaSuccess) {
+					ms = -1.0f;
+				}
+				us[i] = ms >= 0.0f ? (double)ms * 1000.0 : -1.0;
+			}
 		}
 	});
 }
@@ -329,7 +415,8 @@ int vc_batch_info(vc_batch* h, char* buf, size_t cap, size_t* len)
 		}
 		Batch& b = h->b;
 		std::ostringstream o;
-		o << "{\"queries\": " << b.queries.size() << ", \"work_items\": " << b.nitems << ", \"grid\": " << b.grid
+		o << "{\"queries\": " << h->slot.size() << ", \"batched\": " << b.queries.size() << ", \"solo\": "
+		  << h->solo.size() << ", \"work_items\": " << b.nitems << ", \"grid\": " << b.grid
 		  << ", \"threads\": " << b.flavor.threads << ", \"smem\": " << b.smem << ", \"regs\": " << b.regs
 		  << ", \"occupancy\": " << b.occupancy
 		  << ", \"source_bytes\": " << b.source.size() << "}";

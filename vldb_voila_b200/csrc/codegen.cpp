@@ -314,27 +314,34 @@ struct PipeGen {
 		return (int)used.size();
 	}
 
-	/* lowcard=regs: the flush interval (the most tiles whose packed fields take no more
-	 * words than those of a single tile, at least two) and the field layout */
+	/* lowcard=regs|packed: the flush interval F (tiles) and the field layout.  Per row, a
+	 * thread adds its words: about 2.5 instructions per word and code under regs (every code's
+	 * words, under a select), about 5 per word under packed (a shared-memory read-modify-write
+	 * at the row's code); a warp's flush costs about 46 instructions per code and covers F·rows
+	 * rows of each lane.  F minimises the sum (wider fields, more words, fewer flushes). */
 	bool plan_regs() {
 		std::vector<int> w, s, b;
-		const int w1 = regs_pack(V, w, s, b);
-		if (w1 == 0) {
-			return false;
-		}
-		const int limit = std::max(w1, 2);
-		for (int F = 16; F >= 1; F >>= 1) {
-			const int wf = regs_pack((int64_t)F * V, w, s, b);
-			if (wf != 0 && wf <= limit) {
+		double best = 1e30;
+		bool found = false;
+		for (int F = 1; F <= 64; F <<= 1) {
+			const int64_t R = (int64_t)F * V;
+			const int wf = regs_pack(R, w, s, b);
+			/* regs: at most 16 words (32 registers) of accumulators per thread */
+			if (wf == 0 || (!regs_smem && kGmax * wf > 16)) {
+				continue;
+			}
+			const double per_row = (regs_smem ? 5.0 * wf : 2.5 * kGmax * wf) + 46.0 * kGmax / (double)R;
+			if (per_row < best) {
+				best = per_row;
+				found = true;
 				regs_tiles = F;
 				regs_words = wf;
 				rg_word = w;
 				rg_shift = s;
 				rg_bits = b;
-				return kGmax * regs_words <= 48;
 			}
 		}
-		return false;
+		return found;
 	}
 
 	int row_bits(int a) const {
@@ -658,7 +665,90 @@ struct PipeGen {
 		return off;
 	}
 
+	/* The ring without block barriers, for bodies with no block-wide collectives: each stage
+	 * has a full barrier (the bulk copies' bytes) and an empty barrier that every warp arrives
+	 * on once it has read the stage; thread 0 refills the stage of the previous tile as soon as
+	 * all warps have left it, so warps drift apart by up to the ring's depth instead of
+	 * meeting at a barrier after every tile.  A wait that runs out sets the error word and
+	 * the block's abort flag; each warp leaves the loop at its next tile (a warp-uniform
+	 * vote), and thread 0 waits, bounded, for the copies still in flight. */
+	void gen_tma_ring_decoupled() {
+		const int S = fl.stages;
+		const int NW = T / 32;
+		const size_t tile_bytes = tile_region(p.cols.size());
+		size_t base = (smem_sink + 127) & ~(size_t)127;
+		const size_t bar_off = base + (size_t)S * tile_bytes;
+		smem_total = bar_off + 16 * (size_t)S;
+		o << "  unsigned char* const stages = vd_smem + " << base << ";\n";
+		o << "  uint64_t* const full = (uint64_t*)(vd_smem + " << bar_off << ");\n";
+		o << "  uint64_t* const empty = full + " << S << ";\n";
+		o << "  __shared__ int tma_abort;\n";
+		o << "  const int64_t nfull = n / tile;\n";
+		o << "  const int64_t nmine = nfull > (int64_t)blockIdx.x ? (nfull - (int64_t)blockIdx.x + (int64_t)gridDim.x - 1) / "
+		     "(int64_t)gridDim.x : 0;\n";
+		o << "  if (threadIdx.x == 0) {\n";
+		o << "    for (int s = 0; s < " << S << "; s++) { vd::mbar_init(&full[s], 1); vd::mbar_init(&empty[s], " << NW << "); }\n";
+		o << "    vd::mbar_init_fence();\n    tma_abort = 0;\n";
+		o << "  }\n  vd::block_sync();\n";
+		o << "  auto issue = [&](int64_t j) {\n";
+		o << "    const int64_t tj = (int64_t)blockIdx.x + j * (int64_t)gridDim.x;\n";
+		o << "    const int s = (int)(j % " << S << ");\n";
+		o << "    unsigned char* dst = stages + (size_t)s * " << tile_bytes << ";\n";
+		o << "    vd::mbar_expect_tx(&full[s], " << tile_bytes_tx() << ");\n";
+		for (size_t c = 0; c < p.cols.size(); c++) {
+			if (!eager[c]) {
+				continue;
+			}
+			const int tb = type_bytes(p.cols[c].type);
+			o << "    vd::bulk_load(dst + " << tile_region(c) << ", c" << c << " + tj * tile, " << (size_t)T * V * tb
+			  << "u, &full[s]);\n";
+		}
+		o << "  };\n";
+		o << "  int64_t issued = 0;\n";
+		o << "  if (threadIdx.x == 0) {\n";
+		o << "    vd::fence_proxy_async();\n";
+		o << "    for (; issued < " << S << " && issued < nmine; issued++) { issue(issued); }\n";
+		o << "  }\n";
+		o << "  int64_t i = 0;\n";
+		o << "  for (; i < nmine; i++) {\n";
+		o << "    if (threadIdx.x == 0 && i >= 1 && issued < nmine) {\n";
+		o << "      const int64_t r = i - 1;\n";
+		o << "      if (vd::mbar_wait(&empty[r % " << S << "], (uint32_t)((r / " << S << ") & 1))) {\n";
+		o << "        vd::fence_proxy_async();\n        issue(issued);\n        issued++;\n";
+		o << "      } else {\n        atomicOr(err, VD_ERR_WAIT_TIMEOUT);\n        *(volatile int*)&tma_abort = 1;\n      }\n";
+		o << "    }\n";
+		o << "    const int s = (int)(i % " << S << ");\n";
+		o << "    const bool ok = vd::mbar_wait(&full[s], (uint32_t)((i / " << S << ") & 1));\n";
+		o << "    if (!ok) { atomicOr(err, VD_ERR_WAIT_TIMEOUT); *(volatile int*)&tma_abort = 1; }\n";
+		o << "    if (__any_sync(0xffffffffu, !ok || *(volatile int*)&tma_abort != 0)) { break; }\n";
+		o << "    const int64_t t = (int64_t)blockIdx.x + i * (int64_t)gridDim.x;\n";
+		o << "    const unsigned char* stage = stages + (size_t)s * " << tile_bytes << ";\n";
+		emit_body("smem");
+		o << "    __syncwarp();\n";
+		o << "    if (vd::lane_id() == 0u) { vd::mbar_arrive(&empty[s]); }\n";
+		o << "  }\n";
+		/* after an abort: the copies issued but not consumed by thread 0's warp */
+		o << "  if (threadIdx.x == 0) {\n";
+		o << "    for (int64_t j = i; j < issued; j++) {\n";
+		o << "      vd::mbar_wait(&full[j % " << S << "], (uint32_t)((j / " << S << ") & 1), 100000000ull);\n";
+		o << "    }\n  }\n";
+		o << "  vd::block_sync();\n";
+		o << "  if (nfull < ntiles && (int64_t)blockIdx.x == nfull % (int64_t)gridDim.x) {\n";
+		o << "    const int64_t t = nfull;\n";
+		emit_body("ldg");
+		o << "  }\n";
+	}
+
+	/* the body has no block barriers or block-wide votes (warp-level work only) */
+	bool body_warp_only() const {
+		return !sink_block_collective() && (compact_at < 0 || warp_compact());
+	}
+
 	void gen_tma_loop() {
+		if (body_warp_only()) {
+			gen_tma_ring_decoupled();
+			return;
+		}
 		const int S = fl.stages;
 		const size_t tile_bytes = tile_region(p.cols.size());
 		size_t base = (smem_sink + 127) & ~(size_t)127;
@@ -1487,11 +1577,18 @@ struct PipeGen {
 		case Sink::AggDense: {
 			o << "#pragma unroll\n    for (int v = 0; v < " << V << "; v++) {\n";
 			std::string slot = "0";
+			/* a slot array in shared memory has fewer than 2^31 slots: 32-bit index arithmetic */
+			const bool slot32 = dense_in_smem;
 			for (size_t k = 0; k < s.keys.size(); k++) {
-				slot += " + (" + expr(s.keys[k], "v") + " - " + P((unsigned long long)(int64_t)s.keys[k]->b.lo) +
-					") * " + P((unsigned long long)s.key_radix[k]);
+				if (slot32) {
+					slot += " + (int)(" + expr(s.keys[k], "v") + " - " + P((unsigned long long)(int64_t)s.keys[k]->b.lo) +
+						") * (int)" + P((unsigned long long)s.key_radix[k]);
+				} else {
+					slot += " + (" + expr(s.keys[k], "v") + " - " + P((unsigned long long)(int64_t)s.keys[k]->b.lo) +
+						") * " + P((unsigned long long)s.key_radix[k]);
+				}
 			}
-			o << "      const int64_t slot = act[v] ? (" << slot << ") : 0;\n";
+			o << "      const int64_t slot = act[v] ? (int64_t)(" << slot << ") : 0;\n";
 			o << "      " << agg_vals("v") << "\n";
 			if (regs_acc) {
 				o << "      const int code = act[v] ? vd::dict_code(pdict, pcodes, pncodes, slot, " << kGmax << ") : -2;\n";
@@ -2172,9 +2269,7 @@ struct PipeGen {
 		k << "  unsigned long long* const gacc = " << Pptr(st.sink_acc, "unsigned long long*") << ";\n";
 		k << "  const int64_t nslots = " << P((unsigned long long)st.sink_cap) << ";\n";
 		/* a block takes chunks of blockDim.x * kExtractK slots (slot q * blockDim.x + thread of
-		 * the chunk); all keys of a chunk are loaded (from L2, coherent) before any is used, and
-		 * the chunk's result rows are reserved with one atomic */
-		k << "  __shared__ unsigned long long xres[33];\n";
+		 * the chunk); all keys of a chunk are loaded (from L2, coherent) before any is used */
 		k << "  const int64_t chunk = (int64_t)blockDim.x * " << kExtractK << ";\n";
 		if (item) {
 			/* one item = chunks [t_begin, t_end) */
@@ -2195,19 +2290,28 @@ struct PipeGen {
 		}
 		k << "    }\n";
 		k << "    uint64_t w[" << kExtractK << "][" << W << "];\n";
-		k << "    bool take[" << kExtractK << "];\n    int ntake = 0;\n";
+		k << "    bool take[" << kExtractK << "];\n";
 		auto field = [&](int a) {
 			const int bits = s.agg_bits[a];
 			const unsigned long long mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
 			return "((w[q][" + std::to_string(s.agg_word[a]) + "] >> " + std::to_string(s.agg_shift[a]) + ") & " +
 				std::to_string(mask) + "ull)";
 		};
+		/* every word of the chunk is loaded before any slot is cleared (the clears would
+		 * otherwise order each load after the previous slot's stores) */
 		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
 		k << "      const int64_t i = cb + (int64_t)q * blockDim.x + threadIdx.x;\n";
 		k << "#pragma unroll\n      for (int a = 0; a < " << W << "; a++) { w[q][a] = kw[q] != 0 ? __ldcg(&gacc[i * " << W
 		  << " + a]) : 0ull; }\n";
+		k << "    }\n";
+		/* each warp reserves its rows with one atomic; for every q the lanes' rows are
+		 * consecutive (ballot order), so the result columns are written coalesced */
+		k << "    unsigned bal[" << kExtractK << "];\n    int wtot = 0;\n";
+		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
+		k << "      const int64_t i = cb + (int64_t)q * blockDim.x + threadIdx.x;\n";
 		k << "      take[q] = kw[q] != 0 && (int64_t)" << field(s.count_idx) << " > 0;\n";
-		k << "      ntake += take[q] ? 1 : 0;\n";
+		k << "      bal[q] = __ballot_sync(0xffffffffu, take[q]);\n";
+		k << "      wtot += __popc(bal[q]);\n";
 		if (gdirect()) {
 			/* a used slot has a non-zero count */
 			k << "      if (take[q]) {\n";
@@ -2216,10 +2320,14 @@ struct PipeGen {
 		}
 		k << "#pragma unroll\n        for (int a = 0; a < " << W << "; a++) { gacc[i * " << W << " + a] = 0ull; }\n      }\n";
 		k << "    }\n";
-		k << "    int64_t pos = vd::block_reserve(ocount, ntake, xres);\n";
+		k << "    unsigned long long wbase = 0ull;\n";
+		k << "    if (vd::lane_id() == 0u && wtot > 0) { wbase = atomicAdd(ocount, (unsigned long long)wtot); }\n";
+		k << "    wbase = __shfl_sync(0xffffffffu, wbase, 0);\n";
+		k << "    int64_t woff = 0;\n";
 		k << "#pragma unroll\n    for (int q = 0; q < " << kExtractK << "; q++) {\n";
-		k << "    if (take[q]) {\n";
-		k << "    if (pos < ocap) {\n";
+		k << "    const int64_t pos = (int64_t)wbase + woff + __popc(bal[q] & vd::lanemask_lt());\n";
+		k << "    woff += __popc(bal[q]);\n";
+		k << "    if (take[q] && pos < ocap) {\n";
 		k << "      const int64_t cnt = (int64_t)" << field(s.count_idx) << ";\n";
 		int col = 0;
 		for (size_t kk = 0; kk < s.keys.size(); kk++, col++) {
@@ -2242,7 +2350,7 @@ struct PipeGen {
 			}
 			col++;
 		}
-		k << "    }\n    pos++;\n    }\n    }\n  }\n}\n\n";
+		k << "    }\n    }\n  }\n}\n\n";
 		return k.str();
 	}
 };

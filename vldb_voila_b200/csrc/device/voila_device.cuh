@@ -240,6 +240,12 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
 }
 
 /* generic-proxy reads of a stage are ordered before the async-proxy refill of it */
+/* One arrival on the barrier (no transaction bytes). */
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 __device__ __forceinline__ void fence_proxy_async()
 {
 	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -242,12 +242,14 @@ struct Flavor {
 	std::string build = "auto"; /* join build: auto | direct | staged | dense */
 	bool prefetch = true;     /* ldg: load the next tile while the current one is processed */
 	int compact = -2;         /* compact survivors after op k (-1 never, -2 auto) */
-	std::string lowcard = "combine"; /* dense aggregation: combine (warp pre-sum by shuffles) | atomic (per-warp
+	std::string lowcard = "packed";  /* dense aggregation: combine (warp pre-sum by shuffles) | atomic (per-warp
 	                                  * replicas) | private (per-thread accumulators behind a block dictionary)
 	                                  * | redux (warp pre-sum by redux.sync into per-warp replicas) | regs
 	                                  * (per-thread packed register accumulators behind a block dictionary,
 	                                  * folded per warp every few tiles) | packed (the same packed words in
-	                                  * shared memory, one column per thread) */
+	                                  * shared memory, one column per thread); regs and packed run as
+	                                  * combine where they do not apply (survivor compaction, joinN loops,
+	                                  * batches, slots in global memory) */
 	std::string hash = "mix"; /* table positions: mix (finalizer of the packed key) | voila (runtime.hpp hash) */
 	int fill = 50;            /* largest load factor (percent) of group tables */
 	int64_t direct_limit = 64ll << 20; /* auto: direct when the upper-bound table fits this many bytes */

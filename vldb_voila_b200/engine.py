@@ -89,6 +89,8 @@ def lib():
                                    c.POINTER(c.c_float)]),
         "vc_mlp_predict": (c.c_int, [P, P, c.c_int, P]),
         "vc_batch_new": (c.c_int, [c.POINTER(P), c.c_int, c.POINTER(c.c_char_p), c.c_int, c.c_int64, c.POINTER(P)]),
+        "vc_batch_new_split": (c.c_int, [c.POINTER(P), c.c_int, c.POINTER(c.c_char_p), c.c_int, c.c_int64, c.c_int64,
+                                         c.POINTER(P)]),
         "vc_batch_run": (c.c_int, [P, P]),
         "vc_batch_wait": (c.c_int, [P]),
         "vc_batch_latencies": (c.c_int, [P, c.POINTER(c.c_double), c.c_int]),
@@ -468,16 +470,19 @@ class Query:
 
 
 class Batch:
-    """Many queries in one persistent kernel (vc_batch_*); the queries keep their results."""
+    """Many queries in one persistent kernel (vc_batch_*); the queries keep their results.
+    Queries with a pipeline of at least `solo_rows` rows (0 = none) run as their own launches
+    right after the persistent kernel (vc_batch_new_split)."""
 
-    def __init__(self, queries, flavors=None, threads=256, tiles_per_item=64):
+    def __init__(self, queries, flavors=None, threads=256, tiles_per_item=64, solo_rows=0):
         self.queries = list(queries)  # the queries must outlive the batch
         arr = (ctypes.c_void_p * len(self.queries))(*[q._h.value for q in self.queries])
         fl = None
         if flavors is not None:
             fl = (ctypes.c_char_p * len(self.queries))(*[_b(f) if f else None for f in flavors])
         h = ctypes.c_void_p()
-        check(lib().vc_batch_new(arr, len(self.queries), fl, threads, tiles_per_item, ctypes.byref(h)))
+        check(lib().vc_batch_new_split(arr, len(self.queries), fl, threads, tiles_per_item, int(solo_rows),
+                                       ctypes.byref(h)))
         self._h = h
 
     def close(self):

@@ -326,8 +326,9 @@ struct PipeGen {
 		for (int F = 1; F <= 64; F <<= 1) {
 			const int64_t R = (int64_t)F * V;
 			const int wf = regs_pack(R, w, s, b);
-			/* regs: at most 16 words (32 registers) of accumulators per thread */
-			if (wf == 0 || (!regs_smem && kGmax * wf > 16)) {
+			/* regs: at most 16 words (32 registers) of accumulators per thread; packed: at most
+			 * 64 KiB of shared memory per CTA */
+			if (wf == 0 || (!regs_smem && kGmax * wf > 16) || (regs_smem && (size_t)kGmax * wf * T * 8 > 64 * 1024)) {
 				continue;
 			}
 			const double per_row = (regs_smem ? 5.0 * wf : 2.5 * kGmax * wf) + 46.0 * kGmax / (double)R;

@@ -558,12 +558,19 @@ def run_config5(args):
     max_rows = int(float(os.environ.get("VC_BATCH_MAX_ROWS", "60000000")))
     specs = batch_specs(n, 5, 10_000, max_rows)
     t0 = time.time()
-    # learned chooser: trained on autotuner timings of separate seeded workloads
-    train = ch.training_specs(int(os.environ.get("VC_TRAIN_N", "48")), seed=21, min_rows=100_000, max_rows=20_000_000)
+    # VC_CONFIG5_FLAVORS=default: both arms run the default flavor (no tuning, no chooser), which
+    # isolates batching from flavor choice
+    tune = os.environ.get("VC_CONFIG5_FLAVORS", "tuned") != "default"
     reps = int(os.environ.get("VC_TUNE_REPS", "3"))
-    records = [{"spec": s, "features": ch.features(s).tolist(), "times_ms": ch.autotune(s, reps=reps)} for s in train]
-    chooser = ch.Chooser()
-    loss = chooser.fit(records)
+    train, loss, chooser = [], None, None
+    if tune:
+        # learned chooser: trained on autotuner timings of separate seeded workloads
+        train = ch.training_specs(int(os.environ.get("VC_TRAIN_N", "48")), seed=21, min_rows=100_000,
+                                  max_rows=20_000_000)
+        records = [{"spec": s, "features": ch.features(s).tolist(), "times_ms": ch.autotune(s, reps=reps)}
+                   for s in train]
+        chooser = ch.Chooser()
+        loss = chooser.fit(records)
     t_train = time.time() - t0
 
     engines, queries_tuned, tuned, learned, records5 = [], [], [], [], []
@@ -571,11 +578,14 @@ def run_config5(args):
         w = workload(s)
         e = Engine(0)
         e.load_workload(w, on_device=True)
-        times = ch.autotune(s, reps=reps, engine=e)
-        best = min(times, key=times.get)
-        pick = chooser.choose(s)
-        records5.append({"spec": s, "best": best, "best_ms": times[best], "chosen": pick, "chosen_ms": times[pick],
-                         "default_ms": times[ch.DEFAULT]})
+        if tune:
+            times = ch.autotune(s, reps=reps, engine=e)
+            best = min(times, key=times.get)
+            pick = chooser.choose(s)
+            records5.append({"spec": s, "best": best, "best_ms": times[best], "chosen": pick,
+                             "chosen_ms": times[pick], "default_ms": times[ch.DEFAULT]})
+        else:
+            best = pick = ch.DEFAULT
         tuned.append(best)
         learned.append(pick)
         engines.append(e)
@@ -609,21 +619,34 @@ def run_config5(args):
     # queries whose fact pipeline fills the GPU by itself run as their own launches after the
     # persistent kernel (vc_batch_new_split), the rest inside it
     solo_rows = int(float(os.environ.get("VC_BATCH_SOLO_ROWS", str(1 << 22))))
+
+    def time_batch(bt):
+        for _ in range(2):
+            bt.run(stream)
+            bt.wait()
+        ms_list, lat = [], []
+        for rep in range(args.steps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            bt.run(stream)
+            b.record(stream)
+            bt.wait()
+            ms_list.append(a.elapsed_time(b))
+            lat = bt.latencies_us()
+        return ms_list, lat, all(q.result_lines() == e for q, e in zip(queries_learned, expect))
+
     batch = Batch(queries_learned, threads=256, tiles_per_item=16, solo_rows=solo_rows)
-    for _ in range(2):
-        batch.run(stream)
-        batch.wait()
-    batch_ms, batch_lat = [], []
-    for rep in range(args.steps):
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        batch.run(stream)
-        b.record(stream)
-        batch.wait()
-        batch_ms.append(a.elapsed_time(b))
-        batch_lat = batch.latencies_us()
-    exact = all(q.result_lines() == e for q, e in zip(queries_learned, expect))
+    batch_ms, batch_lat, exact = time_batch(batch)
+    unsplit = None
+    if solo_rows > 0:
+        # the same queries all inside the persistent kernel, for comparison
+        batch0 = Batch(queries_learned, threads=256, tiles_per_item=16)
+        ms0, _, exact0 = time_batch(batch0)
+        unsplit = {"batched_ms": statistics.median(ms0), "results_identical": exact0,
+                   "value": statistics.median(plain_ms) / statistics.median(ms0)}
+        exact = exact and exact0
+        batch0.close()
 
     ratio = [r["chosen_ms"] / r["best_ms"] for r in records5]
     rows = sum(workload(s).fact_rows for s in specs)
@@ -642,13 +665,15 @@ def run_config5(args):
         "solo_rows": solo_rows,
         "per_pipeline_ms_by_template": {t: round(sum(ms for s, ms in zip(specs, plain_each) if s.startswith(t)), 3)
                                         for t in sorted({s.split(":")[0] for s in specs})},
+        "flavors": "per-pipeline arm: exhaustively tuned; batch: learned" if tune else "default flavor in both arms",
+        "all_in_one_kernel": unsplit,
         "chooser": {"train_workloads": len(train), "train_loss": loss, "heldout_pipelines": len(records5),
                     "geomean_chosen_over_best": float(np.exp(np.mean(np.log(ratio)))),
                     "max_chosen_over_best": float(np.max(ratio)),
                     "within_10pct_fraction": float(np.mean([r <= 1.10 for r in ratio])),
                     "sum_chosen_ms": sum(r["chosen_ms"] for r in records5),
                     "sum_best_ms": sum(r["best_ms"] for r in records5),
-                    "sum_default_ms": sum(r["default_ms"] for r in records5)},
+                    "sum_default_ms": sum(r["default_ms"] for r in records5)} if records5 else None,
         "setup_s": {"train": round(t_train, 1), "tune": round(t_tune, 1)},
     }
     print(json.dumps(line))

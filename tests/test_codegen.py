@@ -353,3 +353,51 @@ def test_batched_partitioned_aggregation_uses_a_group_table():
     b = Batch([q])
     src = b.source()
     assert "gt_find_or_insert" in src and "scur" not in src
+
+
+def test_direct_group_table_plan():
+    """aggr=auto over a key space no larger than the hash table: the accumulator words are indexed
+    by the packed key (no stored keys, no probes) behind the shared-memory cache; aggr=direct drops
+    the cache; a key space of 2^28 slots and more keeps the hash table."""
+    w, e = offline("groupby:rows=6000000,keys=1500000,zipf=0,seed=3")
+    auto = e.query(w.plan).source()
+    assert "gt_add<2>(gacc, (int64_t)pk, w)" in auto and "gt_cache_add" in auto
+    assert "gt_find_or_insert" not in auto and "gkeys" not in auto
+    direct = e.query(w.plan, "cuda(aggr=direct)").source()
+    assert "gt_cache_add" not in direct and "gt_add<2>(gacc, (int64_t)pk, w)" in direct
+    # the extraction loads every word of its chunk before clearing any slot, and reserves rows per warp
+    ext = direct[direct.index("_extract("):]
+    assert ext.index("__ldcg(&gacc[") < ext.index("= 0ull; }") and "__ballot_sync" in ext
+    wide = ("(aggr hash ((col k)) ((fun count)) (project ((assign k (fun * (col lineitem.l_orderkey) "
+            "(const 1000)))) (scan lineitem (l_orderkey))))")
+    w2, e2 = offline("groupby:rows=100000,keys=1000000,zipf=0,seed=3")
+    assert "gt_find_or_insert" in e2.query(wide, "cuda(aggr=direct)").source()
+
+
+def test_packed_low_cardinality_accumulators():
+    """lowcard=packed (the default): per-thread packed words per block-dictionary code in shared
+    memory, folded per warp by redux.sync; it falls back to warp pre-combining where its words
+    would take more than 64 KiB per CTA, and under survivor compaction (the star chain)."""
+    w, e = offline("sel_aggr:rows=6000000,seed=1")
+    src = e.query(w.plan).source()
+    assert "racc(code, 0) +=" in src and "rflush();" in src and "vd::group_sum_u<" in src
+    assert "warp_combine" not in src
+    assert "warp_combine" in e.query(w.plan, "cuda(threads=1024)").source()
+    regs = e.query(w.plan, "cuda(lowcard=regs)").source()
+    assert "racc_r[" in regs and "code == k ?" in regs
+    ws, es = offline("star:rows=100000")
+    assert "racc(" not in es.query(ws.plan).source()
+
+
+def test_tma_ring_without_block_barriers():
+    """load=tma: a warp-only body (no block collectives) takes the ring with per-stage empty
+    barriers that every warp arrives on; an appending sink keeps the ring with a block barrier
+    per tile."""
+    w, e = offline("sel_aggr:rows=100000")
+    src = e.query(w.plan, "cuda(load=tma,stages=3)").source()
+    assert "vd::mbar_arrive(&empty[s])" in src and "vd::mbar_init(&empty[s], 8)" in src
+    assert "__any_sync(0xffffffffu, !ok" in src
+    emit = ("(select (fun <= (col lineitem.l_shipdate) (const 9000)) "
+            "(scan lineitem (l_shipdate l_quantity)))")
+    src2 = e.query(emit, "cuda(load=tma,stages=2)").source()
+    assert "empty[" not in src2 and "vd::block_any(!ok)" in src2

@@ -1433,9 +1433,10 @@ struct PipeGen {
 				  << " + threadIdx.x] = 0; }\n";
 				o << "  vd::block_sync();\n";
 			}
-			/* per-thread register accumulators: packed words for up to kGmax slots (codes of the
-			 * block's dictionary), summed over regs_tiles tiles, then folded per warp by
-			 * redux.sync into the block's slot array */
+			/* per-thread packed accumulator words (registers for regs, a shared-memory column
+			 * per thread for packed) for up to kGmax slots (codes of the block's dictionary),
+			 * summed over regs_tiles tiles, then folded per warp by redux.sync into the block's
+			 * slot array */
 			regs_smem = fl.lowcard == "packed";
 			regs_acc = (fl.lowcard == "regs" || regs_smem) && dense_in_smem && replicas == 1 && !item && compact_at < 0 &&
 				A() <= 32 &&

@@ -1,0 +1,119 @@
+"""The oracle against the reference itself on seeded random plans (selections, projections,
+hash, global and emitting roots over the lineitem-shaped table): each plan runs through the
+reference's vectorwise flavor, built from its sources by oracle/ref/Makefile, and through the
+oracle, and the sorted result lines must be identical.  CPU only; skipped where the reference
+build or its source tree is absent."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle.voila_oracle import result_lines, run_plan
+from vldb_voila_b200 import generate_workload_host, workload
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.environ.get("VOILA_REFERENCE", "/root/reference")
+RDIR = os.path.join(REPO, "oracle", "_ref", "avx512")
+SPEC = "sel_aggr:rows=20000,seed=81"
+N_PLANS = 16
+
+# the workload's columns and their value ranges (sel_aggr generator)
+COLS = {"l_quantity": (1, 50), "l_extendedprice": (90000, 10500000), "l_discount": (0, 10), "l_tax": (0, 8),
+        "l_returnflag": (65, 82), "l_linestatus": (70, 79), "l_shipdate": (2448623, 2451148)}
+SMALL = ["l_quantity", "l_discount", "l_tax", "l_returnflag", "l_linestatus"]
+# the flag columns' values ({A,N,R}, {F,O}): equality constants mostly hit one of them
+FLAGS = {"l_returnflag": [65, 78, 82], "l_linestatus": [70, 79]}
+
+
+def _have_reference():
+    if not (os.path.isdir(REF) and os.path.exists(os.path.join(RDIR, "ref_gen"))):
+        return False
+    with open("/proc/cpuinfo") as f:
+        return "avx512f" in f.read()
+
+
+def _col(name):
+    return f"(col lineitem.{name})" if name in COLS else f"(col {name})"
+
+
+def _predicate(rng):
+    parts = []
+    for _ in range(int(rng.integers(1, 4))):
+        c = str(rng.choice(list(COLS)))
+        lo, hi = COLS[c]
+        op = str(rng.choice(["<", "<=", ">", ">=", "=", "!="]))
+        v = int(rng.integers(lo, hi + 1))
+        if c in FLAGS and rng.random() < 0.8:
+            v = int(rng.choice(FLAGS[c]))
+        parts.append(f"(fun {op} {_col(c)} (const {v}))")
+    expr = parts[0]
+    for p in parts[1:]:
+        expr = f"(fun {rng.choice(['and', 'or'])} {expr} {p})"
+    return expr
+
+
+def _derived(rng):
+    """One projected column: its plan expression and whether its range is small enough for a key."""
+    k = int(rng.integers(1, 30))
+    choices = [
+        (f"(fun - (col lineitem.l_extendedprice) (fun * (col lineitem.l_quantity) (const {k * 1000})))", False),
+        ("(fun * (col lineitem.l_quantity) (col lineitem.l_discount))", True),
+        (f"(fun + (col lineitem.l_tax) (const {k}))", True),
+        (f"(fun - (const {k}) (col lineitem.l_discount))", True),
+    ]
+    return choices[int(rng.integers(0, len(choices)))]
+
+
+def random_plan(seed):
+    rng = np.random.default_rng(seed)
+    scan = "(scan lineitem (" + " ".join(COLS) + "))"
+    src = f"(select {_predicate(rng)} {scan})" if rng.random() < 0.8 else scan
+    kind = str(rng.choice(["hash", "hash", "global", "emit"]))
+    if kind == "emit":
+        return f"(select {_predicate(rng)} {scan})"
+    dexpr, dsmall = _derived(rng)
+    proj = "(project ((assign x1 " + dexpr + ") " + " ".join(_col(c) for c in COLS) + ") " + src + ")"
+    sums = [str(c) for c in rng.choice(["l_extendedprice", "l_quantity", "x1", "l_discount"],
+                                       size=int(rng.integers(1, 4)), replace=False)]
+    aggs = " ".join(f"(fun sum {_col(c)})" for c in sums)
+    if kind == "global":
+        return f"(aggr global () ({aggs} (fun count)) {proj})"
+    keypool = SMALL + (["x1"] if dsmall else [])
+    keys = [str(c) for c in rng.choice(keypool, size=int(rng.integers(1, 3)), replace=False)]
+    count = " (fun count)" if rng.random() < 0.7 else ""
+    return f"(aggr hash ({' '.join(_col(c) for c in keys)}) ({aggs}{count}) {proj})"
+
+
+def _reference_lines(plan, tmp, tag):
+    gen, run = os.path.join(RDIR, "ref_gen"), os.path.join(RDIR, "ref_run")
+    cxx = (f"g++ -march=skylake-avx512 -mtune=generic -O3 -g0 -std=c++17 -include cstdint -DIS_RELEASE -w "
+           f"-I{REPO}/oracle/ref/shim -I{RDIR}/gen -I{REF} -I{REF}/libs -I{REF}/db-engine-paradigms/include")
+    lib = os.path.join(tmp, f"{tag}.so")
+    r = subprocess.run([gen, "--workload", SPEC, "--flavor", "vectorwise", "--out", lib, "--cxx", cxx,
+                        "--plan", plan], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    res = os.path.join(tmp, f"{tag}.txt")
+    r = subprocess.run([run, "--workload", SPEC, "--lib", lib, "--flavor", "vectorwise", "--threads", "4",
+                        "--reps", "1", "--result", res], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return sorted(line for line in open(res).read().split("\n") if line)
+
+
+@pytest.mark.skipif(not _have_reference(), reason="needs the reference build (oracle/_ref) and its source tree")
+def test_oracle_matches_reference_on_random_plans():
+    w = workload(SPEC)
+    data = generate_workload_host(w)
+    with tempfile.TemporaryDirectory() as tmp:
+        for i in range(N_PLANS):
+            plan = random_plan(1000 + i)
+            expect = _reference_lines(plan, tmp, f"p{i}")
+            assert result_lines(run_plan(plan, data)) == expect, plan
+
+
+def test_random_plans_are_deterministic_and_varied():
+    plans = [random_plan(1000 + i) for i in range(N_PLANS)]
+    assert plans == [random_plan(1000 + i) for i in range(N_PLANS)]
+    roots = {p.split(" ")[0] + " " + p.split(" ")[1] for p in plans}
+    assert {"(aggr hash", "(aggr global", "(select (fun"} <= roots

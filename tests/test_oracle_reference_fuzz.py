@@ -1,8 +1,8 @@
-"""The oracle against the reference itself on seeded random plans (selections, projections,
-hash, global and emitting roots over the lineitem-shaped table): each plan runs through the
-reference's vectorwise flavor, built from its sources by oracle/ref/Makefile, and through the
-oracle, and the sorted result lines must be identical.  CPU only; skipped where the reference
-build or its source tree is absent."""
+"""The oracle against the reference itself on seeded random plans: selections, projections,
+hash, global and emitting roots over the lineitem-shaped table, and Join01 probe chains over the
+star schema.  Each plan runs through the reference's vectorwise flavor, built from its sources
+by oracle/ref/Makefile, and through the oracle, and the sorted result lines must be identical.
+CPU only; skipped where the reference build or its source tree is absent."""
 import os
 import subprocess
 import tempfile
@@ -86,16 +86,16 @@ def random_plan(seed):
     return f"(aggr hash ({' '.join(_col(c) for c in keys)}) ({aggs}{count}) {proj})"
 
 
-def _reference_lines(plan, tmp, tag):
+def _reference_lines(plan, tmp, tag, spec=SPEC):
     gen, run = os.path.join(RDIR, "ref_gen"), os.path.join(RDIR, "ref_run")
     cxx = (f"g++ -march=skylake-avx512 -mtune=generic -O3 -g0 -std=c++17 -include cstdint -DIS_RELEASE -w "
            f"-I{REPO}/oracle/ref/shim -I{RDIR}/gen -I{REF} -I{REF}/libs -I{REF}/db-engine-paradigms/include")
     lib = os.path.join(tmp, f"{tag}.so")
-    r = subprocess.run([gen, "--workload", SPEC, "--flavor", "vectorwise", "--out", lib, "--cxx", cxx,
+    r = subprocess.run([gen, "--workload", spec, "--flavor", "vectorwise", "--out", lib, "--cxx", cxx,
                         "--plan", plan], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-2000:]
     res = os.path.join(tmp, f"{tag}.txt")
-    r = subprocess.run([run, "--workload", SPEC, "--lib", lib, "--flavor", "vectorwise", "--threads", "4",
+    r = subprocess.run([run, "--workload", spec, "--lib", lib, "--flavor", "vectorwise", "--threads", "4",
                         "--reps", "1", "--result", res], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-2000:]
     return sorted(line for line in open(res).read().split("\n") if line)
@@ -117,3 +117,52 @@ def test_random_plans_are_deterministic_and_varied():
     assert plans == [random_plan(1000 + i) for i in range(N_PLANS)]
     roots = {p.split(" ")[0] + " " + p.split(" ")[1] for p in plans}
     assert {"(aggr hash", "(aggr global", "(select (fun"} <= roots
+
+
+STAR_SPEC = "star:rows=20000,dates=300,custs=500,supps=20,parts=400,seed=83"
+N_JOIN_PLANS = 10
+# dimension: (fact foreign key, dimension key, attributes with their ranges)
+DIMS = {"date": ("lo_orderdate", "d_datekey", {"d_year": (1992, 1998), "d_weekday": (0, 6)}),
+        "customer": ("lo_custkey", "c_custkey", {"c_region": (0, 4), "c_mktsegment": (0, 4)}),
+        "part": ("lo_partkey", "p_partkey", {"p_category": (0, 24)})}
+FACT = "(scan lineorder (lo_orderdate lo_custkey lo_suppkey lo_partkey lo_revenue lo_supplycost))"
+
+
+def random_join_plan(seed):
+    """A probe chain of one to three Join01 joins of the fact table with filtered dimensions, a
+    root grouped by dimension attributes (or global), summing fact columns."""
+    rng = np.random.default_rng(seed)
+    cur = FACT
+    if rng.random() < 0.4:
+        cur = f"(select (fun < (col lineorder.lo_revenue) (const {int(rng.integers(1, 10_000_000))})) {cur})"
+    dims = [str(d) for d in rng.choice(list(DIMS), size=int(rng.integers(1, 4)), replace=False)]
+    attrs = []
+    for d in dims:
+        fk, key, cols = DIMS[d]
+        a = str(rng.choice(list(cols)))
+        attrs.append(f"{d}.{a}")
+        src = f"(scan {d} ({key} {' '.join(cols)}))"
+        if rng.random() < 0.7:
+            c = str(rng.choice(list(cols)))
+            lo, hi = cols[c]
+            op = str(rng.choice(["<", "<=", ">=", "=", "!="]))
+            src = f"(select (fun {op} (col {d}.{c}) (const {int(rng.integers(lo, hi + 1))})) {src})"
+        cur = f"(join join01 ((col lineorder.{fk})) () {cur} ((col {d}.{key})) ((col {d}.{a})) {src})"
+    sums = "(fun sum (col lineorder.lo_revenue))"
+    if rng.random() < 0.5:
+        sums += " (fun sum (col lineorder.lo_supplycost))"
+    if rng.random() < 0.25:
+        return f"(aggr global () ({sums} (fun count)) {cur})"
+    keys = [str(a) for a in rng.choice(attrs, size=int(rng.integers(1, len(attrs) + 1)), replace=False)]
+    return f"(aggr hash ({' '.join(f'(col {k})' for k in keys)}) ({sums} (fun count)) {cur})"
+
+
+@pytest.mark.skipif(not _have_reference(), reason="needs the reference build (oracle/_ref) and its source tree")
+def test_oracle_matches_reference_on_random_join_plans():
+    w = workload(STAR_SPEC)
+    data = generate_workload_host(w)
+    with tempfile.TemporaryDirectory() as tmp:
+        for i in range(N_JOIN_PLANS):
+            plan = random_join_plan(2000 + i)
+            expect = _reference_lines(plan, tmp, f"j{i}", STAR_SPEC)
+            assert result_lines(run_plan(plan, data)) == expect, plan

@@ -1,6 +1,6 @@
 """The oracle against the reference itself on seeded random plans: selections, projections,
-hash, global and emitting roots over the lineitem-shaped table, and Join01 probe chains over the
-star schema.  Each plan runs through the reference's vectorwise flavor, built from its sources
+hash, global and emitting roots over the lineitem-shaped table, Join01 probe chains over the star
+schema, JoinN joins and aggregations over aggregations.  Each plan runs through the reference's vectorwise flavor, built from its sources
 by oracle/ref/Makefile, and through the oracle, and the sorted result lines must be identical.
 CPU only; skipped where the reference build or its source tree is absent."""
 import os
@@ -165,4 +165,49 @@ def test_oracle_matches_reference_on_random_join_plans():
         for i in range(N_JOIN_PLANS):
             plan = random_join_plan(2000 + i)
             expect = _reference_lines(plan, tmp, f"j{i}", STAR_SPEC)
+            assert result_lines(run_plan(plan, data)) == expect, plan
+
+
+N_NESTED_PLANS = 8
+
+
+def random_nested_plan(seed):
+    """JoinN (the fact table as the build side, so every key has many matches) or an aggregation
+    over an aggregation (the inner one's outputs named aggr_ht1.key_<i> / aggr_ht1.aggr_<j>, as
+    the reference's translator names them)."""
+    rng = np.random.default_rng(seed)
+    if rng.random() < 0.5:
+        d = str(rng.choice(["customer", "date"]))
+        fk, key, cols = DIMS[d]
+        a = str(rng.choice(list(cols)))
+        src = f"(scan {d} ({key} {' '.join(cols)}))"
+        if rng.random() < 0.6:
+            lo, hi = cols[a]
+            src = f"(select (fun <= (col {d}.{a}) (const {int(rng.integers(lo, hi + 1))})) {src})"
+        pay = str(rng.choice(["lo_revenue", "lo_supplycost"]))
+        join = (f"(join joinN ((col {d}.{key})) () {src} ((col lineorder.{fk})) ((col lineorder.{pay})) "
+                f"(scan lineorder ({fk} {pay})))")
+        return f"(aggr hash ((col {d}.{a})) ((fun sum (col lineorder.{pay})) (fun count)) {join})"
+    k = str(rng.choice(["l_quantity", "l_discount", "l_tax"]))
+    v = str(rng.choice(["l_extendedprice", "l_quantity"]))
+    inner = (f"(aggr hash ((col lineitem.{k}) (col lineitem.l_returnflag)) ((fun sum (col lineitem.{v})) (fun count)) "
+             f"(scan lineitem ({k} l_returnflag {v})))")
+    if rng.random() < 0.5:
+        return f"(aggr hash ((col aggr_ht1.key_1)) ((fun sum (col aggr_ht1.aggr_0)) (fun count)) {inner})"
+    return (f"(aggr global () ((fun sum (col aggr_ht1.aggr_1)) (fun count)) "
+            f"(select (fun > (col aggr_ht1.aggr_1) (const {int(rng.integers(100, 700))})) {inner}))")
+
+
+@pytest.mark.skipif(not _have_reference(), reason="needs the reference build (oracle/_ref) and its source tree")
+def test_oracle_matches_reference_on_random_nested_plans():
+    star = workload(STAR_SPEC)
+    star_data = generate_workload_host(star)
+    flat = workload(SPEC)
+    flat_data = generate_workload_host(flat)
+    with tempfile.TemporaryDirectory() as tmp:
+        for i in range(N_NESTED_PLANS):
+            plan = random_nested_plan(3000 + i)
+            joined = "joinN" in plan
+            spec, data = (STAR_SPEC, star_data) if joined else (SPEC, flat_data)
+            expect = _reference_lines(plan, tmp, f"n{i}", spec)
             assert result_lines(run_plan(plan, data)) == expect, plan

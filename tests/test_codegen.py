@@ -190,7 +190,8 @@ def test_dense_join_tables_follow_the_key_space():
     assert "atomicCAS(&jdt" in src and "join_probe_bucket" not in src
 
 
-@pytest.mark.parametrize("flavor", ["cuda(rows=3)", "cuda(threads=100)", "cuda(aggr=magic)", "gpu(x=1)", "cuda(nokey=1)"])
+@pytest.mark.parametrize("flavor", ["cuda(rows=3)", "cuda(threads=100)", "cuda(aggr=magic)", "gpu(x=1)", "cuda(nokey=1)",
+                                    "cuda(lowcard=stacked)", "cuda(minctas=33)", "cuda(minctas=-1)", "cuda(pgroups=17)"])
 def test_bad_flavors_are_rejected(flavor):
     w, e = offline("sel_aggr:rows=1000")
     with pytest.raises(VoilaError) as ex:

@@ -1,6 +1,6 @@
 """The oracle against the reference itself on seeded random plans: selections, projections,
 hash, global and emitting roots over the lineitem-shaped table, Join01 probe chains over the star
-schema, JoinN joins and aggregations over aggregations.  Each plan runs through the reference's vectorwise flavor, built from its sources
+schema, JoinN joins, aggregations over aggregations and string predicates and keys.  Each plan runs through the reference's vectorwise flavor, built from its sources
 by oracle/ref/Makefile, and through the oracle, and the sorted result lines must be identical.
 CPU only; skipped where the reference build or its source tree is absent."""
 import os
@@ -210,4 +210,43 @@ def test_oracle_matches_reference_on_random_nested_plans():
             joined = "joinN" in plan
             spec, data = (STAR_SPEC, star_data) if joined else (SPEC, flat_data)
             expect = _reference_lines(plan, tmp, f"n{i}", spec)
+            assert result_lines(run_plan(plan, data)) == expect, plan
+
+
+STR_SPEC = "strings:rows=20000,parts=600,seed=84"
+N_STRING_PLANS = 10
+PATTERNS = ["re", "ee", "pink", "a", "zz", "ol", "white", "navy"]
+BRANDS = ["azure", "black", "amber", "coral", "none"]
+
+
+def random_string_plan(seed):
+    """Predicates on string columns (contains on p_name, equality on p_brand) under and/or, for an
+    emitting select over the string table or a join grouped by a string key."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for _ in range(int(rng.integers(1, 3))):
+        if rng.random() < 0.6:
+            parts.append(f"(fun contains (col part.p_name) (const {rng.choice(PATTERNS)}))")
+        else:
+            parts.append(f"(fun {rng.choice(['=', '!='])} (col part.p_brand) (const {rng.choice(BRANDS)}))")
+    pred = parts[0]
+    for p in parts[1:]:
+        pred = f"(fun {rng.choice(['and', 'or'])} {pred} {p})"
+    part = f"(select {pred} (scan part (p_partkey p_name p_brand)))"
+    if rng.random() < 0.25:
+        return part
+    key = str(rng.choice(["p_brand", "p_name"]))
+    return (f"(aggr hash ((col part.{key})) ((fun sum (col lineitem.l_extendedprice)) (fun count)) "
+            f"(join join01 ((col lineitem.l_partkey)) () (scan lineitem (l_partkey l_extendedprice)) "
+            f"((col part.p_partkey)) ((col part.{key})) {part}))")
+
+
+@pytest.mark.skipif(not _have_reference(), reason="needs the reference build (oracle/_ref) and its source tree")
+def test_oracle_matches_reference_on_random_string_plans():
+    w = workload(STR_SPEC)
+    data = generate_workload_host(w)
+    with tempfile.TemporaryDirectory() as tmp:
+        for i in range(N_STRING_PLANS):
+            plan = random_string_plan(4000 + i)
+            expect = _reference_lines(plan, tmp, f"s{i}", STR_SPEC)
             assert result_lines(run_plan(plan, data)) == expect, plan

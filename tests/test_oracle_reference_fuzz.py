@@ -6,6 +6,7 @@ CPU only; skipped where the reference build or its source tree is absent."""
 import os
 import subprocess
 import tempfile
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import pytest
@@ -86,30 +87,44 @@ def random_plan(seed):
     return f"(aggr hash ({' '.join(_col(c) for c in keys)}) ({aggs}{count}) {proj})"
 
 
-def _reference_lines(plan, tmp, tag, spec=SPEC):
+def _reference_results(jobs, tmp):
+    """Sorted result lines of each (tag, plan, spec) job from the reference's vectorwise flavor:
+    the query libraries are generated and compiled in parallel, then run one after another."""
     gen, run = os.path.join(RDIR, "ref_gen"), os.path.join(RDIR, "ref_run")
     cxx = (f"g++ -march=skylake-avx512 -mtune=generic -O3 -g0 -std=c++17 -include cstdint -DIS_RELEASE -w "
            f"-I{REPO}/oracle/ref/shim -I{RDIR}/gen -I{REF} -I{REF}/libs -I{REF}/db-engine-paradigms/include")
-    lib = os.path.join(tmp, f"{tag}.so")
-    r = subprocess.run([gen, "--workload", spec, "--flavor", "vectorwise", "--out", lib, "--cxx", cxx,
-                        "--plan", plan], capture_output=True, text=True)
-    assert r.returncode == 0, r.stderr[-2000:]
-    res = os.path.join(tmp, f"{tag}.txt")
-    r = subprocess.run([run, "--workload", spec, "--lib", lib, "--flavor", "vectorwise", "--threads", "4",
-                        "--reps", "1", "--result", res], capture_output=True, text=True)
-    assert r.returncode == 0, r.stderr[-2000:]
-    return sorted(line for line in open(res).read().split("\n") if line)
+
+    def build(job):
+        tag, plan, spec = job
+        lib = os.path.join(tmp, f"{tag}.so")
+        r = subprocess.run([gen, "--workload", spec, "--flavor", "vectorwise", "--out", lib, "--cxx", cxx,
+                            "--plan", plan], capture_output=True, text=True)
+        return lib, r
+
+    with ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as pool:
+        built = list(pool.map(build, jobs))
+    out = {}
+    for (tag, plan, spec), (lib, r) in zip(jobs, built):
+        assert r.returncode == 0, (plan, r.stderr[-2000:])
+        res = os.path.join(tmp, f"{tag}.txt")
+        r = subprocess.run([run, "--workload", spec, "--lib", lib, "--flavor", "vectorwise", "--threads", "4",
+                            "--reps", "1", "--result", res], capture_output=True, text=True)
+        assert r.returncode == 0, (plan, r.stderr[-2000:])
+        out[tag] = sorted(line for line in open(res).read().split("\n") if line)
+    return out
+
+
+def _check(jobs, data_of):
+    with tempfile.TemporaryDirectory() as tmp:
+        expect = _reference_results(jobs, tmp)
+    for tag, plan, spec in jobs:
+        assert result_lines(run_plan(plan, data_of[spec])) == expect[tag], plan
 
 
 @pytest.mark.skipif(not _have_reference(), reason="needs the reference build (oracle/_ref) and its source tree")
 def test_oracle_matches_reference_on_random_plans():
-    w = workload(SPEC)
-    data = generate_workload_host(w)
-    with tempfile.TemporaryDirectory() as tmp:
-        for i in range(N_PLANS):
-            plan = random_plan(1000 + i)
-            expect = _reference_lines(plan, tmp, f"p{i}")
-            assert result_lines(run_plan(plan, data)) == expect, plan
+    _check([(f"p{i}", random_plan(1000 + i), SPEC) for i in range(N_PLANS)],
+           {SPEC: generate_workload_host(workload(SPEC))})
 
 
 def test_random_plans_are_deterministic_and_varied():
@@ -159,13 +174,8 @@ def random_join_plan(seed):
 
 @pytest.mark.skipif(not _have_reference(), reason="needs the reference build (oracle/_ref) and its source tree")
 def test_oracle_matches_reference_on_random_join_plans():
-    w = workload(STAR_SPEC)
-    data = generate_workload_host(w)
-    with tempfile.TemporaryDirectory() as tmp:
-        for i in range(N_JOIN_PLANS):
-            plan = random_join_plan(2000 + i)
-            expect = _reference_lines(plan, tmp, f"j{i}", STAR_SPEC)
-            assert result_lines(run_plan(plan, data)) == expect, plan
+    _check([(f"j{i}", random_join_plan(2000 + i), STAR_SPEC) for i in range(N_JOIN_PLANS)],
+           {STAR_SPEC: generate_workload_host(workload(STAR_SPEC))})
 
 
 N_NESTED_PLANS = 8
@@ -200,17 +210,9 @@ def random_nested_plan(seed):
 
 @pytest.mark.skipif(not _have_reference(), reason="needs the reference build (oracle/_ref) and its source tree")
 def test_oracle_matches_reference_on_random_nested_plans():
-    star = workload(STAR_SPEC)
-    star_data = generate_workload_host(star)
-    flat = workload(SPEC)
-    flat_data = generate_workload_host(flat)
-    with tempfile.TemporaryDirectory() as tmp:
-        for i in range(N_NESTED_PLANS):
-            plan = random_nested_plan(3000 + i)
-            joined = "joinN" in plan
-            spec, data = (STAR_SPEC, star_data) if joined else (SPEC, flat_data)
-            expect = _reference_lines(plan, tmp, f"n{i}", spec)
-            assert result_lines(run_plan(plan, data)) == expect, plan
+    plans = [random_nested_plan(3000 + i) for i in range(N_NESTED_PLANS)]
+    _check([(f"n{i}", p, STAR_SPEC if "joinN" in p else SPEC) for i, p in enumerate(plans)],
+           {STAR_SPEC: generate_workload_host(workload(STAR_SPEC)), SPEC: generate_workload_host(workload(SPEC))})
 
 
 STR_SPEC = "strings:rows=20000,parts=600,seed=84"
@@ -243,10 +245,5 @@ def random_string_plan(seed):
 
 @pytest.mark.skipif(not _have_reference(), reason="needs the reference build (oracle/_ref) and its source tree")
 def test_oracle_matches_reference_on_random_string_plans():
-    w = workload(STR_SPEC)
-    data = generate_workload_host(w)
-    with tempfile.TemporaryDirectory() as tmp:
-        for i in range(N_STRING_PLANS):
-            plan = random_string_plan(4000 + i)
-            expect = _reference_lines(plan, tmp, f"s{i}", STR_SPEC)
-            assert result_lines(run_plan(plan, data)) == expect, plan
+    _check([(f"s{i}", random_string_plan(4000 + i), STR_SPEC) for i in range(N_STRING_PLANS)],
+           {STR_SPEC: generate_workload_host(workload(STR_SPEC))})

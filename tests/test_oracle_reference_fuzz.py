@@ -1,6 +1,7 @@
 """The oracle against the reference itself on seeded random plans: selections, projections,
 hash, global and emitting roots over the lineitem-shaped table, Join01 probe chains over the star
-schema, JoinN joins, aggregations over aggregations and string predicates and keys.  Each plan runs through the reference's vectorwise flavor, built from its sources
+schema, JoinN joins, aggregations over aggregations, string predicates and keys, sums past int64
+and extract_year keys.  Each plan runs through the reference's vectorwise flavor, built from its sources
 by oracle/ref/Makefile, and through the oracle, and the sorted result lines must be identical.
 CPU only; skipped where the reference build or its source tree is absent."""
 import os
@@ -247,3 +248,34 @@ def random_string_plan(seed):
 def test_oracle_matches_reference_on_random_string_plans():
     _check([(f"s{i}", random_string_plan(4000 + i), STR_SPEC) for i in range(N_STRING_PLANS)],
            {STR_SPEC: generate_workload_host(workload(STR_SPEC))})
+
+
+WIDE_SPEC = "bigsum:rows=40000,seed=85"
+N_WIDE_PLANS = 6
+
+
+def random_wide_plan(seed):
+    """Sums whose bound leaves int64 (values up to ±2e15 over 40,000 rows: the reference types them
+    i128), grouped or global, behind a filter on the group column or the values; and extract_year
+    keys over the lineitem-shaped table."""
+    rng = np.random.default_rng(seed)
+    if rng.random() < 0.3:
+        d = int(rng.integers(2448623, 2451148))
+        return (f"(aggr hash ((col y)) ((fun sum (col lineitem.l_quantity)) (fun count)) (project ((assign y (fun "
+                f"extract_year (col lineitem.l_shipdate))) (col lineitem.l_quantity)) (select (fun >= "
+                f"(col lineitem.l_shipdate) (const {d})) (scan lineitem (l_shipdate l_quantity)))))")
+    sums = " ".join(f"(fun sum (col fact.{c}))" for c in rng.choice(["v", "w"], size=int(rng.integers(1, 3)), replace=False))
+    if rng.random() < 0.5:
+        src = f"(select (fun != (col fact.g) (const {int(rng.integers(0, 4))})) (scan fact (g v w)))"
+    else:
+        src = f"(select (fun > (col fact.v) (const {int(rng.integers(-10**15, 10**15))})) (scan fact (g v w)))"
+    if rng.random() < 0.4:
+        return f"(aggr global () ({sums} (fun count)) {src})"
+    return f"(aggr hash ((col fact.g)) ({sums} (fun count)) {src})"
+
+
+@pytest.mark.skipif(not _have_reference(), reason="needs the reference build (oracle/_ref) and its source tree")
+def test_oracle_matches_reference_on_random_wide_and_year_plans():
+    plans = [random_wide_plan(5000 + i) for i in range(N_WIDE_PLANS)]
+    _check([(f"w{i}", p, SPEC if "extract_year" in p else WIDE_SPEC) for i, p in enumerate(plans)],
+           {WIDE_SPEC: generate_workload_host(workload(WIDE_SPEC)), SPEC: generate_workload_host(workload(SPEC))})

@@ -18,6 +18,14 @@ reference's flush2partitions + re-aggregation) inside the timed region.
 --impl reference times the reference's own CPU implementation (its hyper and vectorwise
 flavors compiled from source into oracle/_ref, all host threads) on the same workload; if
 that build is not usable on this host it falls back to the numpy port of the oracle.
+
+--workload config5 times the mixed batch (256 seeded pipelines) one query after another with
+exhaustively tuned flavors against a batch with learned flavors.  Environment knobs:
+VC_BATCH_N / VC_BATCH_MAX_ROWS (the mix), VC_TRAIN_N / VC_TUNE_REPS (the chooser's training
+set and the autotuner's repetitions), VC_BATCH_SOLO_ROWS (queries with a pipeline of at least
+this many rows run as their own launches after the persistent kernel; 0 = all inside it) and
+VC_CONFIG5_FLAVORS=default (both arms on the default flavor, no tuning).
+--device-only and --host-resident-only run just the query, --steps times, for a profiler.
 """
 import argparse
 import json

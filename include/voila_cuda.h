@@ -276,7 +276,8 @@ int vc_batch_new(vc_query** queries, int n, const char** flavors, int threads, i
 /* vc_batch_new whose queries with a pipeline of at least solo_rows rows (0 = none) run as
  * their own launches, with their own flavors' kernels, on the same stream right after the
  * persistent kernel that runs the rest: a pipeline that fills the GPU by itself gains nothing
- * from the batch's lean shared shapes.  vc_batch_info reports "batched" and "solo" counts;
+ * from the batch's lean shared shapes (a solo query runs the flavor it was created with; its
+ * entry in flavors is not used).  vc_batch_info reports "batched" and "solo" counts;
  * vc_batch_latencies gives a solo query the time from the batch's start to its end.  No
  * counterpart in the reference, which runs queries one at a time. */
 int vc_batch_new_split(vc_query** queries, int n, const char** flavors, int threads, int64_t tiles_per_item,

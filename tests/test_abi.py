@@ -88,3 +88,25 @@ def test_reference_side_glue_library_exports_the_generated_query_abi():
     r = subprocess.run([os.path.join(rdir, "ref_run"), "--workload", "star:rows=1000,custs=50", "--lib", lib,
                         "--flavor", "cuda", "--reps", "1"], capture_output=True, text=True, timeout=120)
     assert r.returncode == 1 and "cuda flavor:" in r.stderr
+
+
+def test_product_code_never_reaches_the_oracle():
+    """The library and its Python binding import, link or run nothing under oracle/ (the oracle
+    is test infrastructure: only tests, smoke() and bench.py's baseline legs use it)."""
+    import ast
+    import os
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "vldb_voila_b200")
+    for name in os.listdir(pkg):
+        if name.endswith(".py"):
+            tree = ast.parse(open(os.path.join(pkg, name)).read())
+            for node in ast.walk(tree):
+                if isinstance(node, ast.Import):
+                    assert not any(a.name.split(".")[0] == "oracle" for a in node.names), name
+                elif isinstance(node, ast.ImportFrom):
+                    assert (node.module or "").split(".")[0] != "oracle", name
+    csrc = os.path.join(pkg, "csrc")
+    for root, _, files in os.walk(csrc):
+        for name in files:
+            if name.endswith((".cpp", ".hpp", ".cu", ".cuh", ".h")):
+                text = open(os.path.join(root, name)).read()
+                assert "oracle/" not in text and "voila_oracle" not in text, name

@@ -178,7 +178,9 @@ int vc_workload_batch(int count, uint64_t seed, int64_t min_rows, int64_t max_ro
  * lowcard=combine|atomic|private|redux|regs|packed, pgroups (groups per CTA of lowcard=private|regs|packed),
  * build=auto|direct|staged|dense, hash=mix|voila, fill, dense, sinksmem, gcap (group table
  * slots), ocap (result rows of an emitting plan), probe (1..32 lanes that probe one join key
- * together), grid, minctas (CTAs per SM the main kernel's registers must allow), graph.
+ * together), grid, minctas (CTAs per SM the main kernel's registers must allow),
+ * stream=ldg|noalloc (column loads through the read-only path, or without L1 allocation so that
+ * probed tables keep L1), graph.
  * VC_ERR_INVALID for an unknown or out-of-range knob; VC_ERR_UNSUPPORTED when the flavor's
  * shared memory exceeds the device's per-CTA limit or build=dense meets a large key space. */
 int vc_query_new(vc_engine* eng, const char* plan, const char* flavor, vc_query** out);

@@ -14,7 +14,8 @@ FLAVORS = ["", "cuda(load=tma,stages=2)", "cuda(lowcard=private,prefetch=0)", "c
            "cuda(aggr=part,load=tma,stages=2,compact=0)", "cuda(frows=1)", "cuda(frows=8,compact=0,aggr=part)",
            "cuda(lowcard=regs)", "cuda(lowcard=regs,load=tma,stages=2,rows=8,pgroups=4)",
            "cuda(aggr=direct)", "cuda(aggr=dcache,cache=256)", "cuda(lowcard=combine)",
-           "cuda(lowcard=packed,load=tma,stages=2,pgroups=3)"]
+           "cuda(lowcard=packed,load=tma,stages=2,pgroups=3)", "cuda(stream=noalloc)",
+           "cuda(stream=noalloc,compact=0,rows=8)"]
 
 
 def offline(spec):
@@ -191,7 +192,8 @@ def test_dense_join_tables_follow_the_key_space():
 
 
 @pytest.mark.parametrize("flavor", ["cuda(rows=3)", "cuda(threads=100)", "cuda(aggr=magic)", "gpu(x=1)", "cuda(nokey=1)",
-                                    "cuda(lowcard=stacked)", "cuda(minctas=33)", "cuda(minctas=-1)", "cuda(pgroups=17)"])
+                                    "cuda(lowcard=stacked)", "cuda(minctas=33)", "cuda(minctas=-1)", "cuda(pgroups=17)",
+                                    "cuda(stream=cg)"])
 def test_bad_flavors_are_rejected(flavor):
     w, e = offline("sel_aggr:rows=1000")
     with pytest.raises(VoilaError) as ex:
@@ -402,3 +404,15 @@ def test_tma_ring_without_block_barriers():
             "(scan lineitem (l_shipdate l_quantity)))")
     src2 = e.query(emit, "cuda(load=tma,stages=2)").source()
     assert "empty[" not in src2 and "vd::block_any(!ok)" in src2
+
+
+def test_stream_noalloc_loads_columns_without_l1_allocation():
+    """stream=noalloc: every column load of the fused kernel (eager tiles and the compaction
+    flush's gathers) takes load mode 2 (ld.global.nc.L1::no_allocate); the default keeps the
+    read-only path."""
+    w, e = offline("star:rows=100000")
+    src = e.query(w.plan, "cuda(stream=noalloc)").source()
+    main = src[src.index("vc_p4_main"):]
+    assert "vd::load_rows<int32_t, 4, 2>(c0" in main and "vd::load_one<int32_t, 2>(" in main
+    assert ", 2>(" not in e.query(w.plan).source()
+    assert "stream=noalloc" in e.query(w.plan, "cuda(stream=noalloc)").info()["flavor"]

@@ -924,6 +924,14 @@ struct PipeGen {
 		}
 	}
 
+	/* template load mode of column c (vd::col_ld): 1 host-resident, 2 stream=noalloc, else 0 */
+	std::string load_mode(size_t c) const {
+		if (p.cols[c].host) {
+			return ", 1";
+		}
+		return fl.stream == "noalloc" ? ", 2" : "";
+	}
+
 	void emit_load_cols(const std::string& src, const std::string& dst, const std::string& r0) {
 		for (size_t c = 0; c < p.cols.size(); c++) {
 			if (!eager[c]) {
@@ -934,7 +942,7 @@ struct PipeGen {
 				o << "    vd::load_rows_smem<" << ct << ", " << V << ">((const " << ct << "*)(stage + " << tile_region(c)
 				  << ") + threadIdx.x * " << V << ", " << dst << c << ");\n";
 			} else {
-				o << "    vd::load_rows<" << ct << ", " << V << (p.cols[c].host ? ", true" : "") << ">(c" << c << ", " << r0
+				o << "    vd::load_rows<" << ct << ", " << V << load_mode(c) << ">(c" << c << ", " << r0
 				  << ", n, " << dst << c << ");\n";
 			}
 		}
@@ -963,7 +971,7 @@ struct PipeGen {
 		for (size_t c = 0; c < p.cols.size(); c++) {
 			if (lazy_first_use[c] == at) {
 				o << "#pragma unroll\n      for (int v = 0; v < " << V << "; v++) { if (act[v]) { x" << c << "[v] = vd::load_one<"
-				  << ctype(p.cols[c].type) << (p.cols[c].host ? ", true" : "") << ">(c" << c << ", row[v]); } }\n";
+				  << ctype(p.cols[c].type) << load_mode(c) << ">(c" << c << ", row[v]); } }\n";
 			}
 		}
 	}

@@ -112,22 +112,56 @@ __device__ __forceinline__ int64_t mulw(int64_t a, int64_t b)
 
 /* ---------------------------------------------------------------- loads ---------- */
 
-/* Loads rows [r0, r0+V) of a column into registers.  Whole tiles use vector loads through
- * the read-only path (the column base is 16-byte aligned and r0 is a multiple of V);
- * the ragged tail falls back to bounds-checked scalar loads. */
-/* One read of column data: through the read-only path from HBM, or a coherent L2 load
- * (ld.global.cg) from a column that lives in pinned host memory (SYS). */
-template <bool SYS, typename T>
+/* A read-only load that does not allocate in L1 (ld.global.nc.L1::no_allocate): column data
+ * streamed once leaves L1 to the join and group tables that are probed again. */
+template <typename T>
+__device__ __forceinline__ T ld_noalloc(const T* p)
+{
+	if constexpr (sizeof(T) == 16) {
+		uint4 r;
+		asm("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+			: "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w) : "l"(p));
+		return *reinterpret_cast<const T*>(&r);
+	} else if constexpr (sizeof(T) == 8) {
+		unsigned long long r;
+		asm("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(r) : "l"(p));
+		return *reinterpret_cast<const T*>(&r);
+	} else if constexpr (sizeof(T) == 4) {
+		unsigned r;
+		asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(r) : "l"(p));
+		return *reinterpret_cast<const T*>(&r);
+	} else if constexpr (sizeof(T) == 2) {
+		unsigned short r;
+		asm("ld.global.nc.L1::no_allocate.u16 %0, [%1];" : "=h"(r) : "l"(p));
+		return *reinterpret_cast<const T*>(&r);
+	} else {
+		static_assert(sizeof(T) == 1, "column element of 1, 2, 4, 8 or 16 bytes");
+		unsigned short r;
+		asm("ld.global.nc.L1::no_allocate.u8 %0, [%1];" : "=h"(r) : "l"(p));
+		const unsigned char b = (unsigned char)r;
+		return *reinterpret_cast<const T*>(&b);
+	}
+}
+
+/* One read of column data, by load mode M: 0 through the read-only path from HBM, 1 a
+ * coherent L2 load (ld.global.cg) from a column that lives in pinned host memory, 2 the
+ * read-only path without L1 allocation (flavor knob stream=noalloc). */
+template <int M, typename T>
 __device__ __forceinline__ T col_ld(const T* p)
 {
-	if constexpr (SYS) {
+	if constexpr (M == 1) {
 		return __ldcg(p);
+	} else if constexpr (M == 2) {
+		return ld_noalloc(p);
 	} else {
 		return __ldg(p);
 	}
 }
 
-template <typename T, int V, bool SYS = false>
+/* Loads rows [r0, r0+V) of a column into registers.  Whole tiles use vector loads (the
+ * column base is 16-byte aligned and r0 is a multiple of V); the ragged tail falls back to
+ * bounds-checked scalar loads. */
+template <typename T, int V, int M = 0>
 __device__ __forceinline__ void load_rows(const T* __restrict__ col, int64_t r0, int64_t n, T (&out)[V])
 {
 	constexpr int bytes = V * (int)sizeof(T);
@@ -137,20 +171,20 @@ __device__ __forceinline__ void load_rows(const T* __restrict__ col, int64_t r0,
 			uint4 tmp[bytes / 16];
 #pragma unroll
 			for (int i = 0; i < bytes / 16; i++) {
-				tmp[i] = col_ld<SYS>(reinterpret_cast<const uint4*>(p) + i);
+				tmp[i] = col_ld<M>(reinterpret_cast<const uint4*>(p) + i);
 			}
 #pragma unroll
 			for (int i = 0; i < V; i++) {
 				out[i] = reinterpret_cast<const T*>(tmp)[i];
 			}
 		} else if constexpr (bytes == 8) {
-			uint2 tmp = col_ld<SYS>(reinterpret_cast<const uint2*>(p));
+			uint2 tmp = col_ld<M>(reinterpret_cast<const uint2*>(p));
 #pragma unroll
 			for (int i = 0; i < V; i++) {
 				out[i] = reinterpret_cast<const T*>(&tmp)[i];
 			}
 		} else if constexpr (bytes == 4) {
-			unsigned int tmp = col_ld<SYS>(reinterpret_cast<const unsigned int*>(p));
+			unsigned int tmp = col_ld<M>(reinterpret_cast<const unsigned int*>(p));
 #pragma unroll
 			for (int i = 0; i < V; i++) {
 				out[i] = reinterpret_cast<const T*>(&tmp)[i];
@@ -158,21 +192,21 @@ __device__ __forceinline__ void load_rows(const T* __restrict__ col, int64_t r0,
 		} else {
 #pragma unroll
 			for (int i = 0; i < V; i++) {
-				out[i] = col_ld<SYS>(p + i);
+				out[i] = col_ld<M>(p + i);
 			}
 		}
 	} else {
 #pragma unroll
 		for (int i = 0; i < V; i++) {
-			out[i] = (r0 + i < n) ? col_ld<SYS>(col + r0 + i) : (T)0;
+			out[i] = (r0 + i < n) ? col_ld<M>(col + r0 + i) : (T)0;
 		}
 	}
 }
 
-template <typename T, bool SYS = false>
+template <typename T, int M = 0>
 __device__ __forceinline__ T load_one(const T* __restrict__ col, int64_t row)
 {
-	return col_ld<SYS>(col + row);
+	return col_ld<M>(col + row);
 }
 
 /* Reads this thread's V consecutive rows of a column tile staged in shared memory. */

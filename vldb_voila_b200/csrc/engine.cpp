@@ -70,6 +70,9 @@ std::string Flavor::str() const
 	if (min_ctas) {
 		o << ",minctas=" << min_ctas;
 	}
+	if (stream != "ldg") {
+		o << ",stream=" << stream;
+	}
 	if (private_groups != 8) {
 		o << ",pgroups=" << private_groups;
 	}
@@ -208,6 +211,11 @@ void Flavor::apply(Flavor& f, const std::string& s0)
 			f.private_groups = num(1, 16);
 		} else if (k == "minctas") {
 			f.min_ctas = num(0, 32);
+		} else if (k == "stream") {
+			if (v != "ldg" && v != "noalloc") {
+				throw Error(1, "stream must be ldg or noalloc");
+			}
+			f.stream = v;
 		} else if (k == "parts") {
 			f.parts = num(0, 2048);
 			if (f.parts && (f.parts < 16 || (f.parts & (f.parts - 1)))) {

@@ -241,6 +241,8 @@ struct Flavor {
 	int stages = 4;           /* tma ring depth */
 	std::string build = "auto"; /* join build: auto | direct | staged | dense */
 	bool prefetch = true;     /* ldg: load the next tile while the current one is processed */
+	std::string stream = "ldg"; /* column loads: ldg (read-only path) | noalloc (read-only path without
+	                             * L1 allocation, so probed tables keep L1) */
 	int compact = -2;         /* compact survivors after op k (-1 never, -2 auto) */
 	std::string lowcard = "packed";  /* dense aggregation: combine (warp pre-sum by shuffles) | atomic (per-warp
 	                                  * replicas) | private (per-thread accumulators behind a block dictionary)
